@@ -1,0 +1,466 @@
+#!/usr/bin/env python3
+"""Benchmark of the WENO path on B200.
+
+Workload (one "step"): FP64 WENO5-JS reconstruction with the MP limiter fused,
+x, y and z sweeps, on a 200^3-cell block (m=n=p=199) with v_size=8 and
+buff_size=6 -- 3 x 148,135,424 = 444.4 M face states per step.  Inputs are
+the seeded smooth-plus-jump field and the true uniform-grid WENO5-JS
+coefficients.  Metric: face-states/s (whole job).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of the reference harness (the
+oracle; the Fortran reference cannot be built here) on the host cores.
+Multi-GPU (torchrun): every rank owns its own 200^3 x 8 block (weak
+scaling); there is no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M = 199
+NV = 8
+BUFF = 6
+ORDER = 5
+METRIC = "WENO5 face-states/s at 199^3 x 8 vars (FP64 WENO5-JS + MP, x/y/z sweeps)"
+
+
+def face_states_per_dir(m=M, nv=NV, buff=BUFF):
+    N = m + 2 * buff + 1
+    return 2 * (N - 6) * N * N * nv
+
+
+def alg_bytes_per_sweep(m=M, nv=NV, buff=BUFF, elem=8, order=ORDER):
+    """Algorithmic HBM bytes of one fused sweep: read the (NC+2H)-long
+    stencil window of every column once, write vL and vR on the NC core faces."""
+    N = m + 2 * buff + 1
+    NC = N - 6
+    H = max((order - 1) // 2, 2)
+    return (NC + 2 * H) * N * N * nv * elem + 2 * NC * N * N * nv * elem
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """NVML samples of SM clock and throttle reasons during the timed region."""
+
+    REASONS = {
+        "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": len(self.samples)}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import datetime
+
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    return rank, ws, local, dist
+
+
+def cpu_reference_run(steps, warmup, sample_nv=2, quiet=False):
+    """Time the oracle (CPU restatement of the reference path) on all host
+    threads: x/y/z WENO5-JS + MP from the reshaped fields, on a sample of
+    `sample_nv` of the 8 variables (same grid, same per-variable work)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from wenostandalone_b200 import fields
+    oracle.build()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    vf = fields.smooth_jump_field(M, M, M, sample_nv, BUFF, seed=0)
+    ins = []
+    for d in range(3):
+        rs = oracle.reshape(vf, M, M, M, BUFF, d)
+        coefs = fields.uniform_weno_coefficients(5, rs.shape[0] - 12)
+        L, R = oracle.order1_copy(vf, M, M, M, BUFF, d)
+        ins.append((rs, coefs, L, R))
+
+    def step():
+        for rs, coefs, L, R in ins:
+            oracle.reconstruct(rs, coefs, 5, vL=L, vR=R)
+            oracle.preserve_monotonicity(rs, L, R)
+
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = (time.perf_counter() - t0) / max(steps, 1)
+    fs = 3 * face_states_per_dir(nv=sample_nv)
+    return {"value": fs / dt, "sec_per_step": dt, "cores": threads, "face_states": fs,
+            "sample": f"x/y/z WENO5-JS + MP on 200^3 cells x {sample_nv} of {NV} variables "
+                      f"({fs/1e6:.1f} M face states per step), from pre-reshaped fields"}
+
+
+def run_reference(args):
+    rank, ws, _, dist = dist_init()
+    if rank != 0:
+        return 0
+    r = cpu_reference_run(args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "face-states/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "WENO5-JS + MP, x/y/z sweeps, 200^3 cells, FP64", "m=n=p": M,
+                   "v_size": NV, "buff_size": BUFF},
+        "cpu_baseline": {"value": r["value"], "unit": "face-states/s", "cores": r["cores"], "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": "face-states/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import _lib as L
+    from wenostandalone_b200 import api, fields
+
+    rank, ws, local, dist = dist_init()
+    if dist is not None:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local if dist is not None else 0)
+    torch.cuda.set_device(dev)
+    wsb.lib()
+
+    g = wsb.Grid(M, M, M, NV, BUFF)
+    vf_host = fields.smooth_jump_field(M, M, M, NV, BUFF, seed=rank)
+    v = torch.from_numpy(vf_host.ravel(order="F")).to(dev)
+    coefs = [tuple(torch.from_numpy(c.ravel(order="F")).to(dev)
+                   for c in fields.uniform_weno_coefficients(ORDER, g.nc(d))) for d in range(3)]
+    cstructs = [api.coefs_struct(c) for c in coefs]
+    nface = int(np.prod(g.face_shape(0)))
+    outs = [(torch.empty(nface, dtype=torch.float64, device=dev),
+             torch.empty(nface, dtype=torch.float64, device=dev)) for _ in range(3)]
+    stream = torch.cuda.Stream(device=dev)
+    sp = int(stream.cuda_stream)
+    flags = wsb.F_MP | wsb.F_FOLDED
+
+    def step(evs=None):
+        for d in range(3):
+            if evs is not None:
+                evs[d][0].record(stream)
+            api.weno(g, d, ORDER, v, cstructs[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
+            if evs is not None:
+                evs[d][1].record(stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    per_kernel = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(3)] for _ in range(K)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+        t_start.record(stream)
+        for k in range(K):
+            step(per_kernel[k])
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / K
+    fs_step = 3 * face_states_per_dir()
+    value = ws * fs_step / (ms_per_step * 1e-3)
+
+    # dominant kernel: the sweep with the largest summed time
+    sums = [sum(per_kernel[k][d][0].elapsed_time(per_kernel[k][d][1]) for k in range(K)) for d in range(3)]
+    dk = int(np.argmax(sums))
+    dk_ms = sums[dk] / K
+    peak, peak_kind = load_peaks()
+    ab = alg_bytes_per_sweep()
+    achieved = ab / (dk_ms * 1e-3) / 1e9
+
+    # FP32-bulk variant (same sweeps, FP32 v_rs_ws field and face states)
+    fp32 = None
+    if not args.no_extras:
+        fp32 = measure_fp32_bulk(g, v, cstructs, outs, stream, K, dev)
+        drop = measure_drop_in(g, v, cstructs, outs, stream, K, dev)
+    else:
+        drop = None
+
+    # end-to-end through the handle API with pinned host buffers
+    e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev) if not args.no_extras else None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_reference_run(steps=1, warmup=0, sample_nv=1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "face-states/s", "n_gpus": ws, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "FP64 WENO5-JS + MP fused, x/y/z sweeps reading v_vf directly "
+                                   "(reshape folded), 200^3 cells x 8 vars, buff_size 6",
+                       "m=n=p": M, "v_size": NV, "buff_size": BUFF, "coefficients": "uniform-grid WENO5-JS",
+                       "field": "seeded smooth-plus-jump", "l2": "inputs (663 MB) and outputs (3.7 GB) exceed "
+                                                                  "the 126 MB L2; no flush",
+                       "parallelism": f"{ws} independent blocks (weak scaling, no collective)"},
+            "roofline": {"bound": "hbm", "kernel": f"sweep_fast_kernel<5,MP,f64> {'xyz'[dk]} sweep",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s",
+                         "alg_bytes_per_launch": ab, "launch_ms": dk_ms,
+                         "traffic": read_traffic()},
+            "per_sweep_ms": [s / K for s in sums],
+            "gpu_launches": 3 * K,
+            "clocks": clk.summary(),
+        }
+        if fp32:
+            line["fp32_bulk"] = fp32
+        if drop:
+            line["drop_in"] = drop
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": "face-states/s", "cores": cpu["cores"],
+                                    "kind": "port", "sample": cpu["sample"]}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def read_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (line 'traffic_bytes_per_launch: <int>'), else None."""
+    p = os.path.join(ROOT, "profiles", "sweep_weno5_mp_fp64_200cubed.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                try:
+                    return int(line.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def measure_fp32_bulk(g, v, cstructs, outs64, stream, K, dev):
+    """FP32-bulk: FP32 sweep fields (reshaped from v_vf) and face states; FP64
+    beta differences and weight normalisation.  Timed on the sweeps; error
+    stated against the FP64 outputs of the same step (max-norm relative)."""
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api
+    sp = int(stream.cuda_stream)
+    rs = [torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float32, device=dev) for d in range(3)]
+    nface = int(np.prod(g.face_shape(0)))
+    o32 = [(torch.empty(nface, dtype=torch.float32, device=dev), torch.empty(nface, dtype=torch.float32, device=dev))
+           for _ in range(3)]
+    for d in range(3):
+        api.reshape(g, d, v, rs[d], stream=sp)
+
+    def step():
+        for d in range(3):
+            api.weno(g, d, ORDER, rs[d], cstructs[d], o32[d][0], o32[d][1], flags=wsb.F_MP, stream=sp)
+
+    for _ in range(3):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    # error vs the FP64 outputs of the folded FP64 step (core faces only)
+    N = g.N[0]
+    errs = []
+    for d in range(3):
+        for a64, a32 in zip(outs64[d], o32[d]):
+            A = a64.view(NV, N, N, N)[:, :, :, 3:N - 3]
+            B = a32.view(NV, N, N, N)[:, :, :, 3:N - 3].double()
+            errs.append(float((A - B).abs().max() / A.abs().max()))
+    fs = 3 * face_states_per_dir()
+    return {"value": fs / (ms * 1e-3), "ms_per_step": ms, "max_rel_err_vs_fp64": max(errs),
+            "data": "smooth-plus-jump (jump on odd variables)",
+            "form": "drop-in (FP32 v_rs_ws, reshaped once outside the timed loop)"}
+
+
+def measure_drop_in(g, v, cstructs, outs, stream, K, dev):
+    """The drop-in form: s_initialize_weno (tiled-transpose reshape into
+    v_rs_ws) then the sweep, per direction."""
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api
+    sp = int(stream.cuda_stream)
+    rs = [torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float64, device=dev) for d in range(3)]
+
+    def step(reshape=True):
+        for d in range(3):
+            if reshape:
+                api.reshape(g, d, v, rs[d], stream=sp)
+            api.weno(g, d, ORDER, rs[d], cstructs[d], outs[d][0], outs[d][1], flags=wsb.F_MP, stream=sp)
+
+    res = {}
+    for reshape in (True, False):
+        for _ in range(3):
+            step(reshape)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(K):
+            step(reshape)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res["with_reshape_ms" if reshape else "sweeps_only_ms"] = e0.elapsed_time(e1) / K
+    fs = 3 * face_states_per_dir()
+    res["value_with_reshape"] = fs / (res["with_reshape_ms"] * 1e-3)
+    res["value_sweeps_only"] = fs / (res["sweeps_only_ms"] * 1e-3)
+    return res
+
+
+def measure_e2e(g, vf_host, coefs, K, dev):
+    """End to end through the C-ABI handle API (what a Fortran caller does):
+    upload v_vf from pinned host memory, x/y/z folded WENO5 + MP, download all
+    six face-state arrays into pinned host memory; wall clock around it."""
+    import ctypes
+
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import _lib as L
+    h = wsb.Harness(g)
+    try:
+        for d in range(3):
+            h.upload_coefficients(d, [np.asarray(c.cpu().numpy()).reshape(s, order="F") for c, s in
+                                      zip(coefs[d], [(g.nc(d), 5, 3), (g.nc(d), 5, 3), (5, g.nc(d)),
+                                                     (5, g.nc(d)), (g.nc(d), 5, 6)])])
+        src = torch.from_numpy(vf_host.ravel(order="F")).pin_memory()
+        nface = int(np.prod(g.face_shape(0)))
+        dst = [torch.empty(nface, dtype=torch.float64).pin_memory() for _ in range(6)]
+        lib = L.lib()
+
+        def step():
+            L.check(lib.weno_sb_upload(h.handle, L.A_V_VF, src.data_ptr()))
+            for d in range(3):
+                L.check(lib.weno_sb_weno(h.handle, d, 5, wsb.F_MP | wsb.F_FOLDED))
+            for d in range(3):
+                L.check(lib.weno_sb_download(h.handle, L.A_VL(d), dst[2 * d].data_ptr()))
+                L.check(lib.weno_sb_download(h.handle, L.A_VR(d), dst[2 * d + 1].data_ptr()))
+
+        step()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            step()
+        dt = (time.perf_counter() - t0) / K
+    finally:
+        h.close()
+    fs = 3 * face_states_per_dir()
+    return {"value": fs / dt, "unit": "face-states/s", "h2d_bytes_per_step": int(vf_host.nbytes),
+            "d2h_bytes_per_step": int(6 * nface * 8), "ms_per_step": dt * 1e3, "steps": K,
+            "path": "weno_sb_upload -> weno_sb_weno x3 (folded, MP) -> weno_sb_download x6, pinned host buffers"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-extras", action="store_true", help="skip FP32/drop-in/e2e side measurements")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,169 @@
+/*
+ * weno_sb.h -- C ABI of the B200 WENO library (libweno_sb.so).
+ *
+ * Drop-in replacement for the device loops of the reference WENO harness
+ * wilfonba/WenoStandalone (inputs/weno_standalone.f90, "f90:" below), which
+ * in turn restate MFC's src/simulation/m_weno.fpp.  Every entry point says
+ * which reference routine it replaces.  All calls return an int status:
+ *   0                      success
+ *   1 .. 999               a cudaError_t from the CUDA runtime
+ *   WENO_SB_ERR_* (>=1000) an argument or library error
+ * weno_sb_last_error_string() describes the last failure of this thread.
+ *
+ * Array layouts are the reference's Fortran allocations (column-major,
+ * first index fastest, variable index slowest), passed as base addresses
+ * (c_loc of the first element):
+ *   v_vf        (N1+6, N2+6, N3+6, V)      f90:163-165  cell field, 3 pad cells
+ *   v_rs_ws_d   (Ns+6, C1, C2, V)          f90:167-169  sweep-ordered field
+ *   vL_d, vR_d  (Ns,   C1, C2, V)          f90:1779-1784 face states
+ *   polyL/R_d   (NC, 5, 3)                 f90:171-176
+ *   dL/R_d      (5, NC)                    f90:178-183
+ *   beta_coef_d (NC, 5, 6)                 f90:185-187
+ * with Nd = cells_d + 2*buff_size, NC = Ns - 6 core faces, and per
+ * direction (Ns, C1, C2) = x: (N1,N2,N3), y: (N2,N1,N3), z: (N3,N2,N1).
+ * For m=n=p these are exactly the harness's arrays; other block shapes use
+ * the general (Ns, C1, C2) extents above.
+ */
+#ifndef WENO_SB_H
+#define WENO_SB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WENO_SB_VERSION 1
+
+/* ---- status codes (>= 1000; smaller positive values are cudaError_t) ---- */
+#define WENO_SB_OK 0
+#define WENO_SB_ERR_ARG 1001         /* invalid argument / shape             */
+#define WENO_SB_ERR_HANDLE 1002      /* unknown or finalized handle          */
+#define WENO_SB_ERR_UNSUPPORTED 1003 /* valid request this build cannot do   */
+#define WENO_SB_ERR_INJECTED 1004    /* failure injected via WENO_SB_FAULT   */
+#define WENO_SB_ERR_TIMEOUT 1005     /* a bounded device wait gave up        */
+#define WENO_SB_ERR_ALIGN 1006       /* pointer alignment requirement unmet  */
+#define WENO_SB_ERR_HOST 1007        /* host allocation failed               */
+
+/* ---- nonlinear weight families (f90:64-75: wenojs, mapped_weno, wenoz, teno) */
+#define WENO_SB_JS 0     /* wenojs = .true.                                  */
+#define WENO_SB_MAPPED 1 /* mapped_weno (compile-time .false. in the harness) */
+#define WENO_SB_Z 2      /* wenoz       (compile-time .false. in the harness) */
+#define WENO_SB_TENO 3   /* teno: wenojs = .false. with teno = .true.         */
+#define WENO_SB_NONE 4   /* wenojs = .false. with every family disabled: the
+                            shipped harness; alpha stays 0 and outputs NaN   */
+
+/* ---- storage precision of sweep fields and face states ---- */
+#define WENO_SB_FP64 0 /* everything FP64 (the reference)                    */
+#define WENO_SB_FP32 1 /* FP32-bulk: FP32 storage and stencil sums, FP64 beta
+                          differences and weight normalisation               */
+
+/* ---- flags for weno_sb_weno / weno_sb_weno_dev ---- */
+#define WENO_SB_F_SPLIT 1u       /* WENO5_SPLIT_KERNELS=1 (f90:1410-1412)    */
+#define WENO_SB_F_SPECIALIZED 2u /* WENO5_SPECIALIZED_COMBINED=1 (f90:1721)  */
+#define WENO_SB_F_MP 4u          /* fuse s_preserve_monotonicity (f90:1544)  */
+#define WENO_SB_F_FOLDED 8u      /* read v_vf directly: reshape folded into
+                                    the sweep (no v_rs_ws needed)            */
+
+/* ---- array ids for the handle API (the harness's module arrays) ---- */
+#define WENO_SB_A_V_VF 0
+#define WENO_SB_A_RS(d) (1 + (d))     /* v_rs_ws_{x,y,z}                     */
+#define WENO_SB_A_VL(d) (4 + (d))     /* vL_{x,y,z}                          */
+#define WENO_SB_A_VR(d) (7 + (d))     /* vR_{x,y,z}                          */
+#define WENO_SB_A_POLYL(d) (10 + (d)) /* poly_coef_cbL_{x,y,z}               */
+#define WENO_SB_A_POLYR(d) (13 + (d)) /* poly_coef_cbR_{x,y,z}               */
+#define WENO_SB_A_DL(d) (16 + (d))    /* d_cbL_{x,y,z}                       */
+#define WENO_SB_A_DR(d) (19 + (d))    /* d_cbR_{x,y,z}                       */
+#define WENO_SB_A_BETA(d) (22 + (d))  /* beta_coef_{x,y,z}                   */
+#define WENO_SB_A_COUNT 25
+
+/* Grid and scheme parameters: the &grid_params namelist (f90:117-118). */
+typedef struct weno_sb_grid {
+    int32_t m_cells, n_cells, p_cells; /* m, n, p (cells - 1 per axis)        */
+    int32_t v_size;                    /* number of variables                 */
+    int32_t buff_size;                 /* ghost layers per side (>= 3)        */
+    int32_t scheme;                    /* WENO_SB_JS / _MAPPED / _Z / _TENO / _NONE */
+    double weno_eps;                   /* regulariser added to beta           */
+    double teno_CT;                    /* TENO cutoff                         */
+} weno_sb_grid;
+
+/* Device pointers to one direction's coefficients (layouts above). */
+typedef struct weno_sb_coefs {
+    const double *polyL, *polyR, *dL, *dR, *beta_coef;
+} weno_sb_coefs;
+
+/* ===================================================================== */
+/* Library                                                                */
+/* ===================================================================== */
+int weno_sb_version(void);
+const char *weno_sb_last_error_string(void);
+/* Extents helper: (Ns, C1, C2) of direction dir, and NC = Ns - 6. */
+int weno_sb_extents(const weno_sb_grid *g, int dir, int64_t *ns, int64_t *c1, int64_t *c2);
+
+/* ===================================================================== */
+/* Handle API: the harness's module state on one GPU.                     */
+/* ===================================================================== */
+
+/* Allocate device mirrors of every array of f90:163-187 plus vL/vR_{x,y,z}
+ * (f90:1779-1790) and a private stream: replaces s_initialize_data's
+ * `target enter data map(alloc:...)` (f90:194-197, 1790).  `precision` is
+ * WENO_SB_FP64 or WENO_SB_FP32 (v_rs_ws and vL/vR stored as float). */
+int weno_sb_init(const weno_sb_grid *g, int precision, int *handle);
+/* Release everything: replaces s_finalize_data (f90:207-219). */
+int weno_sb_finalize(int handle);
+/* Host <-> device copies of one array, always FP64 on the host side
+ * (converted on the fly for FP32 handles): replace `target update to/from`
+ * (f90:199-203, 1791, 1831).  Synchronous. */
+int weno_sb_upload(int handle, int which, const double *host);
+int weno_sb_download(int handle, int which, double *host);
+/* Device address, element count and storage dtype (WENO_SB_FP64/FP32). */
+int weno_sb_array_info(int handle, int which, void **dev_ptr, int64_t *n_elem, int *dtype);
+/* s_initialize_weno_{x,y,z} (f90:281-330): reshape v_vf into v_rs_ws_dir. */
+int weno_sb_initialize_weno(int handle, int dir);
+/* s_weno: order 1 = s_order1_copy_dir (f90:332-390); 3 = s_weno3_kernel
+ * (f90:392-475); 5 = s_weno5_kernel_dispatch / s_weno5_kernel_dir
+ * (f90:477-1417); 7 = s_weno7_kernel (f90:1419-1542).  flags: WENO_SB_F_*. */
+int weno_sb_weno(int handle, int dir, int order, unsigned flags);
+/* s_preserve_monotonicity (f90:1544-1615) on vL/vR_dir, in place. */
+int weno_sb_preserve_monotonicity(int handle, int dir);
+/* f_checksum (f90:1617-1620): sum(|a|) of one array, computed on the GPU. */
+int weno_sb_checksum(int handle, int which, double *result);
+/* Wait for all work queued on the handle's stream. */
+int weno_sb_sync(int handle);
+/* The handle's cudaStream_t (as void*), for callers that order their own
+ * work after the library's. */
+int weno_sb_stream(int handle, void **stream);
+
+/* ===================================================================== */
+/* Device-pointer API: MFC-style calls on caller-owned device arrays.      */
+/* `stream` is a cudaStream_t (NULL = legacy default stream).  FP32-bulk  */
+/* arrays (v_rs_ws, vL, vR) are float when dtype == WENO_SB_FP32; v_vf    */
+/* and the coefficients are always double.                                */
+/* ===================================================================== */
+
+/* s_initialize_weno_dir (f90:281-330). */
+int weno_sb_reshape_dev(const weno_sb_grid *g, int dir, int dtype, const double *v_vf,
+                        void *v_rs_ws, void *stream);
+/* s_order1_copy_dir (f90:332-390). */
+int weno_sb_order1_dev(const weno_sb_grid *g, int dir, int dtype, const double *v_vf,
+                       void *vL, void *vR, void *stream);
+/* Reconstruction, order 3/5/7 (f90:392-1542).  v_in is v_rs_ws_dir, or
+ * v_vf when flags has WENO_SB_F_FOLDED. */
+int weno_sb_weno_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, int dtype,
+                     const void *v_in, const weno_sb_coefs *coefs, void *vL, void *vR,
+                     void *stream);
+/* s_preserve_monotonicity (f90:1544-1615). */
+int weno_sb_preserve_monotonicity_dev(const weno_sb_grid *g, int dir, int dtype,
+                                      const void *v_rs_ws, void *vL, void *vR, void *stream);
+/* f_checksum (f90:1617-1620) of n values on the device.  `scratch` is a
+ * caller-owned device buffer of weno_sb_checksum_scratch_bytes(n) bytes;
+ * the sum is written to the device double *d_result. */
+size_t weno_sb_checksum_scratch_bytes(int64_t n);
+int weno_sb_checksum_dev(int dtype, const void *arr, int64_t n, void *scratch,
+                         double *d_result, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WENO_SB_H */

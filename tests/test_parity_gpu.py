@@ -1,0 +1,259 @@
+"""GPU parity: every kernel family through the C ABI against the CPU oracle.
+
+FP64 bar: max-norm relative error <= 1e-12 per output array (reshape and
+order-1 copy are bit-exact).  The oracle restates the reference harness
+(wilfonba/WenoStandalone inputs/weno_standalone.f90) and is pinned to its
+golden checksums by tests/test_oracle_golden.py.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from gpu_util import from_dev, nan_dev, rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+
+@pytest.fixture(scope="module")
+def wsb():
+    import torch
+    assert torch.cuda.is_available()
+    import wenostandalone_b200 as w
+    w.lib()
+    return w
+
+
+GRIDS = [
+    (23, 23, 23, 3),   # cubic
+    (30, 17, 9, 2),    # non-cubic block
+]
+
+
+def _field(m, n, p, nv, buff=6, seed=3):
+    from wenostandalone_b200 import fields
+    return fields.smooth_jump_field(m, n, p, nv, buff, seed=seed)
+
+
+@pytest.mark.parametrize("dims", GRIDS)
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_reshape_and_order1_exact(wsb, oracle_mod, dims, d):
+    from wenostandalone_b200 import api
+    m, n, p, nv = dims
+    g = wsb.Grid(m, n, p, nv, 6)
+    vf = _field(m, n, p, nv)
+    rs_ref = oracle_mod.reshape(vf, m, n, p, 6, d)
+    L_ref, R_ref = oracle_mod.order1_copy(vf, m, n, p, 6, d)
+    v = to_dev(vf)
+    rs = nan_dev(g.rs_shape(d))
+    api.reshape(g, d, v, rs)
+    L, R = nan_dev(g.face_shape(d)), nan_dev(g.face_shape(d))
+    api.order1_copy(g, d, v, L, R)
+    assert np.array_equal(from_dev(rs, g.rs_shape(d)), rs_ref)
+    assert np.array_equal(from_dev(L, g.face_shape(d)), L_ref)
+    assert np.array_equal(from_dev(R, g.face_shape(d)), R_ref)
+
+
+SCHEMES = [0, 1, 2, 3]  # JS, mapped, Z, TENO
+
+
+def _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel, coef_kind="uniform"):
+    from wenostandalone_b200 import api, fields
+    m, n, p, nv = dims
+    g = wsb.Grid(m, n, p, nv, 6, scheme=scheme)
+    vf = _field(m, n, p, nv)
+    nc = g.nc(d)
+    if coef_kind == "uniform":
+        coefs = fields.uniform_weno_coefficients(order, nc)
+    else:
+        coefs = fields.harness_coefficients(nc, (0.03, 0.05, 0.07)[d])
+    rs = oracle_mod.reshape(vf, m, n, p, 6, d)
+    L_ref, R_ref = oracle_mod.order1_copy(vf, m, n, p, 6, d)
+    oracle_mod.reconstruct(rs, coefs, order, scheme=scheme, vL=L_ref, vR=R_ref)
+    if mp:
+        oracle_mod.preserve_monotonicity(rs, L_ref, R_ref)
+
+    os.environ["WENO_SB_KERNEL"] = kernel
+    try:
+        v = to_dev(vf)
+        L, R = nan_dev(g.face_shape(d)), nan_dev(g.face_shape(d))
+        api.order1_copy(g, d, v, L, R)
+        if folded:
+            src = v
+        else:
+            src = nan_dev(g.rs_shape(d))
+            api.reshape(g, d, v, src)
+        flags = (wsb.F_FOLDED if folded else 0) | (wsb.F_MP if mp else 0)
+        api.weno(g, d, order, src, tuple(to_dev(c) for c in coefs), L, R, flags=flags)
+        Lg, Rg = from_dev(L, g.face_shape(d)), from_dev(R, g.face_shape(d))
+    finally:
+        os.environ.pop("WENO_SB_KERNEL", None)
+    return Lg, Rg, L_ref, R_ref
+
+
+def _flip_fraction(got, ref, tol):
+    den = max(np.nanmax(np.abs(ref)), 1e-300)
+    bad = np.abs(got - ref) / den > tol
+    return float(bad.mean())
+
+
+@pytest.mark.parametrize("kernel", ["auto", "generic"])
+@pytest.mark.parametrize("mp", [False, True])
+@pytest.mark.parametrize("folded", [False, True])
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("order", [3, 5, 7])
+def test_reconstruction_parity(wsb, oracle_mod, order, scheme, folded, mp, kernel):
+    for dims in GRIDS:
+        for d in range(3):
+            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel)
+            if scheme == 3:
+                # TENO's cutoff (omega < CT) may flip on borderline values when
+                # pow() rounds differently; count flips instead of failing on one.
+                for got, ref in ((Lg, Lr), (Rg, Rr)):
+                    assert np.array_equal(np.isnan(got), np.isnan(ref))
+                    assert _flip_fraction(np.nan_to_num(got), np.nan_to_num(ref), TOL64) <= 1e-4
+            else:
+                eL, eR = rel_err(Lg, Lr), rel_err(Rg, Rr)
+                assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_harness_coefficients_weno5(wsb, oracle_mod, d):
+    """The harness's synthetic coefficients (non-summing d, beta_coef(:,:,1)=0)."""
+    for dims in GRIDS:
+        Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, 5, 0, False, False, "auto", "harness")
+        assert rel_err(Lg, Lr) <= TOL64 and rel_err(Rg, Rr) <= TOL64
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_standalone_mp_parity(wsb, oracle_mod, d):
+    from wenostandalone_b200 import api, fields
+    m, n, p, nv = GRIDS[1]
+    g = wsb.Grid(m, n, p, nv, 6)
+    vf = _field(m, n, p, nv)
+    rs = oracle_mod.reshape(vf, m, n, p, 6, d)
+    coefs = fields.uniform_weno_coefficients(7, g.nc(d))
+    Lr, Rr = oracle_mod.reconstruct(rs, coefs, 7)
+    Lg_in, Rg_in = to_dev(Lr), to_dev(Rr)
+    oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+    api.preserve_monotonicity(g, d, to_dev(rs), Lg_in, Rg_in)
+    # the limiter rounds exactly like the reference: bit-identical
+    assert np.array_equal(from_dev(Lg_in, g.face_shape(d)), Lr)
+    assert np.array_equal(from_dev(Rg_in, g.face_shape(d)), Rr)
+
+
+def test_minimum_sizes(wsb, oracle_mod):
+    """Smallest blocks: one cell per axis, buff_size 3 (Ns = 7, one core face), v_size 1."""
+    from wenostandalone_b200 import api, fields
+    for (m, n, p, buff) in ((0, 0, 0, 3), (1, 0, 2, 3), (0, 0, 0, 6)):
+        g = wsb.Grid(m, n, p, 1, buff)
+        vf = fields.smooth_jump_field(m, n, p, 1, buff, seed=5)
+        for d in range(3):
+            coefs = fields.uniform_weno_coefficients(5, g.nc(d))
+            rs = oracle_mod.reshape(vf, m, n, p, buff, d)
+            Lr, Rr = oracle_mod.order1_copy(vf, m, n, p, buff, d)
+            oracle_mod.reconstruct(rs, coefs, 5, vL=Lr, vR=Rr)
+            oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+            for folded in (False, True):
+                v = to_dev(vf)
+                L, R = nan_dev(g.face_shape(d)), nan_dev(g.face_shape(d))
+                api.order1_copy(g, d, v, L, R)
+                src = v
+                if not folded:
+                    src = nan_dev(g.rs_shape(d))
+                    api.reshape(g, d, v, src)
+                api.weno(g, d, 5, src, tuple(to_dev(c) for c in coefs), L, R,
+                         flags=wsb.F_MP | (wsb.F_FOLDED if folded else 0))
+                assert rel_err(from_dev(L, g.face_shape(d)), Lr) <= TOL64
+                assert rel_err(from_dev(R, g.face_shape(d)), Rr) <= TOL64
+
+
+def test_handle_golden_checksums(wsb, oracle_mod):
+    """The reference's golden path through the handle API (200^3 x 8, WENO5-JS,
+    scope=full): Checksum X/Y/Z/T within the reference's rtol 1e-10."""
+    import test_oracle_golden as tg
+    exp = tg.reference_checksums()["weno5_full"]
+    from wenostandalone_b200 import _lib as L
+    g = wsb.Grid(199, 199, 199, 8, 6)
+    with wsb.Harness(g) as h:
+        h.fill_harness_data()
+        for d in range(3):
+            h.s_initialize_weno(d)
+        for d in range(3):
+            h.s_order1_copy(d)
+        for d in range(3):
+            h.s_weno5_kernel_dispatch(d)
+        sums = [h.checksum(L.A_VL(d)) + h.checksum(L.A_VR(d)) for d in range(3)]
+    sums.append(sum(sums))
+    for lab, val in zip("XYZT", sums):
+        assert abs(val - exp[lab]) / exp[lab] <= 1e-10, (lab, val, exp[lab])
+
+
+def test_handle_all_mode_matches_oracle(wsb, oracle_mod):
+    """'all' mode (f90:1651-1682: reshape, copy, WENO3, WENO5, WENO7, MP) at 48^3 x 4."""
+    from wenostandalone_b200 import _lib as L
+    m = 47
+    g = wsb.Grid(m, m, m, 4, 6)
+    exp = oracle_mod.harness_run(m, m, m, 4, 6, all_mode=True)
+    with wsb.Harness(g) as h:
+        h.fill_harness_data(oracle_mod.fill_input_field(m, m, m, 4, 6))
+        for d in range(3):
+            h.s_initialize_weno(d)
+            h.s_order1_copy(d)
+            h.s_weno3_kernel(d)
+            h.s_weno5_kernel_dispatch(d)
+            h.s_weno7_kernel(d)
+            h.s_preserve_monotonicity(d)
+        sums = [h.checksum(L.A_VL(d)) + h.checksum(L.A_VR(d)) for d in range(3)]
+    for a, e in zip(sums, exp):
+        assert abs(a - e) / e <= 1e-12
+
+
+def test_full_size_weno5_mp(wsb, oracle_mod):
+    """200^3 x 8, seeded smooth-plus-jump field, WENO5-JS + MP, every direction,
+    drop-in and folded forms, against the oracle at 1e-12 per array."""
+    import torch
+    from wenostandalone_b200 import api, fields
+    m = 199
+    g = wsb.Grid(m, m, m, 8, 6)
+    vf = fields.smooth_jump_field(m, m, m, 8, 6, seed=0)
+    v = to_dev(vf)
+    for d in range(3):
+        coefs = fields.uniform_weno_coefficients(5, g.nc(d))
+        rs = oracle_mod.reshape(vf, m, m, m, 6, d)
+        Lr, Rr = oracle_mod.order1_copy(vf, m, m, m, 6, d)
+        oracle_mod.reconstruct(rs, coefs, 5, vL=Lr, vR=Rr)
+        oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+        dc = tuple(to_dev(c) for c in coefs)
+        for folded in (False, True):
+            L, R = nan_dev(g.face_shape(d)), nan_dev(g.face_shape(d))
+            api.order1_copy(g, d, v, L, R)
+            src = v
+            if not folded:
+                src = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float64, device="cuda")
+                api.reshape(g, d, v, src)
+            api.weno(g, d, 5, src, dc, L, R, flags=wsb.F_MP | (wsb.F_FOLDED if folded else 0))
+            eL = rel_err(from_dev(L, g.face_shape(d)), Lr)
+            eR = rel_err(from_dev(R, g.face_shape(d)), Rr)
+            assert eL <= TOL64 and eR <= TOL64, (d, folded, eL, eR)
+            del L, R
+        torch.cuda.empty_cache()
+
+
+def test_argument_errors(wsb):
+    import ctypes
+    import torch
+    from wenostandalone_b200 import _lib as L, api
+    g = wsb.Grid(7, 7, 7, 1, 6)
+    t = torch.zeros(10, dtype=torch.float64, device="cuda")
+    with pytest.raises(L.WenoError) as e:
+        api.weno(g, 3, 5, t, (t, t, t, t, t), t, t)
+    assert e.value.code == L.ERR_ARG
+    with pytest.raises(L.WenoError) as e:
+        api.weno(g, 0, 4, t, (t, t, t, t, t), t, t)
+    assert e.value.code == L.ERR_ARG
+    bad = L.WenoGrid(7, 7, 7, 1, 2, 0, 1e-16, 1e-5)
+    rc = L.lib().weno_sb_reshape_dev(ctypes.byref(bad), 0, 0, t.data_ptr(), t.data_ptr(), None)
+    assert rc == L.ERR_ARG and "buff_size" in L.last_error()

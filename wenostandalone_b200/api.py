@@ -1,0 +1,235 @@
+"""Host-side mirror of the reference harness interface over the C ABI.
+
+`Grid` is the &grid_params namelist (wilfonba/WenoStandalone
+inputs/weno_standalone.f90:117-118).  `Harness` owns the harness's module
+arrays on the GPU (f90:87-100) and exposes its routines under their
+reference names: s_initialize_weno_{x,y,z} (f90:281-330),
+s_order1_copy_{x,y,z} (f90:332-390), s_weno3_kernel (f90:392-475),
+s_weno5_kernel_dispatch / s_weno5_kernel_{x,y,z} (f90:477-1417),
+s_weno7_kernel (f90:1419-1542), s_preserve_monotonicity (f90:1544-1615) and
+f_checksum (f90:1617-1620).  The module-level functions are the
+device-pointer calls (arrays as 1-D CUDA tensors in Fortran element order).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+
+
+@dataclass
+class Grid:
+    m_cells: int = 199
+    n_cells: int = 199
+    p_cells: int = 199
+    v_size: int = 8
+    buff_size: int = 6
+    scheme: int = L.JS
+    weno_eps: float = 1e-16
+    teno_CT: float = 1e-5
+
+    @classmethod
+    def from_namelist(cls, m=199, n=199, p=199, v_size=8, buff_size=6, weno_eps=1e-16,
+                      wenojs=True, teno_CT=1e-5, teno_enabled=True):
+        """The namelist's `wenojs` logical: JS when true; when false the
+        harness falls through to TENO (if its compile-time `teno` is on,
+        f90:74) or to no weight family at all (alpha = 0, NaN output)."""
+        scheme = L.JS if wenojs else (L.TENO if teno_enabled else L.NONE)
+        return cls(m, n, p, v_size, buff_size, scheme, weno_eps, teno_CT)
+
+    def c(self) -> L.WenoGrid:
+        return L.WenoGrid(self.m_cells, self.n_cells, self.p_cells, self.v_size, self.buff_size,
+                          self.scheme, self.weno_eps, self.teno_CT)
+
+    @property
+    def N(self):
+        b = self.buff_size
+        return (self.m_cells + 2 * b + 1, self.n_cells + 2 * b + 1, self.p_cells + 2 * b + 1)
+
+    def extents(self, d: int):
+        N1, N2, N3 = self.N
+        return {0: (N1, N2, N3), 1: (N2, N1, N3), 2: (N3, N2, N1)}[d]
+
+    def vf_shape(self):
+        return tuple(n + 6 for n in self.N) + (self.v_size,)
+
+    def rs_shape(self, d):
+        ns, c1, c2 = self.extents(d)
+        return (ns + 6, c1, c2, self.v_size)
+
+    def face_shape(self, d):
+        ns, c1, c2 = self.extents(d)
+        return (ns, c1, c2, self.v_size)
+
+    def nc(self, d):
+        return self.extents(d)[0] - 6
+
+    def face_states(self, d, order=5):
+        """Reconstructed scalars one sweep writes (vL and vR)."""
+        ns, c1, c2 = self.extents(d)
+        nf = ns if order == 3 else ns - 6
+        return 2 * nf * c1 * c2 * self.v_size
+
+
+_OFFSETS = (0.03, 0.05, 0.07)  # f90:190-192
+
+
+class Harness:
+    """The harness's module state on one GPU (handle API)."""
+
+    def __init__(self, grid: Grid, precision: int = L.FP64):
+        self.grid = grid
+        self.precision = precision
+        h = ctypes.c_int(0)
+        check(lib().weno_sb_init(ctypes.byref(grid.c()), precision, ctypes.byref(h)))
+        self.handle = h.value
+
+    # -- data movement (target update to/from) --
+    def shape_of(self, which: int):
+        g = self.grid
+        if which == L.A_V_VF:
+            return g.vf_shape()
+        k, d = divmod(which - 1, 3)
+        nc = g.nc(d)
+        return [g.rs_shape(d), g.face_shape(d), g.face_shape(d), (nc, 5, 3), (nc, 5, 3),
+                (5, nc), (5, nc), (nc, 5, 6)][k]
+
+    def upload(self, which: int, arr: np.ndarray) -> None:
+        a = np.asfortranarray(arr, dtype=np.float64)
+        assert a.shape == tuple(self.shape_of(which)), (a.shape, self.shape_of(which))
+        check(lib().weno_sb_upload(self.handle, which, a.ctypes.data))
+
+    def download(self, which: int) -> np.ndarray:
+        out = np.empty(self.shape_of(which), order="F")
+        check(lib().weno_sb_download(self.handle, which, out.ctypes.data))
+        return out
+
+    def device_ptr(self, which: int) -> int:
+        p = ctypes.c_void_p()
+        check(lib().weno_sb_array_info(self.handle, which, ctypes.byref(p), None, None))
+        return p.value
+
+    def upload_coefficients(self, d: int, coefs) -> None:
+        pL, pR, dL, dR, bc = coefs
+        self.upload(L.A_POLYL(d), pL)
+        self.upload(L.A_POLYR(d), pR)
+        self.upload(L.A_DL(d), dL)
+        self.upload(L.A_DR(d), dR)
+        self.upload(L.A_BETA(d), bc)
+
+    def fill_harness_data(self, field: np.ndarray | None = None) -> None:
+        """s_initialize_data's fill + upload (f90:189-203) with the
+        harness's synthetic field and coefficients."""
+        from . import fields
+        g = self.grid
+        if field is None:
+            field = fields.harness_field(g.m_cells, g.n_cells, g.p_cells, g.v_size, g.buff_size)
+        self.upload(L.A_V_VF, field)
+        for d in range(3):
+            self.upload_coefficients(d, fields.harness_coefficients(g.nc(d), _OFFSETS[d]))
+
+    # -- the reference's routines --
+    def s_initialize_weno(self, d: int) -> None:
+        check(lib().weno_sb_initialize_weno(self.handle, d))
+
+    def s_initialize_weno_x(self): self.s_initialize_weno(0)
+    def s_initialize_weno_y(self): self.s_initialize_weno(1)
+    def s_initialize_weno_z(self): self.s_initialize_weno(2)
+
+    def weno(self, d: int, order: int, flags: int = 0) -> None:
+        check(lib().weno_sb_weno(self.handle, d, order, flags))
+
+    def s_order1_copy(self, d): self.weno(d, 1)
+    def s_weno3_kernel(self, d): self.weno(d, 3)
+    def s_weno5_kernel_dispatch(self, d, split=False):
+        self.weno(d, 5, L.F_SPLIT if split else 0)
+    def s_weno5_kernel_specialized(self, d): self.weno(d, 5, L.F_SPECIALIZED)
+    def s_weno7_kernel(self, d): self.weno(d, 7)
+
+    def s_preserve_monotonicity(self, d: int) -> None:
+        check(lib().weno_sb_preserve_monotonicity(self.handle, d))
+
+    def checksum(self, which: int) -> float:
+        out = ctypes.c_double(0.0)
+        check(lib().weno_sb_checksum(self.handle, which, ctypes.byref(out)))
+        return out.value
+
+    def sync(self) -> None:
+        check(lib().weno_sb_sync(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            check(lib().weno_sb_finalize(self.handle))
+            self.handle = 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib().weno_sb_finalize(self.handle)
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Device-pointer API on CUDA tensors (1-D, Fortran element order)
+# ---------------------------------------------------------------------------
+def _ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        import torch
+        return int(torch.cuda.current_stream().cuda_stream)
+    return int(stream)
+
+
+def _dtype_of(t) -> int:
+    import torch
+    return L.FP32 if t.dtype == torch.float32 else L.FP64
+
+
+def reshape(grid: Grid, d: int, v_vf, out, stream=None) -> None:
+    check(lib().weno_sb_reshape_dev(ctypes.byref(grid.c()), d, _dtype_of(out), _ptr(v_vf), _ptr(out),
+                                    _stream(stream)))
+
+
+def order1_copy(grid: Grid, d: int, v_vf, vL, vR, stream=None) -> None:
+    check(lib().weno_sb_order1_dev(ctypes.byref(grid.c()), d, _dtype_of(vL), _ptr(v_vf), _ptr(vL), _ptr(vR),
+                                   _stream(stream)))
+
+
+def coefs_struct(coefs) -> L.WenoCoefs:
+    pL, pR, dL, dR, bc = coefs
+    return L.WenoCoefs(_ptr(pL), _ptr(pR), _ptr(dL), _ptr(dR), _ptr(bc))
+
+
+def weno(grid: Grid, d: int, order: int, v_in, coefs, vL, vR, flags: int = 0, stream=None) -> None:
+    cs = coefs if isinstance(coefs, L.WenoCoefs) else coefs_struct(coefs)
+    check(lib().weno_sb_weno_dev(ctypes.byref(grid.c()), d, order, flags, _dtype_of(vL), _ptr(v_in),
+                                 ctypes.byref(cs), _ptr(vL), _ptr(vR), _stream(stream)))
+
+
+def preserve_monotonicity(grid: Grid, d: int, v_rs_ws, vL, vR, stream=None) -> None:
+    check(lib().weno_sb_preserve_monotonicity_dev(ctypes.byref(grid.c()), d, _dtype_of(vL), _ptr(v_rs_ws),
+                                                  _ptr(vL), _ptr(vR), _stream(stream)))
+
+
+def checksum(arr, stream=None) -> float:
+    import torch
+    scratch = torch.empty(int(lib().weno_sb_checksum_scratch_bytes(arr.numel())) // 8 + 1,
+                          dtype=torch.float64, device=arr.device)
+    res = torch.empty(1, dtype=torch.float64, device=arr.device)
+    check(lib().weno_sb_checksum_dev(_dtype_of(arr), _ptr(arr), arr.numel(), _ptr(scratch), _ptr(res),
+                                     _stream(stream)))
+    return float(res.item())

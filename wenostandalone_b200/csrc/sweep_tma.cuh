@@ -1,0 +1,299 @@
+// sweep_tma.cuh -- pipelined reconstruction sweep (the hot path).
+//
+// Work decomposition.  A sweep reconstructs vL/vR at `nf` faces along the
+// sweep axis for every cross-section column (a, b, v).  A CTA owns a tile of
+// TJ consecutive faces (one thread per face) and walks over groups of
+// columns.  Each thread loads its face's coefficients (poly, d, beta:
+// indexed by the face only, f90:535-555) into registers once and reuses
+// them for every column, so the coefficient arrays cost nothing per point.
+//
+// Staging.  The stencil window of a column group (TJ + 2H values along the
+// sweep per column, H = stencil half width) is copied global -> shared by a
+// STAGES-deep asynchronous pipeline, so HBM reads stay in flight while the
+// FP64 arithmetic of the previous group runs.  Two tile shapes:
+//   KIND 0  sweep axis contiguous in memory (v_rs_ws in any direction, or
+//           v_vf in x): the tile is R rows of the window, thread f reads
+//           row[f .. f+2H] -- consecutive threads, consecutive words.
+//   KIND 1  sweep axis strided (the folded y/z sweeps read v_vf directly):
+//           the tile is the window x XW consecutive x-columns, row pitch
+//           XW+1 so a warp reading one column at 32 consecutive faces hits
+//           32 distinct banks; the y/z reshape is thereby folded away.
+// Stores go straight from registers to vL/vR, whose face index is the
+// fastest one, so every warp store is one contiguous segment.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "weno_math.cuh"
+#include "sweep_generic.cuh"
+
+namespace wsb {
+
+struct FastArgs {
+    const void* in;
+    void* vL;
+    void* vR;
+    CoefPtrs cp;
+    WenoParams wp;
+    long long ns, nc;
+    int o_first;      // first face handled (0 for WENO3, 3 otherwise)
+    int nf;           // faces handled
+    int TJ;           // faces per tile
+    int n_jt;         // number of face tiles
+    int SW;           // window length along the sweep (TJ + 2H)
+    int pitch;        // KIND 0: smem row pitch (elements); KIND 1: XW + 1
+    int U;            // columns per group (R for KIND 0, XW for KIND 1)
+    // Column groups: U consecutive values of cross axis u, at fixed (w, v).
+    int Nu, Nw, NV, n_ut;
+    long long n_groups;
+    long long sJ;          // input stride along the sweep
+    long long sU, sWw, sV; // input strides of u, w, v
+    long long in_off;      // input offset of (J=0, u=0, w=0, v=0)
+    long long o_sU, o_sW, o_sV;  // output strides of u, w, v
+};
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 8) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int ORDER, bool MPF>
+struct Halo {
+    static constexpr int H0 = (ORDER - 1) / 2;
+    static constexpr int H = (MPF && H0 < 2) ? 2 : H0;
+};
+
+struct GroupInfo {
+    long long in0;   // input offset of (J = 0, first column)
+    long long out0;  // output offset of (face 0, first column)
+    int ucnt;        // valid columns in the group
+};
+
+__device__ __forceinline__ GroupInfo group_info(const FastArgs& a, long long grp) {
+    const unsigned g = (unsigned)grp;
+    const unsigned ut = g % (unsigned)a.n_ut;
+    const unsigned t = g / (unsigned)a.n_ut;
+    const unsigned w = t % (unsigned)a.Nw;
+    const unsigned v = t / (unsigned)a.Nw;
+    const int u0 = (int)ut * a.U;
+    GroupInfo gi;
+    gi.ucnt = min(a.U, a.Nu - u0);
+    gi.in0 = a.in_off + (long long)u0 * a.sU + (long long)w * a.sWw + (long long)v * a.sV;
+    gi.out0 = (long long)u0 * a.o_sU + (long long)w * a.o_sW + (long long)v * a.o_sV;
+    return gi;
+}
+
+template <typename T, int KIND, int XW>
+__device__ __forceinline__ void issue_stage(const FastArgs& a, T* buf, long long grp, int J0, int Jcnt) {
+    const T* __restrict__ in = (const T*)a.in;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const GroupInfo gi = group_info(a, grp);
+    if constexpr (KIND == 0) {
+        for (int r = warp; r < gi.ucnt; r += nw) {
+            const T* src = in + gi.in0 + (long long)r * a.sU + J0;
+            T* dst = buf + r * a.pitch;
+            for (int j = lane; j < Jcnt; j += 32) cp_async_elem(dst + j, src + j);
+        }
+    } else {
+        // rows of XW consecutive u values; 32/XW rows per warp instruction
+        constexpr int RPW = 32 / XW;
+        const int k = lane % XW;
+        if (k < gi.ucnt) {
+            const T* src = in + gi.in0 + k;
+            for (int j = warp * RPW + lane / XW; j < Jcnt; j += nw * RPW)
+                cp_async_elem(buf + j * a.pitch + k, src + (long long)(J0 + j) * a.sJ);
+        }
+    }
+}
+
+template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES>
+__global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(const FastArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    constexpr int H = Halo<ORDER, MPF>::H;
+    const int stage_elems = (KIND == 0) ? a.U * a.pitch : a.SW * a.pitch;
+
+    const int jt = blockIdx.x % a.n_jt;
+    const long long g0 = blockIdx.x / a.n_jt;
+    const long long gstep = gridDim.x / a.n_jt;
+    const int f_first = jt * a.TJ;                 // first face (0-based among the nf handled)
+    const int f_cnt = min(a.TJ, a.nf - f_first);   // faces in this tile
+    const int o_begin = a.o_first + f_first;       // face index o of the tile's first face
+    const int J0 = o_begin + 3 - H;                // first input index of the window
+    const int Jcnt = f_cnt + 2 * H;                // window length (always inside [0, ns+6))
+
+    const int f = threadIdx.x;                     // tile-local face
+    const bool active = f < f_cnt;
+    const long long o = o_begin + f;
+    long long cidx = o - 3;
+    cidx = cidx < 0 ? 0 : (cidx > a.nc - 1 ? a.nc - 1 : cidx);
+    Coef<ORDER> cf;
+    if (active) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
+
+    T* __restrict__ vL = (T*)a.vL;
+    T* __restrict__ vR = (T*)a.vR;
+    const int js = (KIND == 0) ? 1 : a.pitch;     // smem stride along the sweep
+    const int ks = (KIND == 0) ? a.pitch : 1;     // smem stride between columns
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        const long long gg = g0 + s * gstep;
+        if (gg < a.n_groups) issue_stage<T, KIND, XW>(a, smem + s * stage_elems, gg, J0, Jcnt);
+        cp_async_commit();
+    }
+    long long grp = g0;
+    for (int it = 0; grp < a.n_groups; ++it, grp += gstep) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            const long long gg = grp + (long long)(STAGES - 1) * gstep;
+            if (gg < a.n_groups)
+                issue_stage<T, KIND, XW>(a, smem + ((it + STAGES - 1) % STAGES) * stage_elems, gg, J0, Jcnt);
+            cp_async_commit();
+        }
+        if (!active) continue;
+        const GroupInfo gi = group_info(a, grp);
+        const T* buf = smem + (it % STAGES) * stage_elems + (f + H) * js;
+        long long oidx = gi.out0 + o;
+        for (int k = 0; k < gi.ucnt; ++k, oidx += a.o_sU) {
+            const T* base = buf + k * ks;
+            T Lt, Rt;
+            if constexpr (ORDER == 3) {
+                double L, R;
+                weno3_face((double)base[-js], (double)base[0], (double)base[js], cf, a.wp.scheme, a.wp.eps, L, R);
+                Lt = (T)L;
+                Rt = (T)R;
+                if (MPF && o >= 3 && o <= a.ns - 4)
+                    MP<T>::apply(base[-2 * js], base[-js], base[0], base[js], base[2 * js], Lt, Rt);
+            } else if constexpr (ORDER == 5) {
+                const T m2 = base[-2 * js], m1 = base[-js], z0 = base[0], p1 = base[js], p2 = base[2 * js];
+                double L, R;
+                weno5_face<T>((double)m2, (double)m1, (double)z0, (double)p1, (double)p2, cf, a.wp.scheme,
+                              a.wp.eps, a.wp.teno_ct, L, R);
+                Lt = (T)L;
+                Rt = (T)R;
+                if (MPF) MP<T>::apply(m2, m1, z0, p1, p2, Lt, Rt);
+            } else {
+                double s7[7];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) s7[q] = (double)base[(q - 3) * js];
+                double L, R;
+                weno7_face<T>(s7 + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, L, R);
+                Lt = (T)L;
+                Rt = (T)R;
+                if (MPF) MP<T>::apply(base[-2 * js], base[-js], base[0], base[js], base[2 * js], Lt, Rt);
+            }
+            vL[oidx] = Lt;
+            vR[oidx] = Rt;
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// Device error flag for bounded waits (reserved for the TMA loader).
+inline int tma_check_device_error(cudaStream_t) { return 0; }
+
+template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES>
+int launch_fast_t(FastArgs a, cudaStream_t st, int sms) {
+    const int threads = ((a.TJ + 31) / 32) * 32;
+    size_t smem;
+    if (KIND == 0) {
+        a.pitch = a.SW;
+        smem = (size_t)STAGES * a.U * a.pitch * sizeof(T);
+    } else {
+        a.U = XW;
+        a.pitch = XW + 1;
+        smem = (size_t)STAGES * a.SW * a.pitch * sizeof(T);
+    }
+    a.n_ut = (a.Nu + a.U - 1) / a.U;
+    a.n_groups = (long long)a.n_ut * a.Nw * a.NV;
+    auto kfn = sweep_fast_kernel<ORDER, MPF, T, KIND, XW, STAGES>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set = true;
+    }
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, smem);
+    if (occ < 1) occ = 1;
+    long long per_jt = ((long long)sms * occ) / a.n_jt;
+    if (per_jt < 1) per_jt = 1;
+    if (per_jt > a.n_groups) per_jt = a.n_groups;
+    const long long grid = per_jt * a.n_jt;
+    kfn<<<(unsigned)grid, threads, smem, st>>>(a);
+    return 0;
+}
+
+// Returns WENO_SB_ERR_UNSUPPORTED (1003) when the layout does not fit this
+// kernel, so the caller can fall back to the general-stride one.
+template <typename T>
+int launch_tma_sweep(const long long E[3], const SweepGeom& g, int dir, bool folded, int order, bool mp,
+                     const T* in, T* vL, T* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st) {
+    (void)E;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    if (g.c1 > (1LL << 30) || g.c2 > (1LL << 30) || g.cols > (1LL << 31)) return 1003;
+    FastArgs a{};
+    a.in = in;
+    a.vL = vL;
+    a.vR = vR;
+    a.cp = cp;
+    a.wp = wp;
+    a.ns = g.ns;
+    a.nc = g.nc;
+    a.o_first = (order == 3) ? 0 : 3;
+    a.nf = (int)((order == 3) ? g.ns : g.nc);
+    const int Hh = ((order - 1) / 2 < 2 && mp) ? 2 : (order - 1) / 2;
+    const int maxTJ = 224;
+    a.n_jt = (a.nf + maxTJ - 1) / maxTJ;
+    a.TJ = (a.nf + a.n_jt - 1) / a.n_jt;
+    a.SW = a.TJ + 2 * Hh;
+    a.sJ = g.sJ;
+    a.sV = g.sV;
+    a.in_off = g.in_off;
+    a.o_sV = g.ns * g.c1 * g.c2;
+    const bool kind1 = folded && dir != 0;
+    if (!kind1 || dir == 1) {
+        // u = a (first cross axis), w = b
+        a.Nu = (int)g.c1; a.Nw = (int)g.c2; a.sU = g.sA; a.sWw = g.sB;
+        a.o_sU = g.ns; a.o_sW = g.ns * g.c1;
+    } else {
+        // folded z: u = b (x, unit stride), w = a (y)
+        a.Nu = (int)g.c2; a.Nw = (int)g.c1; a.sU = g.sB; a.sWw = g.sA;
+        a.o_sU = g.ns * g.c1; a.o_sW = g.ns;
+    }
+    a.U = 8;
+    a.NV = (int)g.nv;
+    constexpr int S0 = 4, S1 = 3;
+    const int key = order * 4 + (mp ? 2 : 0) + (kind1 ? 1 : 0);
+    switch (key) {
+        case 12: return launch_fast_t<3, false, T, 0, 16, S0>(a, st, sms);
+        case 13: return launch_fast_t<3, false, T, 1, 16, S1>(a, st, sms);
+        case 14: return launch_fast_t<3, true, T, 0, 16, S0>(a, st, sms);
+        case 15: return launch_fast_t<3, true, T, 1, 16, S1>(a, st, sms);
+        case 20: return launch_fast_t<5, false, T, 0, 16, S0>(a, st, sms);
+        case 21: return launch_fast_t<5, false, T, 1, 16, S1>(a, st, sms);
+        case 22: return launch_fast_t<5, true, T, 0, 16, S0>(a, st, sms);
+        case 23: return launch_fast_t<5, true, T, 1, 16, S1>(a, st, sms);
+        case 28: return launch_fast_t<7, false, T, 0, 16, S0>(a, st, sms);
+        case 29: return launch_fast_t<7, false, T, 1, 16, S1>(a, st, sms);
+        case 30: return launch_fast_t<7, true, T, 0, 16, S0>(a, st, sms);
+        case 31: return launch_fast_t<7, true, T, 1, 16, S1>(a, st, sms);
+        default: return 1003;
+    }
+}
+
+}  // namespace wsb

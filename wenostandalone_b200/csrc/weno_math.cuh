@@ -1,0 +1,489 @@
+// weno_math.cuh -- per-face arithmetic of the WENO path, FP64 and FP32-bulk.
+//
+// Restates the per-point bodies of the reference harness
+// (wilfonba/WenoStandalone inputs/weno_standalone.f90, "f90:"):
+//   WENO3  f90:416-468     WENO5  f90:511-662     WENO7  f90:1448-1535
+//   MP     f90:1564-1608
+//
+// Two forms of the nonlinear weights:
+//  * "faithful": the reference's sequence (alpha_k = d_k/beta_k^2, then
+//    omega_k = alpha_k/sum) for every weight family, used for
+//    mapped / Z / TENO / none;
+//  * "one-division JS": omega_k = d_k P_k / sum_m d_m P_m with
+//    P_k = prod_{m != k} beta_m^2, which is the same rational function
+//    multiplied through by prod beta_m^2.  One division per side instead of
+//    2N, the P_k are shared by the left and right states.  It rounds
+//    differently (a few ulp) and is exact in real arithmetic; when the
+//    products leave the normal range (beta > ~1e77 or eps < ~1e-77) the
+//    faithful form is used instead.
+//
+// The MP limiter is written with explicit _rn intrinsics so that no FMA is
+// contracted: its min/max decisions depend on the signs of second
+// differences, and must round exactly as the reference does.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wsb {
+
+enum Scheme { JS = 0, MAPPED = 1, WZ = 2, TENO = 3, NONE = 4 };
+
+// ---------------------------------------------------------------------
+// Coefficient register blocks for one core face (index c).
+// Layouts: poly(c,r,s) = p[c + nc*(r + 5*s)], d(r,c) = d[r + 5*c],
+//          beta(c,r,s) = b[c + nc*(r + 5*s)].
+// ---------------------------------------------------------------------
+template <int ORDER>
+struct Coef;
+
+template <>
+struct Coef<3> {
+    double pL[2], pR[2], dL[2], dR[2], b[2];
+    __device__ __forceinline__ void load(const double* __restrict__ polyL,
+                                         const double* __restrict__ polyR,
+                                         const double* __restrict__ d_L,
+                                         const double* __restrict__ d_R,
+                                         const double* __restrict__ beta, long long nc, long long c) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            pL[r] = __ldg(polyL + c + nc * r);
+            pR[r] = __ldg(polyR + c + nc * r);
+            dL[r] = __ldg(d_L + r + 5 * c);
+            dR[r] = __ldg(d_R + r + 5 * c);
+            b[r] = __ldg(beta + c + nc * r);
+        }
+    }
+};
+
+template <>
+struct Coef<5> {
+    double pL[6], pR[6], dL[3], dR[3], b[9];
+    __device__ __forceinline__ void load(const double* __restrict__ polyL,
+                                         const double* __restrict__ polyR,
+                                         const double* __restrict__ d_L,
+                                         const double* __restrict__ d_R,
+                                         const double* __restrict__ beta, long long nc, long long c) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                pL[2 * r + s] = __ldg(polyL + c + nc * (r + 5 * s));
+                pR[2 * r + s] = __ldg(polyR + c + nc * (r + 5 * s));
+            }
+#pragma unroll
+            for (int s = 0; s < 3; ++s) b[3 * r + s] = __ldg(beta + c + nc * (r + 5 * s));
+            dL[r] = __ldg(d_L + r + 5 * c);
+            dR[r] = __ldg(d_R + r + 5 * c);
+        }
+    }
+};
+
+template <>
+struct Coef<7> {
+    double pL[12], pR[12], dL[4], dR[4], b[24];
+    __device__ __forceinline__ void load(const double* __restrict__ polyL,
+                                         const double* __restrict__ polyR,
+                                         const double* __restrict__ d_L,
+                                         const double* __restrict__ d_R,
+                                         const double* __restrict__ beta, long long nc, long long c) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+                pL[3 * r + s] = __ldg(polyL + c + nc * (r + 5 * s));
+                pR[3 * r + s] = __ldg(polyR + c + nc * (r + 5 * s));
+            }
+#pragma unroll
+            for (int s = 0; s < 6; ++s) b[6 * r + s] = __ldg(beta + c + nc * (r + 5 * s));
+            dL[r] = __ldg(d_L + r + 5 * c);
+            dR[r] = __ldg(d_R + r + 5 * c);
+        }
+    }
+};
+
+__device__ __forceinline__ bool normal_pos(double s) { return s > 1e-300 && s < 1e300; }
+
+// Mapped-WENO transform (f90:419-423, 557-568).
+__device__ __forceinline__ double mapw(double d, double w) {
+    return (d * (1.0 + d - 3.0 * w) + w * w) * (w / (d * d + w * (1.0 - 2.0 * d)));
+}
+
+// ---------------------------------------------------------------------
+// WENO3 (f90:416-468).  v[-1..1] as doubles.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ void weno3_face(const double vm1, const double v0, const double vp1,
+                                           const Coef<3>& c, int scheme, double eps, double& oL,
+                                           double& oR) {
+    const double dvd0 = vp1 - v0;
+    const double dvdm1 = v0 - vm1;
+    const double beta0 = c.b[0] * dvd0 * dvd0 + eps;
+    const double beta1 = c.b[1] * dvdm1 * dvdm1 + eps;
+    const double pL0 = v0 + c.pL[0] * dvd0, pL1 = v0 + c.pL[1] * dvdm1;
+    const double pR0 = v0 + c.pR[0] * dvd0, pR1 = v0 + c.pR[1] * dvdm1;
+    if (scheme == JS) {
+        const double P0 = beta1 * beta1, P1 = beta0 * beta0;
+        const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1;
+        const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1;
+        const double SL = aL0 + aL1, SR = aR0 + aR1;
+        if (normal_pos(SL) && normal_pos(SR)) {
+            oL = (aL0 * pL0 + aL1 * pL1) / SL;
+            oR = (aR0 * pR0 + aR1 * pR1) / SR;
+            return;
+        }
+    }
+    double a0 = 0.0, a1 = 0.0, tau = 0.0, s, w0, w1;
+    if (scheme == JS) {
+        a0 = c.dL[0] / (beta0 * beta0);
+        a1 = c.dL[1] / (beta1 * beta1);
+    } else if (scheme == MAPPED) {
+        a0 = c.dL[0] / (beta0 * beta0);
+        a1 = c.dL[1] / (beta1 * beta1);
+        s = a0 + a1;
+        a0 = mapw(c.dL[0], a0 / s);
+        a1 = mapw(c.dL[1], a1 / s);
+    } else if (scheme == WZ) {
+        tau = fabs(beta1 - beta0);
+        a0 = c.dL[0] * (1.0 + tau / beta0);
+        a1 = c.dL[1] * (1.0 + tau / beta1);
+    }
+    s = a0 + a1;
+    w0 = a0 / s;
+    w1 = a1 / s;
+    oL = w0 * pL0 + w1 * pL1;
+    if (scheme == JS) {
+        a0 = c.dR[0] / (beta0 * beta0);
+        a1 = c.dR[1] / (beta1 * beta1);
+    } else if (scheme == MAPPED) {
+        a0 = c.dR[0] / (beta0 * beta0);
+        a1 = c.dR[1] / (beta1 * beta1);
+        s = a0 + a1;
+        a0 = mapw(c.dR[0], a0 / s);
+        a1 = mapw(c.dR[1], a1 / s);
+    } else if (scheme == WZ) {
+        a0 = c.dR[0] * (1.0 + tau / beta0);
+        a1 = c.dR[1] * (1.0 + tau / beta1);
+    } else {
+        a0 = 0.0;
+        a1 = 0.0;
+    }
+    s = a0 + a1;
+    w0 = a0 / s;
+    w1 = a1 / s;
+    oR = w0 * pR0 + w1 * pR1;
+}
+
+// ---------------------------------------------------------------------
+// WENO5 (f90:511-662).  Differences and beta in FP64; PT is the type of the
+// candidate polynomials (double, or float for FP32-bulk).
+// ---------------------------------------------------------------------
+template <typename PT>
+__device__ __forceinline__ void weno5_face(const double vm2, const double vm1, const double v0,
+                                           const double vp1, const double vp2, const Coef<5>& c,
+                                           int scheme, double eps, double teno_ct, double& oL,
+                                           double& oR) {
+    const double dvd_p1 = vp2 - vp1;
+    const double dvd_0 = vp1 - v0;
+    const double dvd_m1 = v0 - vm1;
+    const double dvd_m2 = vm1 - vm2;
+    const double beta0 = c.b[0] * dvd_p1 * dvd_p1 + c.b[1] * dvd_p1 * dvd_0 + c.b[2] * dvd_0 * dvd_0 + eps;
+    const double beta1 = c.b[3] * dvd_0 * dvd_0 + c.b[4] * dvd_0 * dvd_m1 + c.b[5] * dvd_m1 * dvd_m1 + eps;
+    const double beta2 = c.b[6] * dvd_m1 * dvd_m1 + c.b[7] * dvd_m1 * dvd_m2 + c.b[8] * dvd_m2 * dvd_m2 + eps;
+
+    const PT v0p = (PT)v0, fp1 = (PT)dvd_p1, f0 = (PT)dvd_0, fm1 = (PT)dvd_m1, fm2 = (PT)dvd_m2;
+    const double pL0 = (double)(v0p + (PT)c.pL[0] * fp1 + (PT)c.pL[1] * f0);
+    const double pL1 = (double)(v0p + (PT)c.pL[2] * f0 + (PT)c.pL[3] * fm1);
+    const double pL2 = (double)(v0p + (PT)c.pL[4] * fm1 + (PT)c.pL[5] * fm2);
+    const double pR0 = (double)(v0p + (PT)c.pR[0] * fp1 + (PT)c.pR[1] * f0);
+    const double pR1 = (double)(v0p + (PT)c.pR[2] * f0 + (PT)c.pR[3] * fm1);
+    const double pR2 = (double)(v0p + (PT)c.pR[4] * fm1 + (PT)c.pR[5] * fm2);
+
+    if (scheme == JS) {
+        const double q0 = beta0 * beta0, q1 = beta1 * beta1, q2 = beta2 * beta2;
+        const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+        const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2;
+        const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2;
+        const double SL = aL0 + aL1 + aL2, SR = aR0 + aR1 + aR2;
+        if (normal_pos(SL) && normal_pos(SR)) {
+            oL = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) / SL;
+            oR = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) / SR;
+            return;
+        }
+    }
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, s;
+    double de0 = 0.0, de1 = 0.0, de2 = 0.0, tau = 0.0;
+    if (scheme == JS) {
+        a0 = c.dL[0] / (beta0 * beta0);
+        a1 = c.dL[1] / (beta1 * beta1);
+        a2 = c.dL[2] / (beta2 * beta2);
+    } else if (scheme == MAPPED) {
+        a0 = c.dL[0] / (beta0 * beta0);
+        a1 = c.dL[1] / (beta1 * beta1);
+        a2 = c.dL[2] / (beta2 * beta2);
+        s = a0 + a1 + a2;
+        const double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+        a0 = mapw(c.dL[0], w0);
+        a1 = mapw(c.dL[1], w1);
+        a2 = mapw(c.dL[2], w2);
+    } else if (scheme == WZ) {
+        tau = fabs(beta2 - beta0);
+        a0 = c.dL[0] * (1.0 + (tau / beta0));
+        a1 = c.dL[1] * (1.0 + (tau / beta1));
+        a2 = c.dL[2] * (1.0 + (tau / beta2));
+    } else if (scheme == TENO) {
+        tau = fabs(beta2 - beta0);
+        a0 = pow(1.0 + tau / beta0, 6.0);
+        a1 = pow(1.0 + tau / beta1, 6.0);
+        a2 = pow(1.0 + tau / beta2, 6.0);
+        s = a0 + a1 + a2;
+        de0 = (a0 / s < teno_ct) ? 0.0 : 1.0;
+        de1 = (a1 / s < teno_ct) ? 0.0 : 1.0;
+        de2 = (a2 / s < teno_ct) ? 0.0 : 1.0;
+        a0 = de0 * c.dL[0];
+        a1 = de1 * c.dL[1];
+        a2 = de2 * c.dL[2];
+    }
+    s = a0 + a1 + a2;
+    oL = (a0 / s) * pL0 + (a1 / s) * pL1 + (a2 / s) * pL2;
+    if (scheme == JS) {
+        a0 = c.dR[0] / (beta0 * beta0);
+        a1 = c.dR[1] / (beta1 * beta1);
+        a2 = c.dR[2] / (beta2 * beta2);
+    } else if (scheme == MAPPED) {
+        a0 = c.dR[0] / (beta0 * beta0);
+        a1 = c.dR[1] / (beta1 * beta1);
+        a2 = c.dR[2] / (beta2 * beta2);
+        s = a0 + a1 + a2;
+        const double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+        a0 = mapw(c.dR[0], w0);
+        a1 = mapw(c.dR[1], w1);
+        a2 = mapw(c.dR[2], w2);
+    } else if (scheme == WZ) {
+        a0 = c.dR[0] * (1.0 + (tau / beta0));
+        a1 = c.dR[1] * (1.0 + (tau / beta1));
+        a2 = c.dR[2] * (1.0 + (tau / beta2));
+    } else if (scheme == TENO) {
+        a0 = de0 * c.dR[0];
+        a1 = de1 * c.dR[1];
+        a2 = de2 * c.dR[2];
+    } else {
+        a0 = a1 = a2 = 0.0;
+    }
+    s = a0 + a1 + a2;
+    oR = (a0 / s) * pR0 + (a1 / s) * pR1 + (a2 / s) * pR2;
+}
+
+// ---------------------------------------------------------------------
+// WENO7 (f90:1448-1535).  v[-3..3].  The reference's arrays are sized 0:4
+// with beta(4) = eps; its TENO branch keeps alpha(4) = (1+tau/eps)^6 in the
+// final sum (f90:1491-1506), restated here as written.
+// ---------------------------------------------------------------------
+template <typename PT>
+__device__ __forceinline__ void weno7_face(const double* v /* v[-3..3] */, const Coef<7>& c,
+                                           int scheme, double eps, double teno_ct, double& oL,
+                                           double& oR) {
+    double D[6];  // D[k+3] = dvd(k), k = -3..2
+    D[5] = v[3] - v[2];
+    D[4] = v[2] - v[1];
+    D[3] = v[1] - v[0];
+    D[2] = v[0] - v[-1];
+    D[1] = v[-1] - v[-2];
+    D[0] = v[-2] - v[-3];
+    double beta[5];
+    // beta(3 - r) uses dvd(2-r), dvd(1-r), dvd(-r) with coefficient row r.
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const double a = D[5 - r], b = D[4 - r], e = D[3 - r];
+        beta[3 - r] = c.b[6 * r + 0] * a * a + c.b[6 * r + 1] * a * b + c.b[6 * r + 2] * a * e +
+                      c.b[6 * r + 3] * b * b + c.b[6 * r + 4] * b * e + c.b[6 * r + 5] * e * e + eps;
+    }
+    beta[4] = eps;
+    double pL[4], pR[4];
+    const PT v0p = (PT)v[0];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const PT a = (PT)D[5 - r], b = (PT)D[4 - r], e = (PT)D[3 - r];
+        pL[3 - r] = (double)(v0p + (PT)c.pL[3 * r] * a + (PT)c.pL[3 * r + 1] * b + (PT)c.pL[3 * r + 2] * e);
+        pR[3 - r] = (double)(v0p + (PT)c.pR[3 * r] * a + (PT)c.pR[3 * r + 1] * b + (PT)c.pR[3 * r + 2] * e);
+    }
+    if (scheme == JS) {
+        const double q0 = beta[0] * beta[0], q1 = beta[1] * beta[1], q2 = beta[2] * beta[2],
+                     q3 = beta[3] * beta[3];
+        const double q01 = q0 * q1, q23 = q2 * q3;
+        const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
+        const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2, aL3 = c.dL[3] * P3;
+        const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2, aR3 = c.dR[3] * P3;
+        const double SL = aL0 + aL1 + aL2 + aL3, SR = aR0 + aR1 + aR2 + aR3;
+        if (normal_pos(SL) && normal_pos(SR)) {
+            oL = (aL0 * pL[0] + aL1 * pL[1] + aL2 * pL[2] + aL3 * pL[3]) / SL;
+            oR = (aR0 * pR[0] + aR1 * pR[1] + aR2 * pR[2] + aR3 * pR[3]) / SR;
+            return;
+        }
+    }
+    double alpha[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, delta[4] = {0.0, 0.0, 0.0, 0.0};
+    double tau = 0.0, s;
+    if (scheme == JS || scheme == MAPPED) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) alpha[q] = c.dL[q] / (beta[q] * beta[q]);
+        if (scheme == MAPPED) {
+            s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) alpha[q] = mapw(c.dL[q], alpha[q] / s);
+        }
+    } else if (scheme == WZ) {
+        tau = fabs(beta[3] - beta[0]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double t = tau / beta[q];
+            alpha[q] = c.dL[q] * (1.0 + t * t);
+        }
+    } else if (scheme == TENO) {
+        tau = fabs(beta[4] - beta[3]);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double a3 = pow(1.0 + tau / beta[q], 3.0);
+            alpha[q] = a3 * a3;
+        }
+        s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            delta[q] = (alpha[q] / s < teno_ct) ? 0.0 : 1.0;
+            alpha[q] = delta[q] * c.dL[q];
+        }
+    }
+    s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
+    oL = (alpha[0] / s) * pL[0] + (alpha[1] / s) * pL[1] + (alpha[2] / s) * pL[2] + (alpha[3] / s) * pL[3];
+    if (scheme == JS || scheme == MAPPED) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) alpha[q] = c.dR[q] / (beta[q] * beta[q]);
+        if (scheme == MAPPED) {
+            s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) alpha[q] = mapw(c.dR[q], alpha[q] / s);
+        }
+    } else if (scheme == WZ) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double t = tau / beta[q];
+            alpha[q] = c.dR[q] * (1.0 + t * t);
+        }
+    } else if (scheme == TENO) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) alpha[q] = delta[q] * c.dR[q];
+    }
+    s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
+    oR = (alpha[0] / s) * pR[0] + (alpha[1] / s) * pR[1] + (alpha[2] / s) * pR[2] + (alpha[3] / s) * pR[3];
+}
+
+// ---------------------------------------------------------------------
+// MP limiter (f90:1564-1608), rounding exactly as the reference.
+// ---------------------------------------------------------------------
+// 4-argument minmod of (4dl-dr, dl, 4dr-dl, dr) (f90:1568-1571).  The
+// reference's product of SIGN() sums is +-1 when all four arguments share a
+// sign bit and 0 otherwise, so it equals copysign(min|.|, 4dl-dr) or 0.
+__device__ __forceinline__ double mp_minmod(double dl, double dr) {
+    const double A = __dsub_rn(__dmul_rn(4.0, dl), dr);
+    const double B = __dsub_rn(__dmul_rn(4.0, dr), dl);
+    const double mn = fmin(fmin(fmin(fabs(A), fabs(dl)), fabs(B)), fabs(dr));
+    const int hA = __double2hiint(A);
+    const int same = (hA ^ __double2hiint(B)) | (hA ^ __double2hiint(dl)) | (hA ^ __double2hiint(dr));
+    return (same >= 0) ? copysign(mn, A) : 0.0;
+}
+
+// x + (sign(1/2, lo-x) + sign(1/2, hi-x)) * min(|lo-x|, |hi-x|)  (f90:1582-1583)
+__device__ __forceinline__ double mp_clamp(double x, double lo, double hi) {
+    const double a = __dsub_rn(lo, x), b = __dsub_rn(hi, x);
+    const double f = __dadd_rn(copysign(0.5, a), copysign(0.5, b));
+    return __dadd_rn(x, __dmul_rn(f, fmin(fabs(a), fabs(b))));
+}
+
+__device__ __forceinline__ void mp_limit(const double vm2, const double vm1, const double v0,
+                                         const double vp1, const double vp2, double& L, double& R) {
+    const double kBetaMP = 4.0 / 3.0;  // beta_mp (f90:1556)
+    const double dm1 = __dsub_rn(__dadd_rn(v0, vm2), __dmul_rn(2.0, vm1));
+    const double d0 = __dsub_rn(__dadd_rn(vp1, vm1), __dmul_rn(2.0, v0));
+    const double dp1 = __dsub_rn(__dadd_rn(vp2, v0), __dmul_rn(2.0, vp1));
+    const double mA = mp_minmod(dm1, d0);  // d_MD of vL, d_LC of vR
+    const double mB = mp_minmod(d0, dp1);  // d_LC of vL, d_MD of vR
+    {
+        const double dR1 = __dsub_rn(vp1, v0);
+        const double UL = __dsub_rn(v0, __dmul_rn(2.0, dR1));
+        const double MD = __dmul_rn(__dsub_rn(__dadd_rn(v0, vm1), mA), 0.5);
+        const double LC = __dadd_rn(__dsub_rn(v0, __dmul_rn(dR1, 0.5)), __dmul_rn(kBetaMP, mB));
+        const double lo = fmax(fmin(fmin(v0, vm1), MD), fmin(fmin(v0, UL), LC));
+        const double hi = fmin(fmax(fmax(v0, vm1), MD), fmax(fmax(v0, UL), LC));
+        L = mp_clamp(L, lo, hi);
+    }
+    {
+        const double dL1 = __dsub_rn(v0, vm1);
+        const double UL = __dadd_rn(v0, __dmul_rn(2.0, dL1));
+        const double MD = __dmul_rn(__dsub_rn(__dadd_rn(v0, vp1), mB), 0.5);
+        const double LC = __dadd_rn(__dadd_rn(v0, __dmul_rn(dL1, 0.5)), __dmul_rn(kBetaMP, mA));
+        const double lo = fmax(fmin(fmin(v0, vp1), MD), fmin(fmin(v0, UL), LC));
+        const double hi = fmin(fmax(fmax(v0, vp1), MD), fmax(fmax(v0, UL), LC));
+        R = mp_clamp(R, lo, hi);
+    }
+}
+
+// FP32-bulk MP: same formula in FP32 on the FP32 field.
+__device__ __forceinline__ float mp_minmod_f(float dl, float dr) {
+    const float A = __fsub_rn(__fmul_rn(4.0f, dl), dr);
+    const float B = __fsub_rn(__fmul_rn(4.0f, dr), dl);
+    const float mn = fminf(fminf(fminf(fabsf(A), fabsf(dl)), fabsf(B)), fabsf(dr));
+    const int hA = __float_as_int(A);
+    const int same = (hA ^ __float_as_int(B)) | (hA ^ __float_as_int(dl)) | (hA ^ __float_as_int(dr));
+    return (same >= 0) ? copysignf(mn, A) : 0.0f;
+}
+
+__device__ __forceinline__ float mp_clamp_f(float x, float lo, float hi) {
+    const float a = __fsub_rn(lo, x), b = __fsub_rn(hi, x);
+    const float f = __fadd_rn(copysignf(0.5f, a), copysignf(0.5f, b));
+    return __fadd_rn(x, __fmul_rn(f, fminf(fabsf(a), fabsf(b))));
+}
+
+__device__ __forceinline__ void mp_limit_f(const float vm2, const float vm1, const float v0,
+                                           const float vp1, const float vp2, float& L, float& R) {
+    const float kBetaMP = 4.0f / 3.0f;
+    const float dm1 = __fsub_rn(__fadd_rn(v0, vm2), __fmul_rn(2.0f, vm1));
+    const float d0 = __fsub_rn(__fadd_rn(vp1, vm1), __fmul_rn(2.0f, v0));
+    const float dp1 = __fsub_rn(__fadd_rn(vp2, v0), __fmul_rn(2.0f, vp1));
+    const float mA = mp_minmod_f(dm1, d0);
+    const float mB = mp_minmod_f(d0, dp1);
+    {
+        const float dR1 = __fsub_rn(vp1, v0);
+        const float UL = __fsub_rn(v0, __fmul_rn(2.0f, dR1));
+        const float MD = __fmul_rn(__fsub_rn(__fadd_rn(v0, vm1), mA), 0.5f);
+        const float LC = __fadd_rn(__fsub_rn(v0, __fmul_rn(dR1, 0.5f)), __fmul_rn(kBetaMP, mB));
+        const float lo = fmaxf(fminf(fminf(v0, vm1), MD), fminf(fminf(v0, UL), LC));
+        const float hi = fminf(fmaxf(fmaxf(v0, vm1), MD), fmaxf(fmaxf(v0, UL), LC));
+        L = mp_clamp_f(L, lo, hi);
+    }
+    {
+        const float dL1 = __fsub_rn(v0, vm1);
+        const float UL = __fadd_rn(v0, __fmul_rn(2.0f, dL1));
+        const float MD = __fmul_rn(__fsub_rn(__fadd_rn(v0, vp1), mB), 0.5f);
+        const float LC = __fadd_rn(__fadd_rn(v0, __fmul_rn(dL1, 0.5f)), __fmul_rn(kBetaMP, mA));
+        const float lo = fmaxf(fminf(fminf(v0, vp1), MD), fminf(fminf(v0, UL), LC));
+        const float hi = fminf(fmaxf(fmaxf(v0, vp1), MD), fmaxf(fmaxf(v0, UL), LC));
+        R = mp_clamp_f(R, lo, hi);
+    }
+}
+
+template <typename T>
+struct MP;
+template <>
+struct MP<double> {
+    static __device__ __forceinline__ void apply(double vm2, double vm1, double v0, double vp1,
+                                                 double vp2, double& L, double& R) {
+        mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
+    }
+};
+template <>
+struct MP<float> {
+    static __device__ __forceinline__ void apply(float vm2, float vm1, float v0, float vp1,
+                                                 float vp2, float& L, float& R) {
+        mp_limit_f(vm2, vm1, v0, vp1, vp2, L, R);
+    }
+};
+
+}  // namespace wsb

@@ -1,0 +1,593 @@
+// weno_sb.cu -- C ABI of the B200 WENO library (declared in include/weno_sb.h).
+//
+// Host side: argument checks, handle bookkeeping (the harness's module
+// arrays, f90:87-100, as device allocations), launch geometry, and the
+// dispatch from (order, scheme, flags, precision) to kernel instances.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <algorithm>
+#include <vector>
+
+#include "weno_sb.h"
+#include "layout.cuh"
+#include "sweep_generic.cuh"
+#include "sweep_tma.cuh"
+
+using namespace wsb;
+
+// ----------------------------------------------------------------------
+// Errors
+// ----------------------------------------------------------------------
+namespace {
+
+thread_local std::string g_last_error = "no error";
+
+int set_err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int set_err(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return WENO_SB_OK;
+    return set_err((int)e, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define WSB_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t e__ = (call);                        \
+        if (e__ != cudaSuccess) return cuda_err(e__, #call); \
+    } while (0)
+
+// Host-side fault injection for error-path tests: WENO_SB_FAULT is a comma
+// separated list of operation names ("init", "upload", "download",
+// "launch", "sync"); a listed operation fails with WENO_SB_ERR_INJECTED
+// before it touches the GPU.
+bool fault_injected(const char* op) {
+    const char* env = getenv("WENO_SB_FAULT");
+    if (!env || !*env) return false;
+    const size_t n = strlen(op);
+    for (const char* s = env; *s;) {
+        const char* e = strchr(s, ',');
+        const size_t len = e ? (size_t)(e - s) : strlen(s);
+        if (len == n && strncmp(s, op, n) == 0) return true;
+        if (!e) break;
+        s = e + 1;
+    }
+    return false;
+}
+
+#define WSB_FAULT(op)                                                                      \
+    do {                                                                                   \
+        if (fault_injected(op))                                                            \
+            return set_err(WENO_SB_ERR_INJECTED, "injected failure in '%s' (WENO_SB_FAULT)", op); \
+    } while (0)
+
+// ----------------------------------------------------------------------
+// Grid geometry
+// ----------------------------------------------------------------------
+struct Dims {
+    long long N[3];  // Nd = cells + 2*buff
+    long long E[3];  // Nd + 6 (v_vf extents)
+    long long nv;
+};
+
+int check_grid(const weno_sb_grid* g, Dims* d) {
+    if (!g) return set_err(WENO_SB_ERR_ARG, "grid pointer is NULL");
+    if (g->m_cells < 0 || g->n_cells < 0 || g->p_cells < 0)
+        return set_err(WENO_SB_ERR_ARG, "negative cell count (m=%d n=%d p=%d)", g->m_cells,
+                       g->n_cells, g->p_cells);
+    if (g->v_size < 1) return set_err(WENO_SB_ERR_ARG, "v_size must be >= 1 (got %d)", g->v_size);
+    if (g->buff_size < 3)
+        return set_err(WENO_SB_ERR_ARG, "buff_size must be >= 3 (got %d)", g->buff_size);
+    if (g->scheme < WENO_SB_JS || g->scheme > WENO_SB_NONE)
+        return set_err(WENO_SB_ERR_ARG, "unknown scheme %d", g->scheme);
+    const int cells[3] = {g->m_cells, g->n_cells, g->p_cells};
+    for (int k = 0; k < 3; ++k) {
+        d->N[k] = (long long)cells[k] + 2LL * g->buff_size + 1;
+        d->E[k] = d->N[k] + 6;
+    }
+    d->nv = g->v_size;
+    // 32-bit grid limits on cross-section counts are not a concern; keep
+    // element counts within int64.
+    const long long tot = d->E[0] * d->E[1] * d->E[2] * d->nv;
+    if (tot <= 0 || tot > (1LL << 40)) return set_err(WENO_SB_ERR_ARG, "grid too large");
+    return WENO_SB_OK;
+}
+
+void sweep_ext(const Dims& d, int dir, long long* ns, long long* c1, long long* c2) {
+    if (dir == 0) { *ns = d.N[0]; *c1 = d.N[1]; *c2 = d.N[2]; }
+    else if (dir == 1) { *ns = d.N[1]; *c1 = d.N[0]; *c2 = d.N[2]; }
+    else { *ns = d.N[2]; *c1 = d.N[1]; *c2 = d.N[0]; }
+}
+
+int check_dir(int dir) {
+    if (dir < 0 || dir > 2) return set_err(WENO_SB_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z), got %d", dir);
+    return WENO_SB_OK;
+}
+
+int check_dtype(int dt) {
+    if (dt != WENO_SB_FP64 && dt != WENO_SB_FP32)
+        return set_err(WENO_SB_ERR_ARG, "dtype must be WENO_SB_FP64 or WENO_SB_FP32, got %d", dt);
+    return WENO_SB_OK;
+}
+
+// Sweep geometry for the drop-in layout (v_rs_ws) or the folded one (v_vf).
+SweepGeom make_geom(const Dims& d, int dir, bool folded) {
+    SweepGeom g;
+    sweep_ext(d, dir, &g.ns, &g.c1, &g.c2);
+    g.nc = g.ns - 6;
+    g.nv = d.nv;
+    g.cols = g.c1 * g.c2 * g.nv;
+    if (!folded) {
+        g.sJ = 1;
+        g.sA = g.ns + 6;
+        g.sB = (g.ns + 6) * g.c1;
+        g.sV = (g.ns + 6) * g.c1 * g.c2;
+        g.in_off = 0;
+    } else {
+        const long long E1 = d.E[0], E2 = d.E[1], E3 = d.E[2];
+        g.sV = E1 * E2 * E3;
+        if (dir == 0) {        // J=x, a=y, b=z
+            g.sJ = 1; g.sA = E1; g.sB = E1 * E2; g.in_off = 3 * E1 + 3 * E1 * E2;
+        } else if (dir == 1) { // J=y, a=x, b=z
+            g.sJ = E1; g.sA = 1; g.sB = E1 * E2; g.in_off = 3 + 3 * E1 * E2;
+        } else {               // J=z, a=y, b=x
+            g.sJ = E1 * E2; g.sA = E1; g.sB = 1; g.in_off = 3 * E1 + 3;
+        }
+    }
+    return g;
+}
+
+int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+// ----------------------------------------------------------------------
+// Launchers
+// ----------------------------------------------------------------------
+template <typename T>
+int launch_reshape(const Dims& d, int dir, const double* v_vf, T* rs, cudaStream_t st) {
+    long long ns, c1, c2;
+    sweep_ext(d, dir, &ns, &c1, &c2);
+    const long long E1 = d.E[0], E2 = d.E[1], E3 = d.E[2];
+    if (dir == 0) {
+        // rows (l=y, q=z, var): in row at y=l+3, z=q+3
+        RowCopyArgs a{v_vf + 3 * E1 + 3 * E1 * E2, E1, c1, c2, d.nv, E1, E1 * E2, E1 * E2 * E3};
+        const long long rows = c1 * c2 * d.nv;
+        dim3 blk(32, 8);
+        const unsigned grid = (unsigned)std::min<long long>((rows + 7) / 8, 65535LL * 8);
+        row_copy_kernel<T, 1><<<grid, blk, 0, st>>>(a, rs, nullptr);
+    } else {
+        TransposeArgs a;
+        if (dir == 1) {
+            // out(k=y, l=x, q=z, v) = v_vf(x=l+3, y=k, z=q+3): A=k (E2), B=l (N1), P=q (N3)
+            a = TransposeArgs{v_vf + 3 + 3 * E1 * E2, ns + 6, c1, c2, d.nv, E1, E1 * E2, E1 * E2 * E3,
+                              ns + 6, (ns + 6) * c1, (ns + 6) * c1 * c2};
+        } else {
+            // out(k=z, l=y, q=x, v) = v_vf(x=q+3, y=l+3, z=k): A=k (E3), B=q (N1), P=l (N2)
+            a = TransposeArgs{v_vf + 3 + 3 * E1, ns + 6, c2, c1, d.nv, E1 * E2, E1, E1 * E2 * E3,
+                              (ns + 6) * c1, ns + 6, (ns + 6) * c1 * c2};
+        }
+        dim3 blk(32, 8);
+        const long long planes = a.P * a.V;
+        dim3 grid((unsigned)((a.A + 31) / 32), (unsigned)((a.B + 31) / 32),
+                  (unsigned)std::min<long long>(planes, 65535));
+        transpose_kernel<T, 1><<<grid, blk, 0, st>>>(a, rs, nullptr);
+    }
+    return cuda_err(cudaGetLastError(), "reshape launch");
+}
+
+template <typename T>
+int launch_order1(const Dims& d, int dir, const double* v_vf, T* vL, T* vR, cudaStream_t st) {
+    long long ns, c1, c2;
+    sweep_ext(d, dir, &ns, &c1, &c2);
+    const long long E1 = d.E[0], E2 = d.E[1], E3 = d.E[2];
+    const double* base = v_vf + 3 + 3 * E1 + 3 * E1 * E2;
+    if (dir == 0) {
+        RowCopyArgs a{base, ns, c1, c2, d.nv, E1, E1 * E2, E1 * E2 * E3};
+        const long long rows = c1 * c2 * d.nv;
+        dim3 blk(32, 8);
+        const unsigned grid = (unsigned)std::min<long long>((rows + 7) / 8, 65535LL * 8);
+        row_copy_kernel<T, 2><<<grid, blk, 0, st>>>(a, vL, vR);
+    } else {
+        TransposeArgs a;
+        if (dir == 1) {
+            // vL(j=y, k=x, l=z) = v_vf(x=k+3, y=j+3, z=l+3): A=j, B=k, P=l
+            a = TransposeArgs{base, ns, c1, c2, d.nv, E1, E1 * E2, E1 * E2 * E3, ns, ns * c1, ns * c1 * c2};
+        } else {
+            // vL(j=z, k=y, l=x) = v_vf(x=l+3, y=k+3, z=j+3): A=j, B=l, P=k
+            a = TransposeArgs{base, ns, c2, c1, d.nv, E1 * E2, E1, E1 * E2 * E3, ns * c1, ns, ns * c1 * c2};
+        }
+        dim3 blk(32, 8);
+        const long long planes = a.P * a.V;
+        dim3 grid((unsigned)((a.A + 31) / 32), (unsigned)((a.B + 31) / 32),
+                  (unsigned)std::min<long long>(planes, 65535));
+        transpose_kernel<T, 2><<<grid, blk, 0, st>>>(a, vL, vR);
+    }
+    return cuda_err(cudaGetLastError(), "order-1 copy launch");
+}
+
+template <int ORDER, bool MPF, typename T>
+void launch_generic_t(const SweepGeom& g, const T* in, T* vL, T* vR, const CoefPtrs& cp,
+                      const WenoParams& wp, cudaStream_t st) {
+    const long long nf = (ORDER == 3) ? g.ns : g.nc;
+    dim3 blk(128);
+    const long long tiles = (nf + 127) / 128;
+    const long long want = (long long)num_sms() * 16 / tiles + 1;
+    dim3 grid((unsigned)tiles, (unsigned)std::min<long long>(std::min<long long>(g.cols, want * 8), 65535));
+    sweep_generic_kernel<ORDER, MPF, T><<<grid, blk, 0, st>>>(g, in, vL, vR, cp, wp);
+}
+
+template <typename T>
+int launch_generic(const SweepGeom& g, int order, bool mp, const T* in, T* vL, T* vR,
+                   const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st) {
+    switch (order * 2 + (mp ? 1 : 0)) {
+        case 0: launch_generic_t<0, false, T>(g, in, vL, vR, cp, wp, st); break;
+        case 1: launch_generic_t<0, true, T>(g, in, vL, vR, cp, wp, st); break;
+        case 6: launch_generic_t<3, false, T>(g, in, vL, vR, cp, wp, st); break;
+        case 7: launch_generic_t<3, true, T>(g, in, vL, vR, cp, wp, st); break;
+        case 10: launch_generic_t<5, false, T>(g, in, vL, vR, cp, wp, st); break;
+        case 11: launch_generic_t<5, true, T>(g, in, vL, vR, cp, wp, st); break;
+        case 14: launch_generic_t<7, false, T>(g, in, vL, vR, cp, wp, st); break;
+        case 15: launch_generic_t<7, true, T>(g, in, vL, vR, cp, wp, st); break;
+        default: return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
+    }
+    return cuda_err(cudaGetLastError(), "reconstruction launch");
+}
+
+// Which implementation serves reconstruction sweeps: 0 = automatic (TMA
+// pipeline when the layout allows it), 1 = always the general-stride
+// kernel.  Set through WENO_SB_KERNEL=generic|auto (read per call).
+int kernel_choice() {
+    const char* e = getenv("WENO_SB_KERNEL");
+    if (e && strcmp(e, "generic") == 0) return 1;
+    return 0;
+}
+
+template <typename T>
+int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned flags,
+             const T* in, const weno_sb_coefs* cf, T* vL, T* vR, cudaStream_t st) {
+    const bool folded = (flags & WENO_SB_F_FOLDED) != 0;
+    const bool mp = (flags & WENO_SB_F_MP) != 0;
+    SweepGeom g = make_geom(d, dir, folded);
+    if (g.nc < 1) return set_err(WENO_SB_ERR_ARG, "sweep has no core faces (Ns=%lld)", g.ns);
+    CoefPtrs cp{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
+    WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
+    if (kernel_choice() == 0) {
+        int rc = launch_tma_sweep<T>(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st);
+        if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "tma sweep launch") : rc;
+    }
+    return launch_generic<T>(g, order, mp, in, vL, vR, cp, wp, st);
+}
+
+// ----------------------------------------------------------------------
+// Handles
+// ----------------------------------------------------------------------
+struct Handle {
+    weno_sb_grid grid;
+    Dims dims;
+    int precision = WENO_SB_FP64;
+    cudaStream_t stream = nullptr;
+    void* arr[WENO_SB_A_COUNT] = {};
+    long long n[WENO_SB_A_COUNT] = {};
+    int dtype[WENO_SB_A_COUNT] = {};
+    double* sum_scratch = nullptr;  // kSumBlocks partials + 1 result
+    int device = 0;
+};
+
+std::mutex g_mu;
+std::vector<Handle*> g_handles;
+
+Handle* get_handle(int h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (h < 1 || h > (int)g_handles.size()) return nullptr;
+    return g_handles[h - 1];
+}
+
+void free_handle_arrays(Handle* H) {
+    for (int i = 0; i < WENO_SB_A_COUNT; ++i)
+        if (H->arr[i]) cudaFree(H->arr[i]);
+    if (H->sum_scratch) cudaFree(H->sum_scratch);
+    if (H->stream) cudaStreamDestroy(H->stream);
+}
+
+}  // namespace
+
+// ======================================================================
+// C ABI
+// ======================================================================
+extern "C" {
+
+int weno_sb_version(void) { return WENO_SB_VERSION; }
+
+const char* weno_sb_last_error_string(void) { return g_last_error.c_str(); }
+
+int weno_sb_extents(const weno_sb_grid* g, int dir, int64_t* ns, int64_t* c1, int64_t* c2) {
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc) return rc;
+    if ((rc = check_dir(dir))) return rc;
+    long long a, b, c;
+    sweep_ext(d, dir, &a, &b, &c);
+    if (ns) *ns = a;
+    if (c1) *c1 = b;
+    if (c2) *c2 = c;
+    return WENO_SB_OK;
+}
+
+int weno_sb_init(const weno_sb_grid* g, int precision, int* handle) {
+    WSB_FAULT("init");
+    if (!handle) return set_err(WENO_SB_ERR_ARG, "handle pointer is NULL");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc) return rc;
+    if ((rc = check_dtype(precision))) return rc;
+    Handle* H = new Handle;
+    H->grid = *g;
+    H->dims = d;
+    H->precision = precision;
+    cudaGetDevice(&H->device);
+    const size_t fsz = precision == WENO_SB_FP32 ? sizeof(float) : sizeof(double);
+    auto alloc = [&](int which, long long n, bool field) -> int {
+        H->n[which] = n;
+        H->dtype[which] = field ? precision : WENO_SB_FP64;
+        const size_t bytes = (size_t)n * (field ? fsz : sizeof(double));
+        cudaError_t e = cudaMalloc(&H->arr[which], bytes);
+        if (e != cudaSuccess) return cuda_err(e, "cudaMalloc");
+        e = cudaMemset(H->arr[which], 0, bytes);
+        return cuda_err(e, "cudaMemset");
+    };
+    rc = cuda_err(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!rc) rc = alloc(WENO_SB_A_V_VF, d.E[0] * d.E[1] * d.E[2] * d.nv, false);
+    for (int dir = 0; dir < 3 && !rc; ++dir) {
+        long long ns, c1, c2;
+        sweep_ext(d, dir, &ns, &c1, &c2);
+        const long long nc = ns - 6;
+        if (!rc) rc = alloc(WENO_SB_A_RS(dir), (ns + 6) * c1 * c2 * d.nv, true);
+        if (!rc) rc = alloc(WENO_SB_A_VL(dir), ns * c1 * c2 * d.nv, true);
+        if (!rc) rc = alloc(WENO_SB_A_VR(dir), ns * c1 * c2 * d.nv, true);
+        if (!rc) rc = alloc(WENO_SB_A_POLYL(dir), nc * 15, false);
+        if (!rc) rc = alloc(WENO_SB_A_POLYR(dir), nc * 15, false);
+        if (!rc) rc = alloc(WENO_SB_A_DL(dir), nc * 5, false);
+        if (!rc) rc = alloc(WENO_SB_A_DR(dir), nc * 5, false);
+        if (!rc) rc = alloc(WENO_SB_A_BETA(dir), nc * 30, false);
+    }
+    if (!rc) rc = cuda_err(cudaMalloc((void**)&H->sum_scratch, sizeof(double) * (kSumBlocks + 1)), "cudaMalloc");
+    if (rc) {
+        free_handle_arrays(H);
+        delete H;
+        return rc;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_handles.push_back(H);
+    *handle = (int)g_handles.size();
+    return WENO_SB_OK;
+}
+
+int weno_sb_finalize(int handle) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    cudaStreamSynchronize(H->stream);
+    free_handle_arrays(H);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_handles[handle - 1] = nullptr;
+    }
+    delete H;
+    return WENO_SB_OK;
+}
+
+int weno_sb_array_info(int handle, int which, void** dev_ptr, int64_t* n_elem, int* dtype) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
+    if (dev_ptr) *dev_ptr = H->arr[which];
+    if (n_elem) *n_elem = H->n[which];
+    if (dtype) *dtype = H->dtype[which];
+    return WENO_SB_OK;
+}
+
+int weno_sb_upload(int handle, int which, const double* host) {
+    WSB_FAULT("upload");
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
+    if (!host) return set_err(WENO_SB_ERR_ARG, "host pointer is NULL");
+    const long long n = H->n[which];
+    if (H->dtype[which] == WENO_SB_FP64) {
+        WSB_CUDA(cudaMemcpyAsync(H->arr[which], host, sizeof(double) * n, cudaMemcpyHostToDevice, H->stream));
+    } else {
+        std::vector<float> tmp((size_t)n);
+        for (long long i = 0; i < n; ++i) tmp[i] = (float)host[i];
+        WSB_CUDA(cudaMemcpyAsync(H->arr[which], tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice, H->stream));
+        WSB_CUDA(cudaStreamSynchronize(H->stream));
+    }
+    return cuda_err(cudaStreamSynchronize(H->stream), "upload");
+}
+
+int weno_sb_download(int handle, int which, double* host) {
+    WSB_FAULT("download");
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
+    if (!host) return set_err(WENO_SB_ERR_ARG, "host pointer is NULL");
+    const long long n = H->n[which];
+    if (H->dtype[which] == WENO_SB_FP64) {
+        WSB_CUDA(cudaMemcpyAsync(host, H->arr[which], sizeof(double) * n, cudaMemcpyDeviceToHost, H->stream));
+        return cuda_err(cudaStreamSynchronize(H->stream), "download");
+    }
+    std::vector<float> tmp((size_t)n);
+    WSB_CUDA(cudaMemcpyAsync(tmp.data(), H->arr[which], sizeof(float) * n, cudaMemcpyDeviceToHost, H->stream));
+    WSB_CUDA(cudaStreamSynchronize(H->stream));
+    for (long long i = 0; i < n; ++i) host[i] = (double)tmp[i];
+    return WENO_SB_OK;
+}
+
+int weno_sb_stream(int handle, void** stream) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    if (stream) *stream = (void*)H->stream;
+    return WENO_SB_OK;
+}
+
+int weno_sb_sync(int handle) {
+    WSB_FAULT("sync");
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    int rc = cuda_err(cudaStreamSynchronize(H->stream), "cudaStreamSynchronize");
+    if (rc) return rc;
+    return tma_check_device_error(H->stream);
+}
+
+int weno_sb_reshape_dev(const weno_sb_grid* g, int dir, int dtype, const double* v_vf, void* v_rs_ws,
+                        void* stream) {
+    WSB_FAULT("launch");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc || (rc = check_dir(dir)) || (rc = check_dtype(dtype))) return rc;
+    if (!v_vf || !v_rs_ws) return set_err(WENO_SB_ERR_ARG, "NULL array pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == WENO_SB_FP64) return launch_reshape<double>(d, dir, v_vf, (double*)v_rs_ws, st);
+    return launch_reshape<float>(d, dir, v_vf, (float*)v_rs_ws, st);
+}
+
+int weno_sb_order1_dev(const weno_sb_grid* g, int dir, int dtype, const double* v_vf, void* vL,
+                       void* vR, void* stream) {
+    WSB_FAULT("launch");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc || (rc = check_dir(dir)) || (rc = check_dtype(dtype))) return rc;
+    if (!v_vf || !vL || !vR) return set_err(WENO_SB_ERR_ARG, "NULL array pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == WENO_SB_FP64) return launch_order1<double>(d, dir, v_vf, (double*)vL, (double*)vR, st);
+    return launch_order1<float>(d, dir, v_vf, (float*)vL, (float*)vR, st);
+}
+
+int weno_sb_weno_dev(const weno_sb_grid* g, int dir, int order, unsigned flags, int dtype,
+                     const void* v_in, const weno_sb_coefs* coefs, void* vL, void* vR, void* stream) {
+    WSB_FAULT("launch");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc || (rc = check_dir(dir)) || (rc = check_dtype(dtype))) return rc;
+    if (order != 3 && order != 5 && order != 7)
+        return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 for weno_sb_weno_dev (got %d)", order);
+    if (flags & ~(WENO_SB_F_SPLIT | WENO_SB_F_SPECIALIZED | WENO_SB_F_MP | WENO_SB_F_FOLDED))
+        return set_err(WENO_SB_ERR_ARG, "unknown flag bits 0x%x", flags);
+    if (!v_in || !vL || !vR || !coefs || !coefs->polyL || !coefs->polyR || !coefs->dL || !coefs->dR ||
+        !coefs->beta_coef)
+        return set_err(WENO_SB_ERR_ARG, "NULL array pointer");
+    if ((flags & WENO_SB_F_FOLDED) && dtype != WENO_SB_FP64)
+        return set_err(WENO_SB_ERR_UNSUPPORTED, "the folded form reads the FP64 v_vf; use dtype FP64");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == WENO_SB_FP64)
+        return run_weno<double>(d, g, dir, order, flags, (const double*)v_in, coefs, (double*)vL, (double*)vR, st);
+    return run_weno<float>(d, g, dir, order, flags, (const float*)v_in, coefs, (float*)vL, (float*)vR, st);
+}
+
+int weno_sb_preserve_monotonicity_dev(const weno_sb_grid* g, int dir, int dtype, const void* v_rs_ws,
+                                      void* vL, void* vR, void* stream) {
+    WSB_FAULT("launch");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc || (rc = check_dir(dir)) || (rc = check_dtype(dtype))) return rc;
+    if (!v_rs_ws || !vL || !vR) return set_err(WENO_SB_ERR_ARG, "NULL array pointer");
+    SweepGeom sg = make_geom(d, dir, false);
+    CoefPtrs cp{nullptr, nullptr, nullptr, nullptr, nullptr};
+    WenoParams wp{g->scheme, g->weno_eps, g->teno_CT};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == WENO_SB_FP64)
+        return launch_generic<double>(sg, 0, true, (const double*)v_rs_ws, (double*)vL, (double*)vR, cp, wp, st);
+    return launch_generic<float>(sg, 0, true, (const float*)v_rs_ws, (float*)vL, (float*)vR, cp, wp, st);
+}
+
+size_t weno_sb_checksum_scratch_bytes(int64_t n) {
+    (void)n;
+    return sizeof(double) * kSumBlocks;
+}
+
+int weno_sb_checksum_dev(int dtype, const void* arr, int64_t n, void* scratch, double* d_result,
+                         void* stream) {
+    WSB_FAULT("launch");
+    int rc = check_dtype(dtype);
+    if (rc) return rc;
+    if (n < 0) return set_err(WENO_SB_ERR_ARG, "negative element count");
+    if ((n > 0 && !arr) || !scratch || !d_result) return set_err(WENO_SB_ERR_ARG, "NULL pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    double* part = (double*)scratch;
+    if (dtype == WENO_SB_FP64)
+        abs_sum_partial_kernel<double><<<kSumBlocks, kSumThreads, 0, st>>>((const double*)arr, n, part);
+    else
+        abs_sum_partial_kernel<float><<<kSumBlocks, kSumThreads, 0, st>>>((const float*)arr, n, part);
+    abs_sum_final_kernel<<<1, kSumThreads, 0, st>>>(part, kSumBlocks, d_result);
+    return cuda_err(cudaGetLastError(), "checksum launch");
+}
+
+// ---------------- handle-based wrappers ----------------
+
+int weno_sb_initialize_weno(int handle, int dir) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    int rc = check_dir(dir);
+    if (rc) return rc;
+    return weno_sb_reshape_dev(&H->grid, dir, H->precision, (const double*)H->arr[WENO_SB_A_V_VF],
+                               H->arr[WENO_SB_A_RS(dir)], H->stream);
+}
+
+int weno_sb_weno(int handle, int dir, int order, unsigned flags) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    int rc = check_dir(dir);
+    if (rc) return rc;
+    if (order == 1)
+        return weno_sb_order1_dev(&H->grid, dir, H->precision, (const double*)H->arr[WENO_SB_A_V_VF],
+                                  H->arr[WENO_SB_A_VL(dir)], H->arr[WENO_SB_A_VR(dir)], H->stream);
+    weno_sb_coefs cf{(const double*)H->arr[WENO_SB_A_POLYL(dir)], (const double*)H->arr[WENO_SB_A_POLYR(dir)],
+                     (const double*)H->arr[WENO_SB_A_DL(dir)], (const double*)H->arr[WENO_SB_A_DR(dir)],
+                     (const double*)H->arr[WENO_SB_A_BETA(dir)]};
+    const void* in = (flags & WENO_SB_F_FOLDED) ? H->arr[WENO_SB_A_V_VF] : H->arr[WENO_SB_A_RS(dir)];
+    return weno_sb_weno_dev(&H->grid, dir, order, flags, H->precision, in, &cf, H->arr[WENO_SB_A_VL(dir)],
+                            H->arr[WENO_SB_A_VR(dir)], H->stream);
+}
+
+int weno_sb_preserve_monotonicity(int handle, int dir) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    int rc = check_dir(dir);
+    if (rc) return rc;
+    return weno_sb_preserve_monotonicity_dev(&H->grid, dir, H->precision, H->arr[WENO_SB_A_RS(dir)],
+                                             H->arr[WENO_SB_A_VL(dir)], H->arr[WENO_SB_A_VR(dir)], H->stream);
+}
+
+int weno_sb_checksum(int handle, int which, double* result) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
+    if (!result) return set_err(WENO_SB_ERR_ARG, "result pointer is NULL");
+    int rc = weno_sb_checksum_dev(H->dtype[which], H->arr[which], H->n[which], H->sum_scratch,
+                                  H->sum_scratch + kSumBlocks, H->stream);
+    if (rc) return rc;
+    WSB_CUDA(cudaMemcpyAsync(result, H->sum_scratch + kSumBlocks, sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    return cuda_err(cudaStreamSynchronize(H->stream), "checksum");
+}
+
+}  // extern "C"
