@@ -36,14 +36,16 @@ ORDER = 5
 METRIC = "WENO5 face-states/s at 199^3 x 8 vars (FP64 WENO5-JS + MP, x/y/z sweeps)"
 
 
-def face_states_per_dir(m=M, nv=NV, buff=BUFF):
+def face_states_per_dir(m=None, nv=NV, buff=BUFF):
+    m = M if m is None else m
     N = m + 2 * buff + 1
     return 2 * (N - 6) * N * N * nv
 
 
-def alg_bytes_per_sweep(m=M, nv=NV, buff=BUFF, elem=8, order=ORDER):
+def alg_bytes_per_sweep(m=None, nv=NV, buff=BUFF, elem=8, order=ORDER):
     """Algorithmic HBM bytes of one fused sweep: read the (NC+2H)-long
     stencil window of every column once, write vL and vR on the NC core faces."""
+    m = M if m is None else m
     N = m + 2 * buff + 1
     NC = N - 6
     H = max((order - 1) // 2, 2)
@@ -456,7 +458,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extras", action="store_true", help="skip FP32/drop-in/e2e side measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--m", type=int, default=199, help="cells per axis minus one (m=n=p); 199 = 200^3")
     args = ap.parse_args()
+    global M
+    M = args.m
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
