@@ -129,8 +129,14 @@ int weno_sb_weno(int handle, int dir, int order, unsigned flags);
 int weno_sb_preserve_monotonicity(int handle, int dir);
 /* f_checksum (f90:1617-1620): sum(|a|) of one array, computed on the GPU. */
 int weno_sb_checksum(int handle, int which, double *result);
-/* Wait for all work queued on the handle's stream. */
+/* Wait for all work queued on the handle's stream; also reports a device
+ * timeout (WENO_SB_ERR_TIMEOUT) raised by a pipelined sweep. */
 int weno_sb_sync(int handle);
+/* Synchronise `stream` (a cudaStream_t) and report, then clear, the device
+ * error flag that pipelined sweeps set when a bounded wait for staged data
+ * expires (WENO_SB_ERR_TIMEOUT).  Device-pointer callers use it where the
+ * handle API uses weno_sb_sync. */
+int weno_sb_check_device(void *stream);
 /* The handle's cudaStream_t (as void*), for callers that order their own
  * work after the library's. */
 int weno_sb_stream(int handle, void **stream);
@@ -162,6 +168,17 @@ int weno_sb_preserve_monotonicity_dev(const weno_sb_grid *g, int dir, int dtype,
 size_t weno_sb_checksum_scratch_bytes(int64_t n);
 int weno_sb_checksum_dev(int dtype, const void *arr, int64_t n, void *scratch,
                          double *d_result, void *stream);
+
+/* ===================================================================== */
+/* Diagnostics (no counterpart in the reference; used by the test suite).  */
+/* ===================================================================== */
+/* fast[i] = the library's Newton-refined reciprocal of x[i], ieee[i] = 1/x[i]
+ * by IEEE division, for n device doubles (normal, positive x). */
+int weno_sb_selftest_rcp(const double *d_x, double *d_fast, double *d_ieee, int64_t n, void *stream);
+/* Launch one bounded mbarrier wait that nothing completes, with a limit of
+ * limit_cycles SM clocks (<= 1e8), and return what weno_sb_check_device
+ * reports afterwards: WENO_SB_ERR_TIMEOUT when the bound works. */
+int weno_sb_selftest_timeout(int64_t limit_cycles, void *stream);
 
 #ifdef __cplusplus
 }

@@ -99,7 +99,7 @@ def _flip_fraction(got, ref, tol):
     return float(bad.mean())
 
 
-@pytest.mark.parametrize("kernel", ["auto", "generic"])
+@pytest.mark.parametrize("kernel", ["auto", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
 @pytest.mark.parametrize("scheme", SCHEMES)
@@ -257,3 +257,54 @@ def test_argument_errors(wsb):
     bad = L.WenoGrid(7, 7, 7, 1, 2, 0, 1e-16, 1e-5)
     rc = L.lib().weno_sb_reshape_dev(ctypes.byref(bad), 0, 0, t.data_ptr(), t.data_ptr(), None)
     assert rc == L.ERR_ARG and "buff_size" in L.last_error()
+
+
+def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64"):
+    import torch
+    from wenostandalone_b200 import api, fields
+    m = 47
+    g = wsb.Grid(m, m, m, 3, 6)
+    vf = fields.sinusoid_shock_field(m, m, m, 3, 6, seed=2, shock=False)
+    ref_field = vf if field_for_oracle == "fp64" else vf.astype(np.float32).astype(np.float64)
+    coefs = fields.uniform_weno_coefficients(order, g.nc(d))
+    rs = oracle_mod.reshape(np.asfortranarray(ref_field), m, m, m, 6, d)
+    Lr, Rr = oracle_mod.reconstruct(rs, coefs, order)
+    if mp:
+        oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+    v = to_dev(vf)
+    rs32 = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float32, device="cuda")
+    api.reshape(g, d, v, rs32)
+    L = torch.zeros(int(np.prod(g.face_shape(d))), dtype=torch.float32, device="cuda")
+    R = torch.zeros_like(L)
+    api.weno(g, d, order, rs32, tuple(to_dev(c) for c in coefs), L, R, flags=wsb.F_MP if mp else 0)
+    core = (slice(3, g.extents(d)[0] - 3),)
+    out = []
+    for got, ref in ((L, Lr), (R, Rr)):
+        got = from_dev(got, g.face_shape(d))[core]
+        ref = ref[core]
+        out.append((rel_err(got, ref), float(np.sqrt(np.mean((got - ref) ** 2)) / np.abs(ref).max())))
+    return out
+
+
+@pytest.mark.parametrize("order", [5, 7])
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_fp32_bulk_smooth_error(wsb, oracle_mod, order, d):
+    """FP32-bulk (FP32 fields and face states, FP32 stencil sums, FP64 beta and
+    normalisation) on smooth data vs the FP64 oracle on the FP64 field:
+    max-norm relative error <= 1e-6 per array."""
+    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=False):
+        assert mx <= 1e-6 and rms <= 1e-7, (mx, rms)
+
+
+@pytest.mark.parametrize("order", [5, 7])
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_fp32_bulk_with_mp_error(wsb, oracle_mod, order, d):
+    """With the MP limiter the FP32 storage rounding of the field (2^-24) is
+    amplified by the limiter's curvature bounds (|4 d0 - d1| has coefficient
+    sum 20 over the stencil, times beta_mp = 4/3): against the FP64 field the
+    bar is 4e-6 max / 1e-7 RMS.  Against the oracle run on the same
+    FP32-rounded field (the arithmetic alone) it is 1e-6."""
+    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=True):
+        assert mx <= 4e-6 and rms <= 1e-7, (mx, rms)
+    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=True, field_for_oracle="fp32"):
+        assert mx <= 1e-6, (mx, rms)

@@ -53,7 +53,8 @@ EXPORTED = [
     "weno_sb_preserve_monotonicity", "weno_sb_checksum", "weno_sb_sync",
     "weno_sb_stream", "weno_sb_reshape_dev", "weno_sb_order1_dev",
     "weno_sb_weno_dev", "weno_sb_preserve_monotonicity_dev",
-    "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev",
+    "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev", "weno_sb_check_device",
+    "weno_sb_selftest_rcp", "weno_sb_selftest_timeout",
 ]
 
 
@@ -115,6 +116,9 @@ def lib() -> ctypes.CDLL:
         "weno_sb_preserve_monotonicity_dev": ([gp, i32, i32, vp, vp, vp, vp], i32),
         "weno_sb_checksum_scratch_bytes": ([ctypes.c_int64], ctypes.c_size_t),
         "weno_sb_checksum_dev": ([i32, vp, ctypes.c_int64, vp, vp, vp], i32),
+        "weno_sb_check_device": ([vp], i32),
+        "weno_sb_selftest_rcp": ([vp, vp, vp, ctypes.c_int64, vp], i32),
+        "weno_sb_selftest_timeout": ([ctypes.c_int64, vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

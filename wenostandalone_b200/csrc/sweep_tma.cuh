@@ -114,7 +114,69 @@ __device__ __forceinline__ void issue_stage(const FastArgs& a, T* buf, long long
     }
 }
 
-template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES>
+// Views of a staged column group seen from one face: element q (stencil
+// offset from the face's centre cell) of column k.
+template <typename T>
+struct LinearTile {  // plain row-major staging (cp.async, or TMA without swizzle)
+    const T* p;      // centre element of column 0
+    int js, ks;      // strides along the sweep and between columns
+    __device__ __forceinline__ T operator()(int q, int k) const { return p[k * ks + q * js]; }
+};
+
+template <typename T>
+struct Swz128Tile {  // TMA box of 128-byte rows in the 128B swizzle pattern
+    const unsigned char* base;  // stage base (1024-byte aligned)
+    int row0;                   // window row of the face's centre cell
+    __device__ __forceinline__ T operator()(int q, int k) const {
+        const int row = row0 + q;
+        const int byte = k * (int)sizeof(T);
+        return *reinterpret_cast<const T*>(base + row * 128 + ((((byte >> 4) ^ (row & 7))) << 4) + (byte & 15));
+    }
+};
+
+// Reconstruct columns [kb, ke) of one staged group for this thread's face
+// (index o); the output of column k goes to oidx0 + k*o_sU.
+// SCH >= 0 fixes the weight family at compile time (0 = JS, the common
+// case, so the other families' code is not carried); -1 reads it at run time.
+template <int ORDER, bool MPF, typename T, int SCH, typename Tile>
+__device__ __forceinline__ void compute_columns(const FastArgs& a, const Coef<ORDER>& cf, const Tile& t, int kb,
+                                                int ke, long long oidx0, long long o) {
+    const int scheme = (SCH >= 0) ? SCH : a.wp.scheme;
+    T* __restrict__ vL = (T*)a.vL;
+    T* __restrict__ vR = (T*)a.vR;
+    long long oidx = oidx0 + (long long)kb * a.o_sU;
+    for (int k = kb; k < ke; ++k, oidx += a.o_sU) {
+        T Lt, Rt;
+        if constexpr (ORDER == 3) {
+            double L, R;
+            weno3_face((double)t(-1, k), (double)t(0, k), (double)t(1, k), cf, scheme, a.wp.eps, L, R);
+            Lt = (T)L;
+            Rt = (T)R;
+            if (MPF && o >= 3 && o <= a.ns - 4) MP<T>::apply(t(-2, k), t(-1, k), t(0, k), t(1, k), t(2, k), Lt, Rt);
+        } else if constexpr (ORDER == 5) {
+            const T m2 = t(-2, k), m1 = t(-1, k), z0 = t(0, k), p1 = t(1, k), p2 = t(2, k);
+            double L, R;
+            weno5_face<T>((double)m2, (double)m1, (double)z0, (double)p1, (double)p2, cf, scheme, a.wp.eps,
+                          a.wp.teno_ct, L, R);
+            Lt = (T)L;
+            Rt = (T)R;
+            if (MPF) MP<T>::apply(m2, m1, z0, p1, p2, Lt, Rt);
+        } else {
+            double s7[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) s7[q] = (double)t(q - 3, k);
+            double L, R;
+            weno7_face<T>(s7 + 3, cf, scheme, a.wp.eps, a.wp.teno_ct, L, R);
+            Lt = (T)L;
+            Rt = (T)R;
+            if (MPF) MP<T>::apply(t(-2, k), t(-1, k), t(0, k), t(1, k), t(2, k), Lt, Rt);
+        }
+        vL[oidx] = Lt;
+        vR[oidx] = Rt;
+    }
+}
+
+template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES, int SCH>
 __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(const FastArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
@@ -138,8 +200,6 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(c
     Coef<ORDER> cf;
     if (active) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
 
-    T* __restrict__ vL = (T*)a.vL;
-    T* __restrict__ vR = (T*)a.vR;
     const int js = (KIND == 0) ? 1 : a.pitch;     // smem stride along the sweep
     const int ks = (KIND == 0) ? a.pitch : 1;     // smem stride between columns
 
@@ -161,48 +221,14 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(c
         }
         if (!active) continue;
         const GroupInfo gi = group_info(a, grp);
-        const T* buf = smem + (it % STAGES) * stage_elems + (f + H) * js;
-        long long oidx = gi.out0 + o;
-        for (int k = 0; k < gi.ucnt; ++k, oidx += a.o_sU) {
-            const T* base = buf + k * ks;
-            T Lt, Rt;
-            if constexpr (ORDER == 3) {
-                double L, R;
-                weno3_face((double)base[-js], (double)base[0], (double)base[js], cf, a.wp.scheme, a.wp.eps, L, R);
-                Lt = (T)L;
-                Rt = (T)R;
-                if (MPF && o >= 3 && o <= a.ns - 4)
-                    MP<T>::apply(base[-2 * js], base[-js], base[0], base[js], base[2 * js], Lt, Rt);
-            } else if constexpr (ORDER == 5) {
-                const T m2 = base[-2 * js], m1 = base[-js], z0 = base[0], p1 = base[js], p2 = base[2 * js];
-                double L, R;
-                weno5_face<T>((double)m2, (double)m1, (double)z0, (double)p1, (double)p2, cf, a.wp.scheme,
-                              a.wp.eps, a.wp.teno_ct, L, R);
-                Lt = (T)L;
-                Rt = (T)R;
-                if (MPF) MP<T>::apply(m2, m1, z0, p1, p2, Lt, Rt);
-            } else {
-                double s7[7];
-#pragma unroll
-                for (int q = 0; q < 7; ++q) s7[q] = (double)base[(q - 3) * js];
-                double L, R;
-                weno7_face<T>(s7 + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, L, R);
-                Lt = (T)L;
-                Rt = (T)R;
-                if (MPF) MP<T>::apply(base[-2 * js], base[-js], base[0], base[js], base[2 * js], Lt, Rt);
-            }
-            vL[oidx] = Lt;
-            vR[oidx] = Rt;
-        }
+        const LinearTile<T> tile{smem + (it % STAGES) * stage_elems + (f + H) * js, js, ks};
+        compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, 0, gi.ucnt, gi.out0 + o, o);
     }
     cp_async_wait<0>();
 }
 
-// Device error flag for bounded waits (reserved for the TMA loader).
-inline int tma_check_device_error(cudaStream_t) { return 0; }
-
-template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES>
-int launch_fast_t(FastArgs a, cudaStream_t st, int sms) {
+template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES, int SCH>
+int launch_fast_s(FastArgs a, cudaStream_t st, int sms) {
     const int threads = ((a.TJ + 31) / 32) * 32;
     size_t smem;
     if (KIND == 0) {
@@ -215,7 +241,7 @@ int launch_fast_t(FastArgs a, cudaStream_t st, int sms) {
     }
     a.n_ut = (a.Nu + a.U - 1) / a.U;
     a.n_groups = (long long)a.n_ut * a.Nw * a.NV;
-    auto kfn = sweep_fast_kernel<ORDER, MPF, T, KIND, XW, STAGES>;
+    auto kfn = sweep_fast_kernel<ORDER, MPF, T, KIND, XW, STAGES, SCH>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -230,6 +256,12 @@ int launch_fast_t(FastArgs a, cudaStream_t st, int sms) {
     const long long grid = per_jt * a.n_jt;
     kfn<<<(unsigned)grid, threads, smem, st>>>(a);
     return 0;
+}
+
+template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES>
+int launch_fast_t(FastArgs a, cudaStream_t st, int sms) {
+    if (a.wp.scheme == JS) return launch_fast_s<ORDER, MPF, T, KIND, XW, STAGES, 0>(a, st, sms);
+    return launch_fast_s<ORDER, MPF, T, KIND, XW, STAGES, -1>(a, st, sms);
 }
 
 // Returns WENO_SB_ERR_UNSUPPORTED (1003) when the layout does not fit this

@@ -9,17 +9,18 @@
 //  * "faithful": the reference's sequence (alpha_k = d_k/beta_k^2, then
 //    omega_k = alpha_k/sum) for every weight family, used for
 //    mapped / Z / TENO / none;
-//  * "one-division JS": omega_k = d_k P_k / sum_m d_m P_m with
+//  * "one-reciprocal JS": omega_k = d_k P_k / sum_m d_m P_m with
 //    P_k = prod_{m != k} beta_m^2, which is the same rational function
-//    multiplied through by prod beta_m^2.  One division per side instead of
-//    2N, the P_k are shared by the left and right states.  It rounds
-//    differently (a few ulp) and is exact in real arithmetic; when the
-//    products leave the normal range (beta > ~1e77 or eps < ~1e-77) the
-//    faithful form is used instead.
+//    multiplied through by prod beta_m^2.  The P_k are shared by the left
+//    and right states, and both normalisations use one reciprocal,
+//    1/(S_L S_R).  It rounds differently (a few ulp) and is exact in real
+//    arithmetic; when a sum leaves [2^-498, 2^498) (extreme beta, or
+//    eps < ~1e-37) the faithful form is used instead.
 //
-// The MP limiter is written with explicit _rn intrinsics so that no FMA is
-// contracted: its min/max decisions depend on the signs of second
-// differences, and must round exactly as the reference does.
+// The MP limiter rounds exactly as the reference does (its min/max
+// decisions depend on the signs of second differences): every product and
+// sum is either an explicit _rn intrinsic, which is never contracted into an
+// FMA, or an FMA whose product is exact (by 2, 4 or 1/2).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -104,6 +105,28 @@ struct Coef<7> {
 
 __device__ __forceinline__ bool normal_pos(double s) { return s > 1e-300 && s < 1e300; }
 
+// True when s is positive with 2^-498 <= s < 2^498 (an integer test on the
+// exponent field, so it costs no FP64 issue slot).  Two such values have a
+// product that is a normal number.
+__device__ __forceinline__ bool mid_range(double s) {
+    const unsigned hi = (unsigned)__double2hiint(s);
+    return (hi - (525u << 20)) < (996u << 20);
+}
+
+// Reciprocal of a normal positive double by Newton-Raphson refinement of the
+// hardware seed (PTX rcp.approx.ftz.f64): r <- r + r (1 - s r), twice.  Each
+// step squares the relative error, so any seed better than 2^-14 ends below
+// 2^-53 plus rounding; the GPU tests check the result against IEEE division
+// on random inputs.
+__device__ __forceinline__ double nr_rcp(double s) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
+    double e = fma(-s, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-s, r, 1.0);
+    return fma(r, e, r);
+}
+
 // Mapped-WENO transform (f90:419-423, 557-568).
 __device__ __forceinline__ double mapw(double d, double w) {
     return (d * (1.0 + d - 3.0 * w) + w * w) * (w / (d * d + w * (1.0 - 2.0 * d)));
@@ -126,9 +149,10 @@ __device__ __forceinline__ void weno3_face(const double vm1, const double v0, co
         const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1;
         const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1;
         const double SL = aL0 + aL1, SR = aR0 + aR1;
-        if (normal_pos(SL) && normal_pos(SR)) {
-            oL = (aL0 * pL0 + aL1 * pL1) / SL;
-            oR = (aR0 * pR0 + aR1 * pR1) / SR;
+        if (mid_range(SL) && mid_range(SR)) {
+            const double r = nr_rcp(SL * SR);
+            oL = (aL0 * pL0 + aL1 * pL1) * (SR * r);
+            oR = (aR0 * pR0 + aR1 * pR1) * (SL * r);
             return;
         }
     }
@@ -204,9 +228,10 @@ __device__ __forceinline__ void weno5_face(const double vm2, const double vm1, c
         const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2;
         const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2;
         const double SL = aL0 + aL1 + aL2, SR = aR0 + aR1 + aR2;
-        if (normal_pos(SL) && normal_pos(SR)) {
-            oL = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) / SL;
-            oR = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) / SR;
+        if (mid_range(SL) && mid_range(SR)) {
+            const double r = nr_rcp(SL * SR);
+            oL = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * (SR * r);
+            oR = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * (SL * r);
             return;
         }
     }
@@ -314,9 +339,10 @@ __device__ __forceinline__ void weno7_face(const double* v /* v[-3..3] */, const
         const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2, aL3 = c.dL[3] * P3;
         const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2, aR3 = c.dR[3] * P3;
         const double SL = aL0 + aL1 + aL2 + aL3, SR = aR0 + aR1 + aR2 + aR3;
-        if (normal_pos(SL) && normal_pos(SR)) {
-            oL = (aL0 * pL[0] + aL1 * pL[1] + aL2 * pL[2] + aL3 * pL[3]) / SL;
-            oR = (aR0 * pR[0] + aR1 * pR[1] + aR2 * pR[2] + aR3 * pR[3]) / SR;
+        if (mid_range(SL) && mid_range(SR)) {
+            const double r = nr_rcp(SL * SR);
+            oL = (aL0 * pL[0] + aL1 * pL[1] + aL2 * pL[2] + aL3 * pL[3]) * (SR * r);
+            oR = (aR0 * pR[0] + aR1 * pR[1] + aR2 * pR[2] + aR3 * pR[3]) * (SL * r);
             return;
         }
     }
@@ -381,46 +407,62 @@ __device__ __forceinline__ void weno7_face(const double* v /* v[-3..3] */, const
 // 4-argument minmod of (4dl-dr, dl, 4dr-dl, dr) (f90:1568-1571).  The
 // reference's product of SIGN() sums is +-1 when all four arguments share a
 // sign bit and 0 otherwise, so it equals copysign(min|.|, 4dl-dr) or 0.
+// 4*dl is exact, so fma(4, dl, -dr) rounds exactly like 4*dl - dr.
 __device__ __forceinline__ double mp_minmod(double dl, double dr) {
-    const double A = __dsub_rn(__dmul_rn(4.0, dl), dr);
-    const double B = __dsub_rn(__dmul_rn(4.0, dr), dl);
-    const double mn = fmin(fmin(fmin(fabs(A), fabs(dl)), fabs(B)), fabs(dr));
+    const double A = fma(4.0, dl, -dr);
+    const double B = fma(4.0, dr, -dl);
+    const double mn = fmin(fmin(fabs(A), fabs(dl)), fmin(fabs(B), fabs(dr)));
     const int hA = __double2hiint(A);
     const int same = (hA ^ __double2hiint(B)) | (hA ^ __double2hiint(dl)) | (hA ^ __double2hiint(dr));
     return (same >= 0) ? copysign(mn, A) : 0.0;
 }
 
-// x + (sign(1/2, lo-x) + sign(1/2, hi-x)) * min(|lo-x|, |hi-x|)  (f90:1582-1583)
+// x + (sign(1/2, lo-x) + sign(1/2, hi-x)) * min(|lo-x|, |hi-x|)  (f90:1582-1583).
+// The factor is -1, 0 or +1, so the update is x + copysign(min, lo-x) when
+// lo-x and hi-x share a sign bit and x otherwise.
 __device__ __forceinline__ double mp_clamp(double x, double lo, double hi) {
     const double a = __dsub_rn(lo, x), b = __dsub_rn(hi, x);
-    const double f = __dadd_rn(copysign(0.5, a), copysign(0.5, b));
-    return __dadd_rn(x, __dmul_rn(f, fmin(fabs(a), fabs(b))));
+    const double m = fmin(fabs(a), fabs(b));
+    const bool same = (__double2hiint(a) ^ __double2hiint(b)) >= 0;
+    return same ? __dadd_rn(x, copysign(m, a)) : x;
 }
 
+__device__ __forceinline__ bool sign_clear(double x) { return __double2hiint(x) >= 0; }
+
+// The limiter proper.  min(v0, v0 -/+ 2 dv) and min(v0, v_{j+-1}) are
+// decided by the sign of the difference that produced them (an exact
+// ordering test for finite values), which saves FP64 min/max issue slots;
+// every arithmetic step keeps the reference's rounding (the products by 2,
+// 4 and 1/2 are exact, so they may fuse).
 __device__ __forceinline__ void mp_limit(const double vm2, const double vm1, const double v0,
                                          const double vp1, const double vp2, double& L, double& R) {
     const double kBetaMP = 4.0 / 3.0;  // beta_mp (f90:1556)
-    const double dm1 = __dsub_rn(__dadd_rn(v0, vm2), __dmul_rn(2.0, vm1));
-    const double d0 = __dsub_rn(__dadd_rn(vp1, vm1), __dmul_rn(2.0, v0));
-    const double dp1 = __dsub_rn(__dadd_rn(vp2, v0), __dmul_rn(2.0, vp1));
+    const double dm1 = fma(-2.0, vm1, __dadd_rn(v0, vm2));
+    const double d0 = fma(-2.0, v0, __dadd_rn(vp1, vm1));
+    const double dp1 = fma(-2.0, vp1, __dadd_rn(vp2, v0));
     const double mA = mp_minmod(dm1, d0);  // d_MD of vL, d_LC of vR
     const double mB = mp_minmod(d0, dp1);  // d_LC of vL, d_MD of vR
+    const double dR1 = __dsub_rn(vp1, v0);  // >= 0  <=>  vp1 >= v0
+    const double dL1 = __dsub_rn(v0, vm1);  // >= 0  <=>  v0 >= vm1
+    const bool up_r = sign_clear(dR1), up_l = sign_clear(dL1);
     {
-        const double dR1 = __dsub_rn(vp1, v0);
-        const double UL = __dsub_rn(v0, __dmul_rn(2.0, dR1));
+        const double UL = fma(-2.0, dR1, v0);                      // v0 - 2 dR1: <= v0 iff dR1 >= 0
         const double MD = __dmul_rn(__dsub_rn(__dadd_rn(v0, vm1), mA), 0.5);
-        const double LC = __dadd_rn(__dsub_rn(v0, __dmul_rn(dR1, 0.5)), __dmul_rn(kBetaMP, mB));
-        const double lo = fmax(fmin(fmin(v0, vm1), MD), fmin(fmin(v0, UL), LC));
-        const double hi = fmin(fmax(fmax(v0, vm1), MD), fmax(fmax(v0, UL), LC));
+        const double LC = __dadd_rn(fma(-0.5, dR1, v0), __dmul_rn(kBetaMP, mB));
+        const double mn1 = up_l ? vm1 : v0, mx1 = up_l ? v0 : vm1;  // min/max(v0, vm1)
+        const double mn2 = up_r ? UL : v0, mx2 = up_r ? v0 : UL;    // min/max(v0, UL)
+        const double lo = fmax(fmin(mn1, MD), fmin(mn2, LC));
+        const double hi = fmin(fmax(mx1, MD), fmax(mx2, LC));
         L = mp_clamp(L, lo, hi);
     }
     {
-        const double dL1 = __dsub_rn(v0, vm1);
-        const double UL = __dadd_rn(v0, __dmul_rn(2.0, dL1));
+        const double UL = fma(2.0, dL1, v0);                       // v0 + 2 dL1: >= v0 iff dL1 >= 0
         const double MD = __dmul_rn(__dsub_rn(__dadd_rn(v0, vp1), mB), 0.5);
-        const double LC = __dadd_rn(__dadd_rn(v0, __dmul_rn(dL1, 0.5)), __dmul_rn(kBetaMP, mA));
-        const double lo = fmax(fmin(fmin(v0, vp1), MD), fmin(fmin(v0, UL), LC));
-        const double hi = fmin(fmax(fmax(v0, vp1), MD), fmax(fmax(v0, UL), LC));
+        const double LC = __dadd_rn(fma(0.5, dL1, v0), __dmul_rn(kBetaMP, mA));
+        const double mn1 = up_r ? v0 : vp1, mx1 = up_r ? vp1 : v0;  // min/max(v0, vp1)
+        const double mn2 = up_l ? v0 : UL, mx2 = up_l ? UL : v0;    // min/max(v0, UL)
+        const double lo = fmax(fmin(mn1, MD), fmin(mn2, LC));
+        const double hi = fmin(fmax(mx1, MD), fmax(mx2, LC));
         R = mp_clamp(R, lo, hi);
     }
 }

@@ -19,6 +19,7 @@
 #include "layout.cuh"
 #include "sweep_generic.cuh"
 #include "sweep_tma.cuh"
+#include "sweep_pipe.cuh"
 
 using namespace wsb;
 
@@ -255,12 +256,14 @@ int launch_generic(const SweepGeom& g, int order, bool mp, const T* in, T* vL, T
     return cuda_err(cudaGetLastError(), "reconstruction launch");
 }
 
-// Which implementation serves reconstruction sweeps: 0 = automatic (TMA
-// pipeline when the layout allows it), 1 = always the general-stride
-// kernel.  Set through WENO_SB_KERNEL=generic|auto (read per call).
+// Which implementation serves reconstruction sweeps, from WENO_SB_KERNEL
+// (read per call): "auto" (default: TMA pipeline for FP64 when the layout
+// allows it, else the cp.async pipeline, else the general-stride kernel),
+// "tma", "cpasync" or "generic" to pin one for testing.
 int kernel_choice() {
     const char* e = getenv("WENO_SB_KERNEL");
     if (e && strcmp(e, "generic") == 0) return 1;
+    if (e && strcmp(e, "cpasync") == 0) return 2;
     return 0;
 }
 
@@ -273,9 +276,16 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (g.nc < 1) return set_err(WENO_SB_ERR_ARG, "sweep has no core faces (Ns=%lld)", g.ns);
     CoefPtrs cp{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
-    if (kernel_choice() == 0) {
+    const int choice = kernel_choice();
+    if constexpr (sizeof(T) == 8) {
+        if (choice == 0) {
+            int rc = launch_pipe_sweep(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st, num_sms());
+            if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "tma sweep launch") : rc;
+        }
+    }
+    if (choice == 0 || choice == 2) {
         int rc = launch_tma_sweep<T>(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st);
-        if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "tma sweep launch") : rc;
+        if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "cp.async sweep launch") : rc;
     }
     return launch_generic<T>(g, order, mp, in, vL, vR, cp, wp, st);
 }
@@ -456,7 +466,16 @@ int weno_sb_sync(int handle) {
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
     int rc = cuda_err(cudaStreamSynchronize(H->stream), "cudaStreamSynchronize");
     if (rc) return rc;
-    return tma_check_device_error(H->stream);
+    return weno_sb_check_device(H->stream);
+}
+
+int weno_sb_check_device(void* stream) {
+    const int v = pipe_check_device_error((cudaStream_t)stream);
+    if (v == 0) return WENO_SB_OK;
+    if (v == WENO_SB_ERR_TIMEOUT)
+        return set_err(v, "a pipelined sweep gave up a bounded wait for its staged data (device timeout)");
+    if (v < 1000) return cuda_err((cudaError_t)v, "device check");
+    return set_err(v, "device error flag %d", v);
 }
 
 int weno_sb_reshape_dev(const weno_sb_grid* g, int dir, int dtype, const double* v_vf, void* v_rs_ws,
@@ -588,6 +607,23 @@ int weno_sb_checksum(int handle, int which, double* result) {
     if (rc) return rc;
     WSB_CUDA(cudaMemcpyAsync(result, H->sum_scratch + kSumBlocks, sizeof(double), cudaMemcpyDeviceToHost, H->stream));
     return cuda_err(cudaStreamSynchronize(H->stream), "checksum");
+}
+
+int weno_sb_selftest_rcp(const double* d_x, double* d_fast, double* d_ieee, int64_t n, void* stream) {
+    if (n < 0 || (n > 0 && (!d_x || !d_fast || !d_ieee))) return set_err(WENO_SB_ERR_ARG, "bad self-test arguments");
+    if (n == 0) return WENO_SB_OK;
+    selftest_rcp_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, (cudaStream_t)stream>>>(
+        d_x, d_fast, d_ieee, n);
+    return cuda_err(cudaGetLastError(), "self-test launch");
+}
+
+int weno_sb_selftest_timeout(int64_t limit_cycles, void* stream) {
+    if (limit_cycles < 0 || limit_cycles > 100000000LL)
+        return set_err(WENO_SB_ERR_ARG, "limit_cycles must be in [0, 1e8]");
+    selftest_timeout_kernel<<<1, 32, 0, (cudaStream_t)stream>>>((long long)limit_cycles);
+    int rc = cuda_err(cudaGetLastError(), "self-test launch");
+    if (rc) return rc;
+    return weno_sb_check_device(stream);
 }
 
 }  // extern "C"
