@@ -169,6 +169,23 @@ size_t weno_sb_checksum_scratch_bytes(int64_t n);
 int weno_sb_checksum_dev(int dtype, const void *arr, int64_t n, void *scratch,
                          double *d_result, void *stream);
 
+/* f_checksum of up to 16 arrays in one call, allocating nothing.
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory: Fortran drivers whose device heap belongs to the OpenMP/OpenACC
+ * offload runtime (as in MFC), and time-step loops that must not call
+ * cudaMalloc/cudaFree because those calls can synchronise the whole device.
+ * arrays[a] (device pointers) and n[a] are host arrays of `count` entries;
+ * sum(|arrays[a]|) is written to the device double d_results[a].  The
+ * scratch is a static device array of 16 x 592 doubles (74 KB) in the
+ * library, held on every GPU that loads it until exit: count > 16 is
+ * rejected with WENO_SB_ERR_ARG.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the one array, so calls that overlap
+ * on the GPU (different streams, or host threads) race; each call rewrites
+ * every partial it reads, so nothing needs clearing between calls. */
+int weno_sb_checksum_noalloc(int dtype, const void *const *arrays, const int64_t *n, int count,
+                             double *d_results, void *stream);
+
 /* ===================================================================== */
 /* Diagnostics (no counterpart in the reference; used by the test suite).  */
 /* ===================================================================== */

@@ -54,7 +54,7 @@ EXPORTED = [
     "weno_sb_stream", "weno_sb_reshape_dev", "weno_sb_order1_dev",
     "weno_sb_weno_dev", "weno_sb_preserve_monotonicity_dev",
     "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev", "weno_sb_check_device",
-    "weno_sb_selftest_rcp", "weno_sb_selftest_timeout",
+    "weno_sb_selftest_rcp", "weno_sb_selftest_timeout", "weno_sb_checksum_noalloc",
 ]
 
 
@@ -119,6 +119,7 @@ def lib() -> ctypes.CDLL:
         "weno_sb_check_device": ([vp], i32),
         "weno_sb_selftest_rcp": ([vp, vp, vp, ctypes.c_int64, vp], i32),
         "weno_sb_selftest_timeout": ([ctypes.c_int64, vp], i32),
+        "weno_sb_checksum_noalloc": ([i32, ctypes.POINTER(ctypes.c_void_p), i64p, i32, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -609,6 +609,61 @@ int weno_sb_checksum(int handle, int which, double* result) {
     return cuda_err(cudaStreamSynchronize(H->stream), "checksum");
 }
 
+// ---------------- checksum without allocation ----------------
+// Partial sums for weno_sb_checksum_noalloc: kSumBlocks doubles for each of
+// up to kNoAllocMaxArrays arrays (74 KB), resident on every GPU that loads
+// the library until the process exits.  Host code may not use the symbol
+// as a device address: the address comes from cudaGetSymbolAddress, looked
+// up once per device on that device's first call.
+static constexpr int kNoAllocMaxArrays = 16;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxArrays * kSumBlocks];
+static constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+int weno_sb_checksum_noalloc(int dtype, const void* const* arrays, const int64_t* n, int count,
+                             double* d_results, void* stream) {
+    WSB_FAULT("launch");
+    int rc = check_dtype(dtype);
+    if (rc) return rc;
+    if (count < 1 || count > kNoAllocMaxArrays)
+        return set_err(WENO_SB_ERR_ARG,
+                       "count must be 1..%d: the static scratch holds the partial sums of at most %d arrays (got %d)",
+                       kNoAllocMaxArrays, kNoAllocMaxArrays, count);
+    if (!arrays || !n || !d_results) return set_err(WENO_SB_ERR_ARG, "NULL pointer");
+    for (int a = 0; a < count; ++a) {
+        if (n[a] < 0) return set_err(WENO_SB_ERR_ARG, "negative element count for array %d", a);
+        if (n[a] > 0 && !arrays[a]) return set_err(WENO_SB_ERR_ARG, "NULL device pointer for array %d", a);
+    }
+    int dev = 0;
+    WSB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return set_err(WENO_SB_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, kNoAllocMaxDevices);
+    double* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+            if (e != cudaSuccess) return cuda_err(e, "cudaGetSymbolAddress(g_noalloc_partials)");
+            g_noalloc_addr[dev] = (double*)p;
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int a = 0; a < count; ++a) {
+        double* part = scratch + (size_t)a * kSumBlocks;
+        // every one of the kSumBlocks partials is rewritten before it is read,
+        // so nothing left by an earlier call needs clearing
+        if (dtype == WENO_SB_FP64)
+            abs_sum_partial_kernel<double><<<kSumBlocks, kSumThreads, 0, st>>>((const double*)arrays[a], n[a], part);
+        else
+            abs_sum_partial_kernel<float><<<kSumBlocks, kSumThreads, 0, st>>>((const float*)arrays[a], n[a], part);
+        abs_sum_final_kernel<<<1, kSumThreads, 0, st>>>(part, kSumBlocks, d_results + a);
+    }
+    return cuda_err(cudaGetLastError(), "checksum (no-alloc) launch");
+}
+
 int weno_sb_selftest_rcp(const double* d_x, double* d_fast, double* d_ieee, int64_t n, void* stream) {
     if (n < 0 || (n > 0 && (!d_x || !d_fast || !d_ieee))) return set_err(WENO_SB_ERR_ARG, "bad self-test arguments");
     if (n == 0) return WENO_SB_OK;
