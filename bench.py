@@ -208,6 +208,9 @@ def run_ours(args):
     coefs = [tuple(torch.from_numpy(c.ravel(order="F")).to(dev)
                    for c in fields.uniform_weno_coefficients(ORDER, g.nc(d))) for d in range(3)]
     cstructs = [api.coefs_struct(c) for c in coefs]
+    # the coefficients are face-independent (uniform grid): the sweeps take
+    # them from the kernel-parameter bank through weno_sb_weno_uniform_dev
+    faces = [api.face_coefs(fields.uniform_weno_coefficients(ORDER, g.nc(d))) for d in range(3)]
     nface = int(np.prod(g.face_shape(0)))
     outs = [(torch.empty(nface, dtype=torch.float64, device=dev),
              torch.empty(nface, dtype=torch.float64, device=dev)) for _ in range(3)]
@@ -215,11 +218,14 @@ def run_ours(args):
     sp = int(stream.cuda_stream)
     flags = wsb.F_MP | wsb.F_FOLDED
 
-    def step(evs=None):
+    def step(evs=None, per_face=False):
         for d in range(3):
             if evs is not None:
                 evs[d][0].record(stream)
-            api.weno(g, d, ORDER, v, cstructs[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
+            if per_face:
+                api.weno(g, d, ORDER, v, cstructs[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
+            else:
+                api.weno_uniform(g, d, ORDER, v, faces[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
             if evs is not None:
                 evs[d][1].record(stream)
 
@@ -262,11 +268,27 @@ def run_ours(args):
     ab = alg_bytes_per_sweep()
     achieved = ab / (dk_ms * 1e-3) / 1e9
 
+    # the same step with per-face coefficient arrays (stretched-grid form)
+    per_face = None
+    if not args.no_extras:
+        for _ in range(3):
+            step(per_face=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(K):
+            step(per_face=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pf_ms = e0.elapsed_time(e1) / K
+        per_face = {"ms_per_step": pf_ms, "value": 3 * face_states_per_dir() / (pf_ms * 1e-3),
+                    "entry": "weno_sb_weno_dev (coefficient arrays read per face)"}
+
     # FP32-bulk variant (same sweeps, FP32 v_rs_ws field and face states)
     fp32 = None
     if not args.no_extras:
-        fp32 = measure_fp32_bulk(g, v, cstructs, outs, stream, K, dev)
-        drop = measure_drop_in(g, v, cstructs, outs, stream, K, dev)
+        fp32 = measure_fp32_bulk(g, v, faces, outs, stream, K, dev)
+        drop = measure_drop_in(g, v, faces, outs, stream, K, dev)
     else:
         drop = None
 
@@ -288,7 +310,8 @@ def run_ours(args):
                        "field": "seeded smooth-plus-jump", "l2": "inputs (663 MB) and outputs (3.7 GB) exceed "
                                                                   "the 126 MB L2; no flush",
                        "parallelism": f"{ws} independent blocks (weak scaling, no collective)"},
-            "roofline": {"bound": "hbm", "kernel": f"sweep_fast_kernel<5,MP,f64> {'xyz'[dk]} sweep",
+            "roofline": {"bound": "hbm", "kernel": f"sweep_pipe_kernel<5,MP,JS,uniform> {'xyz'[dk]} sweep "
+                                                   f"({'row tiles' if dk == 0 else '128B-swizzled column tiles'})",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
@@ -298,6 +321,8 @@ def run_ours(args):
             "gpu_launches": 3 * K,
             "clocks": clk.summary(),
         }
+        if per_face:
+            line["per_face_coefficients"] = per_face
         if fp32:
             line["fp32_bulk"] = fp32
         if drop:
@@ -330,7 +355,7 @@ def read_traffic():
     return None
 
 
-def measure_fp32_bulk(g, v, cstructs, outs64, stream, K, dev):
+def measure_fp32_bulk(g, v, faces, outs64, stream, K, dev):
     """FP32-bulk: FP32 sweep fields (reshaped from v_vf) and face states; FP64
     beta differences and weight normalisation.  Timed on the sweeps; error
     stated against the FP64 outputs of the same step (max-norm relative)."""
@@ -348,7 +373,7 @@ def measure_fp32_bulk(g, v, cstructs, outs64, stream, K, dev):
 
     def step():
         for d in range(3):
-            api.weno(g, d, ORDER, rs[d], cstructs[d], o32[d][0], o32[d][1], flags=wsb.F_MP, stream=sp)
+            api.weno_uniform(g, d, ORDER, rs[d], faces[d], o32[d][0], o32[d][1], flags=wsb.F_MP, stream=sp)
 
     for _ in range(3):
         step()
@@ -374,7 +399,7 @@ def measure_fp32_bulk(g, v, cstructs, outs64, stream, K, dev):
             "form": "drop-in (FP32 v_rs_ws, reshaped once outside the timed loop)"}
 
 
-def measure_drop_in(g, v, cstructs, outs, stream, K, dev):
+def measure_drop_in(g, v, faces, outs, stream, K, dev):
     """The drop-in form: s_initialize_weno (tiled-transpose reshape into
     v_rs_ws) then the sweep, per direction."""
     import torch
@@ -388,7 +413,7 @@ def measure_drop_in(g, v, cstructs, outs, stream, K, dev):
         for d in range(3):
             if reshape:
                 api.reshape(g, d, v, rs[d], stream=sp)
-            api.weno(g, d, ORDER, rs[d], cstructs[d], outs[d][0], outs[d][1], flags=wsb.F_MP, stream=sp)
+            api.weno_uniform(g, d, ORDER, rs[d], faces[d], outs[d][0], outs[d][1], flags=wsb.F_MP, stream=sp)
 
     res = {}
     for reshape in (True, False):

@@ -65,6 +65,7 @@ extern "C" {
 #define WENO_SB_F_MP 4u          /* fuse s_preserve_monotonicity (f90:1544)  */
 #define WENO_SB_F_FOLDED 8u      /* read v_vf directly: reshape folded into
                                     the sweep (no v_rs_ws needed)            */
+#define WENO_SB_F_ACCUMULATE 16u /* adjoint: add into gv instead of writing it */
 
 /* ---- array ids for the handle API (the harness's module arrays) ---- */
 #define WENO_SB_A_V_VF 0
@@ -92,6 +93,16 @@ typedef struct weno_sb_grid {
 typedef struct weno_sb_coefs {
     const double *polyL, *polyR, *dL, *dR, *beta_coef;
 } weno_sb_coefs;
+
+/* One face's coefficients, on the host, for grids where every face uses the
+ * same values (uniform spacing, and the harness's synthetic data):
+ * polyL[s][r] = polyL(j,r,s), dL[r] = dL(r,j), beta_coef[s][r] =
+ * beta_coef(j,r,s) for any core face j. */
+typedef struct weno_sb_face_coefs {
+    double polyL[3][5], polyR[3][5];
+    double dL[5], dR[5];
+    double beta_coef[6][5];
+} weno_sb_face_coefs;
 
 /* ===================================================================== */
 /* Library                                                                */
@@ -159,6 +170,28 @@ int weno_sb_order1_dev(const weno_sb_grid *g, int dir, int dtype, const double *
 int weno_sb_weno_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, int dtype,
                      const void *v_in, const weno_sb_coefs *coefs, void *vL, void *vR,
                      void *stream);
+/* The same reconstruction for face-independent coefficients given on the
+ * host (MFC on a uniform grid; the harness's synthetic coefficients, which
+ * f90:256-277 fills identically for every face): the kernels take them from
+ * the kernel-parameter bank instead of per-thread registers.  The handle
+ * API uses this path by itself when the uploaded coefficient arrays are
+ * face-independent. */
+int weno_sb_weno_uniform_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, int dtype,
+                             const void *v_in, const weno_sb_face_coefs *face, void *vL, void *vR,
+                             void *stream);
+/* Adjoint (vector-Jacobian product) of one sweep -- no counterpart in the
+ * reference, which has no derivatives.  With the sweep's outputs
+ * (vL, vR) = F(v_in) for order 3/5/7, JS or TENO weights (the grid's
+ * scheme) and the MP limiter when flags has WENO_SB_F_MP, it computes
+ * gv = (dF/dv)^T (gL, gR), recomputing beta and the weights from v_in
+ * instead of storing them.  gL, gR have the face layout; v_in and gv the
+ * layout of v_rs_ws, or of v_vf with WENO_SB_F_FOLDED.  gv is overwritten
+ * (the cells no face reads get 0) unless WENO_SB_F_ACCUMULATE adds into it,
+ * so the three folded sweeps can sum into one gv.  Coefficients come either
+ * per face (coefs) or face-independent (face); pass exactly one.  FP64. */
+int weno_sb_vjp_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, const double *v_in,
+                    const weno_sb_coefs *coefs, const weno_sb_face_coefs *face, const double *gL,
+                    const double *gR, double *gv, void *stream);
 /* s_preserve_monotonicity (f90:1544-1615). */
 int weno_sb_preserve_monotonicity_dev(const weno_sb_grid *g, int dir, int dtype,
                                       const void *v_rs_ws, void *vL, void *vR, void *stream);
@@ -185,6 +218,33 @@ int weno_sb_checksum_dev(int dtype, const void *arr, int64_t n, void *scratch,
  * every partial it reads, so nothing needs clearing between calls. */
 int weno_sb_checksum_noalloc(int dtype, const void *const *arrays, const int64_t *n, int count,
                              double *d_results, void *stream);
+
+/* ===================================================================== */
+/* Batches of uneven blocks (no counterpart in the reference, which runs   */
+/* one block): one persistent launch, captured in a CUDA graph.            */
+/* ===================================================================== */
+typedef struct weno_sb_block {
+    weno_sb_grid grid;     /* this block's extents, v_size and weights      */
+    int32_t dir, order;    /* sweep direction 0/1/2, order 3/5/7            */
+    uint32_t flags;        /* WENO_SB_F_MP, WENO_SB_F_FOLDED                */
+    int32_t dtype;         /* WENO_SB_FP64, or WENO_SB_FP32: v_in, vL, vR are
+                              float (for a folded FP32 entry v_in is an FP32
+                              copy of v_vf)                                 */
+    const void *v_in;      /* v_rs_ws_dir, or v_vf with WENO_SB_F_FOLDED     */
+    weno_sb_coefs coefs;   /* per-face coefficient arrays (device)           */
+    void *vL, *vR;         /* face states (device)                           */
+} weno_sb_block;
+
+/* Validate the blocks and build the device work list (allocates). */
+int weno_sb_batch_create(const weno_sb_block *blocks, int n, int *batch);
+/* Time the candidate tile shapes (CTA width x columns per work item) on
+ * `stream` and keep the fastest; with WENO_SB_TUNE_CACHE naming a file,
+ * a batch of the same composition reuses the recorded choice. */
+int weno_sb_batch_autotune(int batch, void *stream, int *threads, int *cols_per_item, double *best_ms);
+/* Run every block's sweep: one graph launch (counter reset + persistent
+ * kernel), captured on first use. */
+int weno_sb_batch_launch(int batch, void *stream);
+int weno_sb_batch_destroy(int batch);
 
 /* ===================================================================== */
 /* Diagnostics (no counterpart in the reference; used by the test suite).  */

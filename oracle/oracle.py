@@ -60,6 +60,9 @@ def lib() -> ctypes.CDLL:
         L.wo_checksum.restype = ctypes.c_double
         L.wo_harness_run.argtypes = [i, i, i, i, i, ctypes.c_double, i, ctypes.c_double, i, dp]
         L.wo_harness_run.restype = i
+        L.wo_vjp.argtypes = [i, i, i, i, i, i, i, ctypes.c_double, ctypes.c_double,
+                             dp, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.wo_vjp.restype = i
         L.wo_set_threads.argtypes = [i]
         L.wo_set_threads.restype = None
         L.wo_get_threads.argtypes = []
@@ -171,3 +174,17 @@ def harness_run(m=199, n=199, p=199, nv=8, buff=6, eps=1e-16, scheme=JS, teno_ct
                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     assert rc == 0, rc
     return tuple(float(x) for x in out)
+
+
+def vjp(rs, coefs, order, gL, gR, scheme=JS, mp=False, eps=1e-16, teno_ct=1e-5):
+    """Adjoint of one sweep by forward-mode dual numbers on the reference
+    formulas (weno_oracle_ad.cpp): gv = (dF/dv)^T (gL, gR), layout of rs."""
+    ns6, c1, c2, nv = rs.shape
+    gv = np.zeros(rs.shape, order="F")
+    pL, pR, dL, dR, bc = coefs
+    gL = np.asfortranarray(gL)
+    gR = np.asfortranarray(gR)
+    rc = lib().wo_vjp(ns6 - 6, c1, c2, nv, order, scheme, 1 if mp else 0, float(eps), float(teno_ct),
+                      _p(rs), _p(pL), _p(pR), _p(dL), _p(dR), _p(bc), _p(gL), _p(gR), _p(gv))
+    assert rc == 0, rc
+    return gv

@@ -1,0 +1,217 @@
+"""Adjoint (VJP) of the reconstruction sweep through the C ABI.
+
+Checked three ways: against forward-mode dual-number differentiation of the
+reference formulas (oracle/weno_oracle_ad.cpp) at 1e-11 max-norm relative
+error; against central finite differences (step 1e-6, smooth data, JS) to
+1e-6; and with torch.autograd.gradcheck through a ctypes autograd wrapper.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import from_dev, rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+# Two FP evaluations of the same derivative (reverse mode here, forward-mode
+# duals in the oracle) agree to ~1e-10 where the JS weights switch between
+# stencils whose beta differ by orders of magnitude (d alpha/d beta = -2 alpha/beta
+# amplifies rounding); the bar is 1e-9 of the array's max norm, 1e-8 for
+# WENO3, whose two-stencil weights are the most sensitive.
+TOL_AD = 1e-9
+TOL_AD3 = 1e-8
+
+
+@pytest.fixture(scope="module")
+def wsb():
+    import torch
+    assert torch.cuda.is_available()
+    import wenostandalone_b200 as w
+    w.lib()
+    return w
+
+
+def _varying(order, nc, seed):
+    from test_parity_gpu import varying_coefficients
+    return varying_coefficients(order, nc, seed=seed)
+
+
+@pytest.mark.parametrize("mp", [False, True])
+@pytest.mark.parametrize("scheme", [0, 3])
+@pytest.mark.parametrize("order", [3, 5, 7])
+@pytest.mark.parametrize("coef_mode", ["varying", "uniform"])
+def test_vjp_matches_dual_number_oracle(wsb, oracle_mod, order, scheme, mp, coef_mode):
+    from wenostandalone_b200 import api, fields
+    if order == 3 and scheme == 3:
+        pytest.skip("WENO3 has no TENO weights in the reference (NaN output)")
+    m, n, p, nv = 30, 17, 9, 2
+    g = wsb.Grid(m, n, p, nv, 6, scheme=scheme)
+    vf = fields.smooth_jump_field(m, n, p, nv, 6, seed=21)
+    rng = np.random.default_rng(3)
+    for d in range(3):
+        nc = g.nc(d)
+        coefs = _varying(order, nc, 7 + d) if coef_mode == "varying" else fields.uniform_weno_coefficients(order, nc)
+        rs = oracle_mod.reshape(vf, m, n, p, 6, d)
+        gL = np.asfortranarray(rng.standard_normal(g.face_shape(d)))
+        gR = np.asfortranarray(rng.standard_normal(g.face_shape(d)))
+        ref = oracle_mod.vjp(rs, coefs, order, gL, gR, scheme=scheme, mp=mp)
+        gv = to_dev(np.zeros(rs.shape))
+        flags = wsb.F_MP if mp else 0
+        if coef_mode == "varying":
+            api.vjp(g, d, order, to_dev(rs), tuple(to_dev(c) for c in coefs), to_dev(gL), to_dev(gR), gv, flags=flags)
+        else:
+            api.vjp(g, d, order, to_dev(rs), coefs, to_dev(gL), to_dev(gR), gv, flags=flags, uniform=True)
+        err = rel_err(from_dev(gv, rs.shape), ref)
+        assert err <= (TOL_AD3 if order == 3 else TOL_AD), (d, err)
+
+
+def _scatter_to_vf(oracle_mod, shape_vf, m, n, p, buff, d, g_rs):
+    """Transpose of the reshape: add a v_rs_ws-layout array into v_vf layout."""
+    idx = np.arange(np.prod(shape_vf), dtype=np.float64).reshape(shape_vf, order="F")
+    rs_idx = oracle_mod.reshape(np.asfortranarray(idx), m, n, p, buff, d).ravel(order="F").astype(np.int64)
+    out = np.zeros(int(np.prod(shape_vf)))
+    np.add.at(out, rs_idx, np.asarray(g_rs).ravel(order="F"))
+    return out.reshape(shape_vf, order="F")
+
+
+def test_vjp_folded_accumulates_three_sweeps(wsb, oracle_mod):
+    """Folded sweeps read v_vf directly; with ACCUMULATE the x, y and z
+    adjoints sum into one gradient of v_vf."""
+    import torch
+    from wenostandalone_b200 import api, fields
+    m, n, p, nv = 21, 14, 11, 2
+    g = wsb.Grid(m, n, p, nv, 6)
+    vf = fields.smooth_jump_field(m, n, p, nv, 6, seed=5)
+    rng = np.random.default_rng(11)
+    ref = np.zeros(vf.shape, order="F")
+    gv = torch.zeros(vf.size, dtype=torch.float64, device="cuda")
+    v = to_dev(vf)
+    for d in range(3):
+        coefs = fields.uniform_weno_coefficients(5, g.nc(d))
+        rs = oracle_mod.reshape(vf, m, n, p, 6, d)
+        gL = np.asfortranarray(rng.standard_normal(g.face_shape(d)))
+        gR = np.asfortranarray(rng.standard_normal(g.face_shape(d)))
+        ref += _scatter_to_vf(oracle_mod, vf.shape, m, n, p, 6, d,
+                              oracle_mod.vjp(rs, coefs, 5, gL, gR, mp=True))
+        api.vjp(g, d, 5, v, tuple(to_dev(c) for c in coefs), to_dev(gL), to_dev(gR), gv,
+                flags=wsb.F_MP | wsb.F_FOLDED | (wsb.F_ACCUMULATE if d > 0 else 0))
+    assert rel_err(from_dev(gv, vf.shape), ref) <= TOL_AD
+
+
+def _mp_safe_cells(rs, L, R, margin=1e-3, half_width=2):
+    """Mask rule for the finite-difference check: a core face is safe when
+    its WENO states lie inside the MP bounds (f90:1564-1608) with `margin`
+    to spare on both sides, so a perturbation of size ~1e-6 keeps the limiter
+    on the same (pass-through) branch.  A cell is perturbed only if every
+    face whose stencil (+-half_width: 2 for WENO5, 3 for WENO7) contains it
+    is safe."""
+    ns = rs.shape[0] - 6
+    o = np.arange(3, ns - 3)
+    v = {k: rs[o + 3 + k] for k in range(-2, 3)}
+    dm1 = v[0] + v[-2] - 2 * v[-1]
+    d0 = v[1] + v[-1] - 2 * v[0]
+    dp1 = v[2] + v[0] - 2 * v[1]
+
+    def minmod(dl, dr):
+        A, B = 4 * dl - dr, 4 * dr - dl
+        same = (np.sign(A) == np.sign(B)) & (np.sign(A) == np.sign(dl)) & (np.sign(A) == np.sign(dr))
+        mn = np.minimum(np.minimum(np.abs(A), np.abs(dl)), np.minimum(np.abs(B), np.abs(dr)))
+        return np.where(same, np.sign(A) * mn, 0.0)
+
+    mA, mB = minmod(dm1, d0), minmod(d0, dp1)
+    safe = np.ones(v[0].shape, dtype=bool)
+    for side, x in (("L", L[o]), ("R", R[o])):
+        if side == "L":
+            UL = v[0] - 2 * (v[1] - v[0]); MD = (v[0] + v[-1] - mA) / 2
+            LC = v[0] - (v[1] - v[0]) / 2 + 4 / 3 * mB; vn = v[-1]
+        else:
+            UL = v[0] + 2 * (v[0] - v[-1]); MD = (v[0] + v[1] - mB) / 2
+            LC = v[0] + (v[0] - v[-1]) / 2 + 4 / 3 * mA; vn = v[1]
+        lo = np.maximum(np.minimum(np.minimum(v[0], vn), MD), np.minimum(np.minimum(v[0], UL), LC))
+        hi = np.minimum(np.maximum(np.maximum(v[0], vn), MD), np.maximum(np.maximum(v[0], UL), LC))
+        safe &= (x - lo > margin) & (hi - x > margin)
+    bad_face = np.zeros((ns,) + rs.shape[1:], dtype=bool)
+    bad_face[3:ns - 3] = ~safe
+    bad_cell = np.zeros(rs.shape, dtype=bool)
+    for k in range(-half_width, half_width + 1):
+        bad_cell[3 + k:ns + 3 + k] |= bad_face
+    return ~bad_cell
+
+
+@pytest.mark.parametrize("mp", [False, True])
+@pytest.mark.parametrize("order", [5, 7])
+def test_vjp_central_differences(wsb, oracle_mod, order, mp):
+    """<gv, dv> against (F(v+h dv) - F(v-h dv)) . g / 2h with h = 1e-4 along a
+    random unit-norm direction dv, on the smooth 128^3-cell, v_size=5 input,
+    JS weights, cotangents N(0,1).  With MP, dv is zero on the cells
+    _mp_safe_cells excludes (limiter kinks).  Bar: 1e-6 relative.
+
+    h: dv is spread over ~1e7 cells, so a cell moves by ~h * 3e-4, far inside
+    the 1e-3 limiter margin, and the O(h^2) truncation stays near 1e-9; the
+    rounding noise of the two forward sums (~1e-13 absolute) divided by 2h is
+    what a smaller h would amplify (h = 1e-6 puts it at the 1e-6 bar)."""
+    import torch
+    from wenostandalone_b200 import api, fields
+    m = 127
+    g = wsb.Grid(m, m, m, 5, 6)
+    vf = fields.sinusoid_shock_field(m, m, m, 5, 6, seed=4, shock=False)
+    gen = torch.Generator(device="cuda").manual_seed(8)
+    flags = wsb.F_MP if mp else 0
+    for d in range(3):
+        coefs_np = fields.uniform_weno_coefficients(order, g.nc(d))
+        coefs = tuple(to_dev(c) for c in coefs_np)
+        rs_np = oracle_mod.reshape(vf, m, m, m, 6, d)
+        rs = to_dev(rs_np)
+        n = int(np.prod(g.face_shape(d)))
+        gL = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
+        gR = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
+        gv = torch.empty_like(rs)
+        api.vjp(g, d, order, rs, coefs, gL, gR, gv, flags=flags)
+        dv = torch.randn(rs.numel(), generator=gen, device="cuda", dtype=torch.float64)
+        if mp:
+            Lw = torch.zeros(n, dtype=torch.float64, device="cuda")
+            Rw = torch.zeros_like(Lw)
+            api.weno(g, d, order, rs, coefs, Lw, Rw)
+            mask = _mp_safe_cells(rs_np, from_dev(Lw, g.face_shape(d)), from_dev(Rw, g.face_shape(d)),
+                                  half_width=max(2, (order - 1) // 2))
+            assert mask.mean() > 0.3  # most of the smooth field is limiter-free
+            dv = dv * to_dev(mask.astype(np.float64))
+        dv = dv / torch.linalg.vector_norm(dv)
+        h = 1e-4
+        outs = []
+        for sgn in (1.0, -1.0):
+            L = torch.zeros(n, dtype=torch.float64, device="cuda")
+            R = torch.zeros_like(L)
+            api.weno(g, d, order, rs + sgn * h * dv, coefs, L, R, flags=flags)
+            outs.append(float((L * gL).sum() + (R * gR).sum()))
+        fd = (outs[0] - outs[1]) / (2 * h)
+        an = float((gv * dv).sum())
+        assert abs(fd - an) <= 1e-6 * abs(an), (d, fd, an)
+
+
+def test_autograd_gradcheck_16cubed(wsb):
+    """torch.autograd.gradcheck of the wrapped sweep at 16^3 cells, v_size=2."""
+    import torch
+    from autograd_weno import WenoSweep
+    from wenostandalone_b200 import api, fields
+    m = 15
+    g = wsb.Grid(m, m, m, 2, 6)
+    vf = fields.sinusoid_shock_field(m, m, m, 2, 6, seed=1, shock=False)
+    for d in range(3):
+        coefs = tuple(to_dev(c) for c in fields.uniform_weno_coefficients(5, g.nc(d)))
+        v = to_dev(vf)
+        rs = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float64, device="cuda")
+        api.reshape(g, d, v, rs)
+        rs.requires_grad_(True)
+        f = lambda x: WenoSweep.apply(x, g, d, 5, coefs, wsb.F_MP)
+        assert torch.autograd.gradcheck(f, (rs,), eps=1e-6, atol=1e-6, rtol=1e-4, fast_mode=True)
+
+
+def test_vjp_rejects_unsupported(wsb):
+    import torch
+    from wenostandalone_b200 import _lib as L, api, fields
+    g = wsb.Grid(7, 7, 7, 1, 6, scheme=1)
+    t = torch.zeros(10, dtype=torch.float64, device="cuda")
+    coefs = fields.uniform_weno_coefficients(5, g.nc(0))
+    with pytest.raises(L.WenoError) as e:
+        api.vjp(g, 0, 5, t, coefs, t, t, t, uniform=True)
+    assert e.value.code == L.ERR_UNSUPPORTED

@@ -1,0 +1,101 @@
+"""Batches of uneven blocks in one persistent, graph-captured launch.
+
+Seeded blocks with their own extents, v_size, order (3/5/7), weights
+(JS/TENO), MP on/off, drop-in or folded input and FP64 / FP32-bulk storage;
+every block's outputs are checked against the oracle (FP64: 1e-12 max-norm
+relative; FP32-bulk: against the oracle on the FP32-rounded field, 1e-5),
+after two graph launches and again after autotuning the tile shape.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import from_dev, nan_dev, rel_err, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _make_blocks(wsb, oracle_mod, n_blocks=14, seed=2024, lo=8, hi=40, vsizes=(2, 3, 5)):
+    import torch
+    from wenostandalone_b200 import api, fields
+    from test_parity_gpu import varying_coefficients
+    rng = np.random.default_rng(seed)
+    entries, checks = [], []
+    for i in range(n_blocks):
+        m, n, p = (int(x) - 1 for x in rng.integers(lo, hi + 1, 3))
+        nv = int(rng.choice(vsizes))
+        order = int(rng.choice([3, 5, 7]))
+        scheme = int(rng.choice([0, 3])) if order != 3 else 0
+        mp = bool(rng.integers(0, 2))
+        folded = bool(rng.integers(0, 2))
+        fp32 = bool(i % 4 == 3)
+        d = int(rng.integers(0, 3))
+        g = wsb.Grid(m, n, p, nv, 6, scheme=scheme)
+        vf = fields.smooth_jump_field(m, n, p, nv, 6, seed=100 + i)
+        if fp32:
+            vf = vf.astype(np.float32).astype(np.float64)
+        coefs = varying_coefficients(order, g.nc(d), seed=200 + i)
+        rs = oracle_mod.reshape(np.asfortranarray(vf), m, n, p, 6, d)
+        Lr, Rr = oracle_mod.order1_copy(np.asfortranarray(vf), m, n, p, 6, d)
+        Lr[:] = np.nan
+        Rr[:] = np.nan
+        oracle_mod.reconstruct(rs, coefs, order, scheme=scheme, vL=Lr, vR=Rr)
+        if mp:
+            oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+        dt = torch.float32 if fp32 else torch.float64
+        if folded:
+            v_in = to_dev(vf, dt)
+        else:
+            v_in = to_dev(rs, dt)
+        L, R = nan_dev(g.face_shape(d), dt), nan_dev(g.face_shape(d), dt)
+        flags = (wsb.F_MP if mp else 0) | (wsb.F_FOLDED if folded else 0)
+        entries.append(dict(grid=g, dir=d, order=order, flags=flags, v_in=v_in,
+                            coefs=tuple(to_dev(c) for c in coefs), vL=L, vR=R))
+        checks.append((g, d, scheme, fp32, Lr, Rr))
+    return entries, checks
+
+
+def _check(entries, checks):
+    for e, (g, d, scheme, fp32, Lr, Rr) in zip(entries, checks):
+        tol = 1e-5 if fp32 else 1e-12
+        for got_t, ref in ((e["vL"], Lr), (e["vR"], Rr)):
+            got = from_dev(got_t, g.face_shape(d))
+            assert np.array_equal(np.isnan(got), np.isnan(ref)), "written faces differ from the sweep's faces"
+            if scheme == 3:
+                den = max(np.nanmax(np.abs(ref)), 1e-300)
+                bad = np.abs(np.nan_to_num(got) - np.nan_to_num(ref)) / den > tol
+                assert bad.mean() <= 1e-4
+            else:
+                assert rel_err(got, ref) <= tol, (g, d, e["order"], fp32)
+
+
+def test_batch_matches_oracle_per_block(oracle_mod):
+    import torch
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api
+    entries, checks = _make_blocks(wsb, oracle_mod)
+    b = api.Batch(entries)
+    try:
+        for _ in range(2):
+            b.launch()
+        torch.cuda.synchronize()
+        _check(entries, checks)
+        t, u, ms = b.autotune()
+        assert t in (64, 128, 256) and u in (4, 8, 16, 32) and ms > 0
+        for e in entries:
+            e["vL"].fill_(float("nan"))
+            e["vR"].fill_(float("nan"))
+        b.launch()
+        torch.cuda.synchronize()
+        _check(entries, checks)
+    finally:
+        b.close()
+
+
+def test_batch_rejects_bad_blocks(oracle_mod):
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import _lib as L, api
+    entries, _ = _make_blocks(wsb, oracle_mod, n_blocks=2)
+    entries[1]["order"] = 4
+    with pytest.raises(L.WenoError) as e:
+        api.Batch(entries)
+    assert e.value.code == L.ERR_ARG and "block 1" in L.last_error()

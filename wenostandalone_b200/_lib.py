@@ -27,7 +27,7 @@ JS, MAPPED, Z, TENO, NONE = 0, 1, 2, 3, 4
 # storage precision
 FP64, FP32 = 0, 1
 # flags
-F_SPLIT, F_SPECIALIZED, F_MP, F_FOLDED = 1, 2, 4, 8
+F_SPLIT, F_SPECIALIZED, F_MP, F_FOLDED, F_ACCUMULATE = 1, 2, 4, 8, 16
 
 # array ids of the handle API
 A_V_VF = 0
@@ -52,9 +52,10 @@ EXPORTED = [
     "weno_sb_array_info", "weno_sb_initialize_weno", "weno_sb_weno",
     "weno_sb_preserve_monotonicity", "weno_sb_checksum", "weno_sb_sync",
     "weno_sb_stream", "weno_sb_reshape_dev", "weno_sb_order1_dev",
-    "weno_sb_weno_dev", "weno_sb_preserve_monotonicity_dev",
+    "weno_sb_weno_dev", "weno_sb_weno_uniform_dev", "weno_sb_vjp_dev", "weno_sb_preserve_monotonicity_dev",
     "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev", "weno_sb_check_device",
     "weno_sb_selftest_rcp", "weno_sb_selftest_timeout", "weno_sb_checksum_noalloc",
+    "weno_sb_batch_create", "weno_sb_batch_autotune", "weno_sb_batch_launch", "weno_sb_batch_destroy",
 ]
 
 
@@ -71,6 +72,21 @@ class WenoCoefs(ctypes.Structure):
     """struct weno_sb_coefs: device pointers of one direction's coefficients."""
     _fields_ = [("polyL", ctypes.c_void_p), ("polyR", ctypes.c_void_p), ("dL", ctypes.c_void_p),
                 ("dR", ctypes.c_void_p), ("beta_coef", ctypes.c_void_p)]
+
+
+class WenoFaceCoefs(ctypes.Structure):
+    """struct weno_sb_face_coefs: one face's coefficients on the host,
+    index order [s][r] (polyL(j,r,s) -> polyL[s][r])."""
+    _fields_ = [("polyL", (ctypes.c_double * 5) * 3), ("polyR", (ctypes.c_double * 5) * 3),
+                ("dL", ctypes.c_double * 5), ("dR", ctypes.c_double * 5),
+                ("beta_coef", (ctypes.c_double * 5) * 6)]
+
+
+class WenoBlock(ctypes.Structure):
+    """struct weno_sb_block: one entry of a batch."""
+    _fields_ = [("grid", WenoGrid), ("dir", ctypes.c_int32), ("order", ctypes.c_int32),
+                ("flags", ctypes.c_uint32), ("dtype", ctypes.c_int32), ("v_in", ctypes.c_void_p),
+                ("coefs", WenoCoefs), ("vL", ctypes.c_void_p), ("vR", ctypes.c_void_p)]
 
 
 class WenoError(RuntimeError):
@@ -113,6 +129,9 @@ def lib() -> ctypes.CDLL:
         "weno_sb_reshape_dev": ([gp, i32, i32, vp, vp, vp], i32),
         "weno_sb_order1_dev": ([gp, i32, i32, vp, vp, vp, vp], i32),
         "weno_sb_weno_dev": ([gp, i32, i32, u32, i32, vp, ctypes.POINTER(WenoCoefs), vp, vp, vp], i32),
+        "weno_sb_weno_uniform_dev": ([gp, i32, i32, u32, i32, vp, ctypes.POINTER(WenoFaceCoefs), vp, vp, vp], i32),
+        "weno_sb_vjp_dev": ([gp, i32, i32, u32, vp, ctypes.POINTER(WenoCoefs), ctypes.POINTER(WenoFaceCoefs),
+                             vp, vp, vp, vp], i32),
         "weno_sb_preserve_monotonicity_dev": ([gp, i32, i32, vp, vp, vp, vp], i32),
         "weno_sb_checksum_scratch_bytes": ([ctypes.c_int64], ctypes.c_size_t),
         "weno_sb_checksum_dev": ([i32, vp, ctypes.c_int64, vp, vp, vp], i32),
@@ -120,6 +139,11 @@ def lib() -> ctypes.CDLL:
         "weno_sb_selftest_rcp": ([vp, vp, vp, ctypes.c_int64, vp], i32),
         "weno_sb_selftest_timeout": ([ctypes.c_int64, vp], i32),
         "weno_sb_checksum_noalloc": ([i32, ctypes.POINTER(ctypes.c_void_p), i64p, i32, vp, vp], i32),
+        "weno_sb_batch_create": ([ctypes.POINTER(WenoBlock), i32, ctypes.POINTER(ctypes.c_int)], i32),
+        "weno_sb_batch_autotune": ([i32, vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_double)], i32),
+        "weno_sb_batch_launch": ([i32, vp], i32),
+        "weno_sb_batch_destroy": ([i32], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

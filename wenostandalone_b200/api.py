@@ -220,6 +220,47 @@ def weno(grid: Grid, d: int, order: int, v_in, coefs, vL, vR, flags: int = 0, st
                                  ctypes.byref(cs), _ptr(vL), _ptr(vR), _stream(stream)))
 
 
+def face_coefs(coefs, face: int = 0) -> L.WenoFaceCoefs:
+    """One face's coefficients (from numpy arrays in the harness layouts) as
+    the weno_sb_face_coefs struct."""
+    pL, pR, dL, dR, bc = (np.asarray(c) for c in coefs)
+    f = L.WenoFaceCoefs()
+    for s in range(3):
+        for r in range(5):
+            f.polyL[s][r] = float(pL[face, r, s])
+            f.polyR[s][r] = float(pR[face, r, s])
+    for r in range(5):
+        f.dL[r] = float(dL[r, face])
+        f.dR[r] = float(dR[r, face])
+    for s in range(6):
+        for r in range(5):
+            f.beta_coef[s][r] = float(bc[face, r, s])
+    return f
+
+
+def weno_uniform(grid: Grid, d: int, order: int, v_in, face, vL, vR, flags: int = 0, stream=None) -> None:
+    """Reconstruction with face-independent coefficients (`face`: a
+    WenoFaceCoefs, or numpy coefficient arrays whose face 0 is used)."""
+    f = face if isinstance(face, L.WenoFaceCoefs) else face_coefs(face)
+    check(lib().weno_sb_weno_uniform_dev(ctypes.byref(grid.c()), d, order, flags, _dtype_of(vL), _ptr(v_in),
+                                         ctypes.byref(f), _ptr(vL), _ptr(vR), _stream(stream)))
+
+
+def vjp(grid: Grid, d: int, order: int, v_in, coefs, gL, gR, gv, flags: int = 0, stream=None,
+        uniform: bool = False) -> None:
+    """Adjoint of one sweep: gv = (dF/dv)^T (gL, gR).  `coefs`: device
+    coefficient tensors (per face), or with uniform=True numpy arrays /
+    a WenoFaceCoefs whose face 0 applies to every face."""
+    if uniform:
+        f = coefs if isinstance(coefs, L.WenoFaceCoefs) else face_coefs(coefs)
+        cs, fp = None, ctypes.byref(f)
+    else:
+        cs = coefs if isinstance(coefs, L.WenoCoefs) else coefs_struct(coefs)
+        cs, fp = ctypes.byref(cs), None
+    check(lib().weno_sb_vjp_dev(ctypes.byref(grid.c()), d, order, flags, _ptr(v_in), cs, fp, _ptr(gL), _ptr(gR),
+                                _ptr(gv), _stream(stream)))
+
+
 def preserve_monotonicity(grid: Grid, d: int, v_rs_ws, vL, vR, stream=None) -> None:
     check(lib().weno_sb_preserve_monotonicity_dev(ctypes.byref(grid.c()), d, _dtype_of(vL), _ptr(v_rs_ws),
                                                   _ptr(vL), _ptr(vR), _stream(stream)))
@@ -233,3 +274,53 @@ def checksum(arr, stream=None) -> float:
     check(lib().weno_sb_checksum_dev(_dtype_of(arr), _ptr(arr), arr.numel(), _ptr(scratch), _ptr(res),
                                      _stream(stream)))
     return float(res.item())
+
+
+class Batch:
+    """Many uneven blocks' sweeps in one persistent, graph-captured launch.
+
+    `entries`: sequence of dicts with keys grid (Grid), dir, order, flags,
+    v_in, coefs (5 device tensors), vL, vR (CUDA tensors; float32 tensors
+    select FP32-bulk storage)."""
+
+    def __init__(self, entries):
+        import torch
+        n = len(entries)
+        arr = (L.WenoBlock * n)()
+        self._keep = []
+        for i, e in enumerate(entries):
+            b = arr[i]
+            b.grid = e["grid"].c()
+            b.dir = e["dir"]
+            b.order = e["order"]
+            b.flags = e.get("flags", 0)
+            b.dtype = L.FP32 if e["vL"].dtype == torch.float32 else L.FP64
+            b.v_in = _ptr(e["v_in"])
+            b.coefs = coefs_struct(e["coefs"])
+            b.vL = _ptr(e["vL"])
+            b.vR = _ptr(e["vR"])
+            self._keep.append(e)
+        h = ctypes.c_int(0)
+        check(lib().weno_sb_batch_create(arr, n, ctypes.byref(h)))
+        self.handle = h.value
+
+    def autotune(self, stream=None):
+        t, u, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(lib().weno_sb_batch_autotune(self.handle, _stream(stream), ctypes.byref(t), ctypes.byref(u),
+                                           ctypes.byref(ms)))
+        return t.value, u.value, ms.value
+
+    def launch(self, stream=None):
+        check(lib().weno_sb_batch_launch(self.handle, _stream(stream)))
+
+    def close(self):
+        if self.handle:
+            check(lib().weno_sb_batch_destroy(self.handle))
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib().weno_sb_batch_destroy(self.handle)
+        except Exception:
+            pass

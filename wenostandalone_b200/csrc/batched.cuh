@@ -1,0 +1,142 @@
+// batched.cuh -- many uneven blocks in one persistent launch.
+//
+// Each batch entry is one sweep of one block (its own extents, v_size,
+// order 3/5/7, JS or TENO weights, MP on/off, FP64 or FP32-bulk storage,
+// drop-in or folded input).  The entries are cut into work items
+// (entry, face tile, group of U columns); a persistent grid of CTAs takes
+// items from a global atomic counter until the list is exhausted, so large
+// and small blocks share the GPU without one launch per block and without
+// a tail of idle SMs.  Nothing waits on another CTA: a CTA that finds the
+// counter past the end simply exits.
+//
+// Inside an item, thread f owns face f of the tile, loads that face's
+// coefficients once for the item and reads its stencil straight from
+// global memory (the tile's columns are contiguous along the sweep for the
+// drop-in layout and for x; L1 serves the overlap of neighbouring faces).
+#pragma once
+
+#include "weno_math.cuh"
+#include "sweep_generic.cuh"
+
+namespace wsb {
+
+struct BatchEntry {
+    SweepGeom g;        // extents and input strides (drop-in or folded)
+    const void* in;
+    void* vL;
+    void* vR;
+    CoefPtrs cp;
+    WenoParams wp;
+    int order;          // 3, 5, 7
+    int mp;             // fused MP limiter
+    int fp32;           // FP32-bulk storage (input and face states are float)
+    int o_first, nf;    // faces handled
+    int n_jt;           // face tiles
+    int TJ;             // faces per tile (<= blockDim.x)
+    long long n_groups; // column groups of U columns
+    long long item0;    // first work item of this entry
+};
+
+template <int ORDER, typename T>
+__device__ __forceinline__ void batch_item(const BatchEntry& e, long long grp, int jt, int U) {
+    const int f = threadIdx.x;
+    if (f >= e.TJ) return;
+    const int fi = jt * e.TJ + f;
+    if (fi >= e.nf) return;
+    const long long o = e.o_first + fi;
+    long long c = o - 3;
+    c = c < 0 ? 0 : (c > e.g.nc - 1 ? e.g.nc - 1 : c);
+    Coef<ORDER> cf;
+    cf.load(e.cp.polyL, e.cp.polyR, e.cp.dL, e.cp.dR, e.cp.beta, e.g.nc, c);
+    const T* __restrict__ in = (const T*)e.in;
+    T* __restrict__ vL = (T*)e.vL;
+    T* __restrict__ vR = (T*)e.vR;
+    const long long col0 = grp * U;
+    const long long col1 = min(col0 + U, e.g.cols);
+    for (long long col = col0; col < col1; ++col) {
+        const long long a = col % e.g.c1;
+        const long long t = col / e.g.c1;
+        const long long b = t % e.g.c2;
+        const long long v = t / e.g.c2;
+        const T* __restrict__ p = in + e.g.in_off + (o + 3) * e.g.sJ + a * e.g.sA + b * e.g.sB + v * e.g.sV;
+        const long long oi = o + e.g.ns * col;
+        const long long sJ = e.g.sJ;
+        T Lt, Rt;
+        if constexpr (ORDER == 3) {
+            double L, R;
+            weno3_face((double)__ldg(p - sJ), (double)__ldg(p), (double)__ldg(p + sJ), cf, e.wp.scheme, e.wp.eps, L,
+                       R);
+            Lt = (T)L;
+            Rt = (T)R;
+            if (e.mp && o >= 3 && o <= e.g.ns - 4)
+                MP<T>::apply(__ldg(p - 2 * sJ), __ldg(p - sJ), __ldg(p), __ldg(p + sJ), __ldg(p + 2 * sJ), Lt, Rt);
+        } else if constexpr (ORDER == 5) {
+            const T m2 = __ldg(p - 2 * sJ), m1 = __ldg(p - sJ), z0 = __ldg(p), p1 = __ldg(p + sJ), p2 = __ldg(p + 2 * sJ);
+            double L, R;
+            weno5_face<T>((double)m2, (double)m1, (double)z0, (double)p1, (double)p2, cf, e.wp.scheme, e.wp.eps,
+                          e.wp.teno_ct, L, R);
+            Lt = (T)L;
+            Rt = (T)R;
+            if (e.mp) MP<T>::apply(m2, m1, z0, p1, p2, Lt, Rt);
+        } else {
+            double s7[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) s7[q] = (double)__ldg(p + (q - 3) * sJ);
+            double L, R;
+            weno7_face<T>(s7 + 3, cf, e.wp.scheme, e.wp.eps, e.wp.teno_ct, L, R);
+            Lt = (T)L;
+            Rt = (T)R;
+            if (e.mp) MP<T>::apply(__ldg(p - 2 * sJ), __ldg(p - sJ), __ldg(p), __ldg(p + sJ), __ldg(p + 2 * sJ), Lt, Rt);
+        }
+        vL[oi] = Lt;
+        vR[oi] = Rt;
+    }
+}
+
+// Persistent kernel: CTAs take items from *counter until n_items.
+__global__ void __launch_bounds__(256, 1)
+    batch_kernel(const BatchEntry* __restrict__ entries, int n_entries, long long n_items,
+                 unsigned long long* __restrict__ counter, int U) {
+    __shared__ long long s_item;
+    __shared__ int s_entry;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const long long it = (long long)atomicAdd(counter, 1ull);
+            s_item = it;
+            // entry of this item: entries are sorted by item0 (binary search)
+            int lo = 0, hi = n_entries - 1;
+            if (it < n_items) {
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (entries[mid].item0 <= it) lo = mid;
+                    else hi = mid - 1;
+                }
+            }
+            s_entry = lo;
+        }
+        __syncthreads();
+        const long long it = s_item;
+        const int ei = s_entry;
+        __syncthreads();
+        if (it >= n_items) break;
+        const BatchEntry& e = entries[ei];
+        const long long local = it - e.item0;
+        const int jt = (int)(local % e.n_jt);
+        const long long grp = local / e.n_jt;
+        if (e.fp32) {
+            switch (e.order) {
+                case 3: batch_item<3, float>(e, grp, jt, U); break;
+                case 5: batch_item<5, float>(e, grp, jt, U); break;
+                default: batch_item<7, float>(e, grp, jt, U); break;
+            }
+        } else {
+            switch (e.order) {
+                case 3: batch_item<3, double>(e, grp, jt, U); break;
+                case 5: batch_item<5, double>(e, grp, jt, U); break;
+                default: batch_item<7, double>(e, grp, jt, U); break;
+            }
+        }
+    }
+}
+
+}  // namespace wsb

@@ -29,6 +29,12 @@ struct WenoParams {
     double eps, teno_ct;
 };
 
+// Face-independent coefficients passed by value (laid out as Coef<ORDER>);
+// used when the coefficient pointers are null.
+struct UniCoefs {
+    double v[56];
+};
+
 template <typename T>
 __device__ __forceinline__ double ld(const T* p) { return (double)__ldg(p); }
 
@@ -36,7 +42,7 @@ __device__ __forceinline__ double ld(const T* p) { return (double)__ldg(p); }
 template <int ORDER, bool MPF, typename T>
 __global__ void __launch_bounds__(128) sweep_generic_kernel(SweepGeom g, const T* __restrict__ in,
                                                             T* __restrict__ vL, T* __restrict__ vR,
-                                                            CoefPtrs cp, WenoParams wp) {
+                                                            CoefPtrs cp, WenoParams wp, const UniCoefs uc) {
     using PT = T;  // polynomial sums in the storage precision
     const long long o0 = (ORDER == 3) ? 0 : 3;
     const long long nf = (ORDER == 3) ? g.ns : g.nc;
@@ -47,7 +53,10 @@ __global__ void __launch_bounds__(128) sweep_generic_kernel(SweepGeom g, const T
     c = c < 0 ? 0 : (c > g.nc - 1 ? g.nc - 1 : c);
 
     Coef<(ORDER == 0 ? 3 : ORDER)> cf;
-    if constexpr (ORDER != 0) cf.load(cp.polyL, cp.polyR, cp.dL, cp.dR, cp.beta, g.nc, c);
+    if constexpr (ORDER != 0) {
+        if (cp.polyL) cf.load(cp.polyL, cp.polyR, cp.dL, cp.dR, cp.beta, g.nc, c);
+        else cf = *reinterpret_cast<const Coef<ORDER>*>(uc.v);
+    }
 
     for (long long col = blockIdx.y; col < g.cols; col += gridDim.y) {
         const long long a = col % g.c1;

@@ -34,6 +34,24 @@ namespace wsb {
 
 __device__ int g_wsb_device_error = 0;
 
+// Tuning: CTAs per SM the FP64 WENO3/5 pipeline kernels are compiled for
+// (register cap 65536 / (256 * this)), and whether WENO5-JS with
+// face-independent coefficients processes two columns per iteration.
+#ifndef WSB_PIPE_MIN_BLOCKS
+#define WSB_PIPE_MIN_BLOCKS 2
+#endif
+#ifndef WSB_PIPE_PAIRS
+#define WSB_PIPE_PAIRS 1
+#endif
+// Stage-ring depths of the row-tile (KIND 0) and swizzled column-tile
+// (KIND 1) instances of WENO3/5; WENO7 keeps 6 / 3 (one CTA per SM).
+#ifndef WSB_PIPE_STAGES0
+#define WSB_PIPE_STAGES0 6
+#endif
+#ifndef WSB_PIPE_STAGES1
+#define WSB_PIPE_STAGES1 3
+#endif
+
 constexpr long long kWaitLimitCycles = 2000000000LL;  // ~1 s at 2 GHz
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -52,20 +70,29 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, u
                  : "memory");
 }
 
-// Bounded wait for the phase with parity `parity` to complete.
+__device__ __forceinline__ bool mbar_try(unsigned addr, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with parity `parity` to complete.  The clock
+// is read once every 16 polls; `backoff_ns` > 0 sleeps between polls (the
+// producer uses it, since it has STAGES-1 stages of slack and would
+// otherwise take issue slots from the consumer warps).
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity,
-                                          long long limit = kWaitLimitCycles) {
+                                          long long limit = kWaitLimitCycles, unsigned backoff_ns = 0) {
     const unsigned addr = smem_u32(bar);
+    if (mbar_try(addr, parity)) return true;
     const long long t0 = clock64();
-    while (true) {
-        unsigned ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if (clock64() - t0 > limit) {
+    for (unsigned it = 1;; ++it) {
+        if (backoff_ns) __nanosleep(backoff_ns);
+        if (mbar_try(addr, parity)) return true;
+        if ((it & 15u) == 0 && clock64() - t0 > limit) {
             atomicExch(&g_wsb_device_error, 1005 /* WENO_SB_ERR_TIMEOUT */);
             return false;
         }
@@ -92,14 +119,17 @@ struct PipeArgs {
     int dir;
 };
 
-template <int ORDER, bool MPF, int KIND, int STAGES, int SCH>
-__global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2))
+template <int ORDER, bool MPF, int KIND, int STAGES, int SCH, bool UNI>
+__global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : WSB_PIPE_MIN_BLOCKS))
     sweep_pipe_kernel(const __grid_constant__ CUtensorMap tmap, const PipeArgs P) {
     using T = double;
     const FastArgs& a = P.a;
     extern __shared__ __align__(1024) unsigned char smem_pipe[];
-    // 1024-byte aligned stage ring, then the barriers
-    unsigned char* ring = (unsigned char*)(((uintptr_t)smem_pipe + 1023) & ~(uintptr_t)1023);
+    // 1024-byte aligned stage ring, then the barriers.  The ring pointer is
+    // formed by indexing the shared array (not through an integer cast) so
+    // the compiler keeps it in the shared window and emits LDS, not generic
+    // loads.
+    unsigned char* ring = smem_pipe + ((1024u - (smem_u32(smem_pipe) & 1023u)) & 1023u);
     unsigned long long* full = (unsigned long long*)(ring + (size_t)STAGES * P.stage_bytes);
     unsigned long long* empty = full + STAGES;
     constexpr int H = Halo<ORDER, MPF>::H;
@@ -131,7 +161,7 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2))
         int i = 0;
         for (long long g = g0; g < a.n_groups; g += gstep, ++i) {
             const int s = i % STAGES;
-            if (i >= STAGES && !mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1)) return;
+            if (i >= STAGES && !mbar_wait(&empty[s], ((i / STAGES) & 1) ^ 1, kWaitLimitCycles, 256)) return;
             // group -> (u tile, w, v)
             const unsigned gg = (unsigned)g;
             const unsigned ut = gg % (unsigned)a.n_ut;
@@ -164,8 +194,12 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2))
     const long long o = o_begin + f;
     long long cidx = o - 3;
     cidx = cidx < 0 ? 0 : (cidx > a.nc - 1 ? a.nc - 1 : cidx);
-    Coef<ORDER> cf;
-    if (active) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
+    Coef<ORDER> cfr;
+    if constexpr (!UNI) {
+        if (active) cfr.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
+    }
+    const Coef<ORDER>& cf = UNI ? *reinterpret_cast<const Coef<ORDER>*>(a.ucf) : cfr;
+    constexpr bool PAIRS = WSB_PIPE_PAIRS && (ORDER == 5 && SCH == 0 && UNI);  // needs the registers UNI frees
 
     int i = 0;
     for (long long g = g0; g < a.n_groups; g += gstep, ++i) {
@@ -183,14 +217,20 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2))
                 const int ucnt = min(a.U, a.Nu - u0);
                 const LinearTile<T> tile{(const T*)st + (f + H + P.off), 1, P.SWp};
                 const long long oidx0 = (long long)u0 * a.o_sU + w * a.o_sW + v * a.o_sV + o;
-                compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, 0, ucnt, oidx0, o);
+                if constexpr (PAIRS)
+                    compute_js5_pairs<MPF>(a, *reinterpret_cast<const Coef<5>*>(&cf), tile, 0, ucnt, oidx0);
+                else
+                    compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, 0, ucnt, oidx0, o);
             } else {
                 const int u0 = (int)ut * 16 - 1;  // u of tile column 0
                 const int kb = (u0 < 0) ? 1 : 0;
                 const int ke = min(16, a.Nu - u0);
                 const Swz128Tile<T> tile{st, f + H};
                 const long long oidx0 = (long long)u0 * a.o_sU + w * a.o_sW + v * a.o_sV + o;
-                compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, kb, ke, oidx0, o);
+                if constexpr (PAIRS)
+                    compute_js5_pairs<MPF>(a, *reinterpret_cast<const Coef<5>*>(&cf), tile, kb, ke, oidx0);
+                else
+                    compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, kb, ke, oidx0, o);
             }
         }
         __syncwarp();
@@ -228,12 +268,12 @@ inline int sweep_path_override() {
     return 0;
 }
 
-template <int ORDER, bool MPF, int KIND, int STAGES, int SCH>
+template <int ORDER, bool MPF, int KIND, int STAGES, int SCH, bool UNI>
 int launch_pipe_s(const CUtensorMap& map, PipeArgs P, cudaStream_t st, int sms) {
     const int cons = (P.a.TJ + 31) / 32;
     const int threads = (cons + 1) * 32;
     const size_t smem = 1024 + (size_t)STAGES * P.stage_bytes + 2 * STAGES * sizeof(unsigned long long);
-    auto kfn = sweep_pipe_kernel<ORDER, MPF, KIND, STAGES, SCH>;
+    auto kfn = sweep_pipe_kernel<ORDER, MPF, KIND, STAGES, SCH, UNI>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
@@ -251,14 +291,18 @@ int launch_pipe_s(const CUtensorMap& map, PipeArgs P, cudaStream_t st, int sms) 
 
 template <int ORDER, bool MPF, int KIND, int STAGES>
 int launch_pipe_t(const CUtensorMap& map, PipeArgs P, cudaStream_t st, int sms) {
-    if (P.a.wp.scheme == JS) return launch_pipe_s<ORDER, MPF, KIND, STAGES, 0>(map, P, st, sms);
-    return launch_pipe_s<ORDER, MPF, KIND, STAGES, -1>(map, P, st, sms);
+    const bool uni = P.a.cp.polyL == nullptr;  // face-independent coefficients in P.a.ucf
+    if (P.a.wp.scheme == JS)
+        return uni ? launch_pipe_s<ORDER, MPF, KIND, STAGES, 0, true>(map, P, st, sms)
+                   : launch_pipe_s<ORDER, MPF, KIND, STAGES, 0, false>(map, P, st, sms);
+    return uni ? launch_pipe_s<ORDER, MPF, KIND, STAGES, -1, true>(map, P, st, sms)
+               : launch_pipe_s<ORDER, MPF, KIND, STAGES, -1, false>(map, P, st, sms);
 }
 
 // FP64 TMA sweep when the layout allows it; 1003 (unsupported) otherwise.
 inline int launch_pipe_sweep(const long long E[3], const SweepGeom& g, int dir, bool folded, int order, bool mp,
                              const double* in, double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp,
-                             cudaStream_t st, int sms) {
+                             cudaStream_t st, int sms, const double* ucf = nullptr) {
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return 1003;
     if (((uintptr_t)in & 15) != 0) return 1003;
@@ -267,6 +311,10 @@ inline int launch_pipe_sweep(const long long E[3], const SweepGeom& g, int dir, 
     PipeArgs P{};
     FastArgs& a = P.a;
     a.in = in; a.vL = vL; a.vR = vR; a.cp = cp; a.wp = wp;
+    if (ucf) {
+        for (int q = 0; q < 56; ++q) a.ucf[q] = ucf[q];
+        a.cp = CoefPtrs{nullptr, nullptr, nullptr, nullptr, nullptr};
+    }
     a.ns = g.ns; a.nc = g.nc;
     a.o_first = (order == 3) ? 0 : 3;
     a.nf = (int)((order == 3) ? g.ns : g.nc);
@@ -327,14 +375,14 @@ inline int launch_pipe_sweep(const long long E[3], const SweepGeom& g, int dir, 
     if (r != CUDA_SUCCESS) return 1003;
     const int key = order * 4 + (mp ? 2 : 0) + (kind1 ? 1 : 0);
     switch (key) {
-        case 12: return launch_pipe_t<3, false, 0, 6>(map, P, st, sms);
-        case 13: return launch_pipe_t<3, false, 1, 3>(map, P, st, sms);
-        case 14: return launch_pipe_t<3, true, 0, 6>(map, P, st, sms);
-        case 15: return launch_pipe_t<3, true, 1, 3>(map, P, st, sms);
-        case 20: return launch_pipe_t<5, false, 0, 6>(map, P, st, sms);
-        case 21: return launch_pipe_t<5, false, 1, 3>(map, P, st, sms);
-        case 22: return launch_pipe_t<5, true, 0, 6>(map, P, st, sms);
-        case 23: return launch_pipe_t<5, true, 1, 3>(map, P, st, sms);
+        case 12: return launch_pipe_t<3, false, 0, WSB_PIPE_STAGES0>(map, P, st, sms);
+        case 13: return launch_pipe_t<3, false, 1, WSB_PIPE_STAGES1>(map, P, st, sms);
+        case 14: return launch_pipe_t<3, true, 0, WSB_PIPE_STAGES0>(map, P, st, sms);
+        case 15: return launch_pipe_t<3, true, 1, WSB_PIPE_STAGES1>(map, P, st, sms);
+        case 20: return launch_pipe_t<5, false, 0, WSB_PIPE_STAGES0>(map, P, st, sms);
+        case 21: return launch_pipe_t<5, false, 1, WSB_PIPE_STAGES1>(map, P, st, sms);
+        case 22: return launch_pipe_t<5, true, 0, WSB_PIPE_STAGES0>(map, P, st, sms);
+        case 23: return launch_pipe_t<5, true, 1, WSB_PIPE_STAGES1>(map, P, st, sms);
         case 28: return launch_pipe_t<7, false, 0, 6>(map, P, st, sms);
         case 29: return launch_pipe_t<7, false, 1, 3>(map, P, st, sms);
         case 30: return launch_pipe_t<7, true, 0, 6>(map, P, st, sms);

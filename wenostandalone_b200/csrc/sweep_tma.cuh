@@ -50,6 +50,10 @@ struct FastArgs {
     long long sU, sWw, sV; // input strides of u, w, v
     long long in_off;      // input offset of (J=0, u=0, w=0, v=0)
     long long o_sU, o_sW, o_sV;  // output strides of u, w, v
+    // Face-independent coefficients (laid out as Coef<ORDER>), used by the
+    // UNI kernel instances straight from the kernel-parameter (constant)
+    // bank instead of 27-56 registers per thread.
+    double ucf[56];
 };
 
 template <typename T>
@@ -121,6 +125,10 @@ struct LinearTile {  // plain row-major staging (cp.async, or TMA without swizzl
     const T* p;      // centre element of column 0
     int js, ks;      // strides along the sweep and between columns
     __device__ __forceinline__ T operator()(int q, int k) const { return p[k * ks + q * js]; }
+    __device__ __forceinline__ void pair(int q, int k, T& x, T& y) const {
+        x = p[k * ks + q * js];
+        y = p[(k + 1) * ks + q * js];
+    }
 };
 
 template <typename T>
@@ -131,6 +139,13 @@ struct Swz128Tile {  // TMA box of 128-byte rows in the 128B swizzle pattern
         const int row = row0 + q;
         const int byte = k * (int)sizeof(T);
         return *reinterpret_cast<const T*>(base + row * 128 + ((((byte >> 4) ^ (row & 7))) << 4) + (byte & 15));
+    }
+    // columns k and k+1 (k even, doubles): one 16-byte chunk, one LDS.128
+    __device__ __forceinline__ void pair(int q, int k, T& x, T& y) const {
+        const int row = row0 + q;
+        const double2 v = *reinterpret_cast<const double2*>(base + row * 128 + ((((k >> 1) ^ (row & 7))) << 4));
+        x = v.x;
+        y = v.y;
     }
 };
 
@@ -176,6 +191,42 @@ __device__ __forceinline__ void compute_columns(const FastArgs& a, const Coef<OR
     }
 }
 
+// WENO5-JS (+MP) on columns [kb, ke), two columns per iteration: both
+// columns' straight-line fast paths are issued before either fallback
+// check, so the compiler interleaves two independent dependency chains.
+// Pairs start at an even column (the swizzled tile serves a pair with one
+// 16-byte load); a pair member outside [kb, ke) is computed but not stored.
+template <bool MPF, typename Tile>
+__device__ __forceinline__ void compute_js5_pairs(const FastArgs& a, const Coef<5>& cf, const Tile& t, int kb,
+                                                  int ke, long long oidx0) {
+    double* __restrict__ vL = (double*)a.vL;
+    double* __restrict__ vR = (double*)a.vR;
+    const double eps = a.wp.eps;
+    for (int k = kb & ~1; k < ke; k += 2) {
+        double A[5], B[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) t.pair(q - 2, k, A[q], B[q]);
+        double LA, RA, LB, RB;
+        const bool okA = weno5_js_fast<double>(A[0], A[1], A[2], A[3], A[4], cf, eps, LA, RA);
+        const bool okB = weno5_js_fast<double>(B[0], B[1], B[2], B[3], B[4], cf, eps, LB, RB);
+        if (!okA) weno5_face<double>(A[0], A[1], A[2], A[3], A[4], cf, JS, eps, a.wp.teno_ct, LA, RA);
+        if (!okB) weno5_face<double>(B[0], B[1], B[2], B[3], B[4], cf, JS, eps, a.wp.teno_ct, LB, RB);
+        if (MPF) {
+            mp_limit(A[0], A[1], A[2], A[3], A[4], LA, RA);
+            mp_limit(B[0], B[1], B[2], B[3], B[4], LB, RB);
+        }
+        const long long oa = oidx0 + (long long)k * a.o_sU;
+        if (k >= kb) {
+            vL[oa] = LA;
+            vR[oa] = RA;
+        }
+        if (k + 1 < ke) {
+            vL[oa + a.o_sU] = LB;
+            vR[oa + a.o_sU] = RB;
+        }
+    }
+}
+
 template <int ORDER, bool MPF, typename T, int KIND, int XW, int STAGES, int SCH>
 __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(const FastArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -198,7 +249,10 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(c
     long long cidx = o - 3;
     cidx = cidx < 0 ? 0 : (cidx > a.nc - 1 ? a.nc - 1 : cidx);
     Coef<ORDER> cf;
-    if (active) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
+    if (active) {
+        if (a.cp.polyL) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
+        else cf = *reinterpret_cast<const Coef<ORDER>*>(a.ucf);  // face-independent coefficients
+    }
 
     const int js = (KIND == 0) ? 1 : a.pitch;     // smem stride along the sweep
     const int ks = (KIND == 0) ? a.pitch : 1;     // smem stride between columns
@@ -268,7 +322,8 @@ int launch_fast_t(FastArgs a, cudaStream_t st, int sms) {
 // kernel, so the caller can fall back to the general-stride one.
 template <typename T>
 int launch_tma_sweep(const long long E[3], const SweepGeom& g, int dir, bool folded, int order, bool mp,
-                     const T* in, T* vL, T* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st) {
+                     const T* in, T* vL, T* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st,
+                     const double* ucf = nullptr) {
     (void)E;
     static int sms = 0;
     if (!sms) {
@@ -284,6 +339,10 @@ int launch_tma_sweep(const long long E[3], const SweepGeom& g, int dir, bool fol
     a.vR = vR;
     a.cp = cp;
     a.wp = wp;
+    if (ucf) {
+        for (int q = 0; q < 56; ++q) a.ucf[q] = ucf[q];
+        a.cp = CoefPtrs{nullptr, nullptr, nullptr, nullptr, nullptr};
+    }
     a.ns = g.ns;
     a.nc = g.nc;
     a.o_first = (order == 3) ? 0 : 3;

@@ -17,10 +17,10 @@
 //    arithmetic; when a sum leaves [2^-498, 2^498) (extreme beta, or
 //    eps < ~1e-37) the faithful form is used instead.
 //
-// The MP limiter rounds exactly as the reference does (its min/max
-// decisions depend on the signs of second differences): every product and
-// sum is either an explicit _rn intrinsic, which is never contracted into an
-// FMA, or an FMA whose product is exact (by 2, 4 or 1/2).
+// The MP limiter is a continuous, piecewise-linear function of the stencil
+// (min, max, minmod, median), so it may be evaluated in any form that is
+// equal in exact arithmetic: a comparison that rounds the other way near a
+// tie changes the result by a rounding only.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -298,6 +298,40 @@ __device__ __forceinline__ void weno5_face(const double vm2, const double vm1, c
     oR = (a0 / s) * pR0 + (a1 / s) * pR1 + (a2 / s) * pR2;
 }
 
+// WENO5-JS in the one-reciprocal form with no fallback inside: computes oL
+// and oR unconditionally and returns false when a normalisation sum left
+// the range where the form is valid, in which case the caller redoes the
+// face with weno5_face.  Straight-line code, so two columns can interleave.
+template <typename PT>
+__device__ __forceinline__ bool weno5_js_fast(const double vm2, const double vm1, const double v0,
+                                              const double vp1, const double vp2, const Coef<5>& c,
+                                              double eps, double& oL, double& oR) {
+    const double dvd_p1 = vp2 - vp1;
+    const double dvd_0 = vp1 - v0;
+    const double dvd_m1 = v0 - vm1;
+    const double dvd_m2 = vm1 - vm2;
+    const double beta0 = c.b[0] * dvd_p1 * dvd_p1 + c.b[1] * dvd_p1 * dvd_0 + c.b[2] * dvd_0 * dvd_0 + eps;
+    const double beta1 = c.b[3] * dvd_0 * dvd_0 + c.b[4] * dvd_0 * dvd_m1 + c.b[5] * dvd_m1 * dvd_m1 + eps;
+    const double beta2 = c.b[6] * dvd_m1 * dvd_m1 + c.b[7] * dvd_m1 * dvd_m2 + c.b[8] * dvd_m2 * dvd_m2 + eps;
+    const PT v0p = (PT)v0, fp1 = (PT)dvd_p1, f0 = (PT)dvd_0, fm1 = (PT)dvd_m1, fm2 = (PT)dvd_m2;
+    const double pL0 = (double)(v0p + (PT)c.pL[0] * fp1 + (PT)c.pL[1] * f0);
+    const double pL1 = (double)(v0p + (PT)c.pL[2] * f0 + (PT)c.pL[3] * fm1);
+    const double pL2 = (double)(v0p + (PT)c.pL[4] * fm1 + (PT)c.pL[5] * fm2);
+    const double pR0 = (double)(v0p + (PT)c.pR[0] * fp1 + (PT)c.pR[1] * f0);
+    const double pR1 = (double)(v0p + (PT)c.pR[2] * f0 + (PT)c.pR[3] * fm1);
+    const double pR2 = (double)(v0p + (PT)c.pR[4] * fm1 + (PT)c.pR[5] * fm2);
+    const double q0 = beta0 * beta0, q1 = beta1 * beta1, q2 = beta2 * beta2;
+    const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+    const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2;
+    const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2;
+    const double SL = aL0 + aL1 + aL2, SR = aR0 + aR1 + aR2;
+    const bool ok = mid_range(SL) && mid_range(SR);
+    const double r = nr_rcp(SL * SR);
+    oL = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * (SR * r);
+    oR = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * (SL * r);
+    return ok;
+}
+
 // ---------------------------------------------------------------------
 // WENO7 (f90:1448-1535).  v[-3..3].  The reference's arrays are sized 0:4
 // with beta(4) = eps; its TENO branch keeps alpha(4) = (1+tau/eps)^6 in the
@@ -406,108 +440,109 @@ __device__ __forceinline__ void weno7_face(const double* v /* v[-3..3] */, const
 // ---------------------------------------------------------------------
 // 4-argument minmod of (4dl-dr, dl, 4dr-dl, dr) (f90:1568-1571).  The
 // reference's product of SIGN() sums is +-1 when all four arguments share a
-// sign bit and 0 otherwise, so it equals copysign(min|.|, 4dl-dr) or 0.
-// 4*dl is exact, so fma(4, dl, -dr) rounds exactly like 4*dl - dr.
+// sign and 0 otherwise.  With m = min(|dl|,|dr|) and M = max(|dl|,|dr|) the
+// four share a sign exactly when dl, dr do and 4m > M, and then the least
+// magnitude is min(4m - M, m) (|4dr - dl| >= 3m > m for the other pair), so
+// the result is copysign(min(4m - M, m), dl) or 0 with two comparisons.
 __device__ __forceinline__ double mp_minmod(double dl, double dr) {
-    const double A = fma(4.0, dl, -dr);
-    const double B = fma(4.0, dr, -dl);
-    const double mn = fmin(fmin(fabs(A), fabs(dl)), fmin(fabs(B), fabs(dr)));
-    const int hA = __double2hiint(A);
-    const int same = (hA ^ __double2hiint(B)) | (hA ^ __double2hiint(dl)) | (hA ^ __double2hiint(dr));
-    return (same >= 0) ? copysign(mn, A) : 0.0;
-}
-
-// x + (sign(1/2, lo-x) + sign(1/2, hi-x)) * min(|lo-x|, |hi-x|)  (f90:1582-1583).
-// The factor is -1, 0 or +1, so the update is x + copysign(min, lo-x) when
-// lo-x and hi-x share a sign bit and x otherwise.
-__device__ __forceinline__ double mp_clamp(double x, double lo, double hi) {
-    const double a = __dsub_rn(lo, x), b = __dsub_rn(hi, x);
-    const double m = fmin(fabs(a), fabs(b));
-    const bool same = (__double2hiint(a) ^ __double2hiint(b)) >= 0;
-    return same ? __dadd_rn(x, copysign(m, a)) : x;
+    const double a = fabs(dl), b = fabs(dr);
+    const bool al = a < b;
+    const double m = al ? a : b, M = al ? b : a;
+    const double t = fma(4.0, m, -M);  // |4 dl - dr| or |4 dr - dl| of the smaller one
+    const bool same = ((__double2hiint(dl) ^ __double2hiint(dr)) >= 0) && (t > 0.0);
+    return same ? copysign(t < m ? t : m, dl) : 0.0;
 }
 
 __device__ __forceinline__ bool sign_clear(double x) { return __double2hiint(x) >= 0; }
 
-// The limiter proper.  min(v0, v0 -/+ 2 dv) and min(v0, v_{j+-1}) are
-// decided by the sign of the difference that produced them (an exact
-// ordering test for finite values), which saves FP64 min/max issue slots;
-// every arithmetic step keeps the reference's rounding (the products by 2,
-// 4 and 1/2 are exact, so they may fuse).
+// min / max as one comparison and a select (no NaN special-casing: the
+// limiter's bound candidates are finite whenever the field is).
+template <typename T>
+__device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
+template <typename T>
+__device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+// median(x, lo, hi) for lo <= hi; a NaN x stays NaN, as in the reference.
+template <typename T>
+__device__ __forceinline__ T sclamp(T x, T lo, T hi) { return (x < lo) ? lo : ((hi < x) ? hi : x); }
+
+// The limiter proper (f90:1564-1608).  Every step is continuous in the data
+// (min, max, minmod, median), so roundings that differ from the reference's
+// move the result by roundings only; the forms below are the reference's
+// expressions rearranged in exact arithmetic:
+//  * the final update x + (sign(1/2, lo-x) + sign(1/2, hi-x)) min(|lo-x|, |hi-x|)
+//    is median(x, lo, hi), and lo <= v0 <= hi always (each term of lo is a
+//    min over a set containing v0, each term of hi a max), so it is
+//    max(lo, min(x, hi));
+//  * min/max(v0, v0 -+ 2 dv) and min/max(v0, v_{j+-1}) follow from the sign
+//    of the difference, without a comparison.
 __device__ __forceinline__ void mp_limit(const double vm2, const double vm1, const double v0,
                                          const double vp1, const double vp2, double& L, double& R) {
     const double kBetaMP = 4.0 / 3.0;  // beta_mp (f90:1556)
-    const double dm1 = fma(-2.0, vm1, __dadd_rn(v0, vm2));
-    const double d0 = fma(-2.0, v0, __dadd_rn(vp1, vm1));
-    const double dp1 = fma(-2.0, vp1, __dadd_rn(vp2, v0));
+    const double dm1 = fma(-2.0, vm1, v0 + vm2);
+    const double d0 = fma(-2.0, v0, vp1 + vm1);
+    const double dp1 = fma(-2.0, vp1, vp2 + v0);
     const double mA = mp_minmod(dm1, d0);  // d_MD of vL, d_LC of vR
     const double mB = mp_minmod(d0, dp1);  // d_LC of vL, d_MD of vR
-    const double dR1 = __dsub_rn(vp1, v0);  // >= 0  <=>  vp1 >= v0
-    const double dL1 = __dsub_rn(v0, vm1);  // >= 0  <=>  v0 >= vm1
+    const double dR1 = vp1 - v0;           // >= 0  <=>  vp1 >= v0
+    const double dL1 = v0 - vm1;           // >= 0  <=>  v0 >= vm1
     const bool up_r = sign_clear(dR1), up_l = sign_clear(dL1);
     {
-        const double UL = fma(-2.0, dR1, v0);                      // v0 - 2 dR1: <= v0 iff dR1 >= 0
-        const double MD = __dmul_rn(__dsub_rn(__dadd_rn(v0, vm1), mA), 0.5);
-        const double LC = __dadd_rn(fma(-0.5, dR1, v0), __dmul_rn(kBetaMP, mB));
+        const double UL = fma(-2.0, dR1, v0);  // <= v0 iff dR1 >= 0
+        const double MD = ((v0 + vm1) - mA) * 0.5;
+        const double LC = fma(kBetaMP, mB, fma(-0.5, dR1, v0));
         const double mn1 = up_l ? vm1 : v0, mx1 = up_l ? v0 : vm1;  // min/max(v0, vm1)
         const double mn2 = up_r ? UL : v0, mx2 = up_r ? v0 : UL;    // min/max(v0, UL)
-        const double lo = fmax(fmin(mn1, MD), fmin(mn2, LC));
-        const double hi = fmin(fmax(mx1, MD), fmax(mx2, LC));
-        L = mp_clamp(L, lo, hi);
+        const double lo = smax(smin(mn1, MD), smin(mn2, LC));
+        const double hi = smin(smax(mx1, MD), smax(mx2, LC));
+        L = sclamp(L, lo, hi);
     }
     {
-        const double UL = fma(2.0, dL1, v0);                       // v0 + 2 dL1: >= v0 iff dL1 >= 0
-        const double MD = __dmul_rn(__dsub_rn(__dadd_rn(v0, vp1), mB), 0.5);
-        const double LC = __dadd_rn(fma(0.5, dL1, v0), __dmul_rn(kBetaMP, mA));
+        const double UL = fma(2.0, dL1, v0);   // >= v0 iff dL1 >= 0
+        const double MD = ((v0 + vp1) - mB) * 0.5;
+        const double LC = fma(kBetaMP, mA, fma(0.5, dL1, v0));
         const double mn1 = up_r ? v0 : vp1, mx1 = up_r ? vp1 : v0;  // min/max(v0, vp1)
         const double mn2 = up_l ? v0 : UL, mx2 = up_l ? UL : v0;    // min/max(v0, UL)
-        const double lo = fmax(fmin(mn1, MD), fmin(mn2, LC));
-        const double hi = fmin(fmax(mx1, MD), fmax(mx2, LC));
-        R = mp_clamp(R, lo, hi);
+        const double lo = smax(smin(mn1, MD), smin(mn2, LC));
+        const double hi = smin(smax(mx1, MD), smax(mx2, LC));
+        R = sclamp(R, lo, hi);
     }
 }
 
-// FP32-bulk MP: same formula in FP32 on the FP32 field.
+// FP32-bulk MP: the same limiter in FP32 on the FP32 field.
 __device__ __forceinline__ float mp_minmod_f(float dl, float dr) {
-    const float A = __fsub_rn(__fmul_rn(4.0f, dl), dr);
-    const float B = __fsub_rn(__fmul_rn(4.0f, dr), dl);
-    const float mn = fminf(fminf(fminf(fabsf(A), fabsf(dl)), fabsf(B)), fabsf(dr));
-    const int hA = __float_as_int(A);
-    const int same = (hA ^ __float_as_int(B)) | (hA ^ __float_as_int(dl)) | (hA ^ __float_as_int(dr));
-    return (same >= 0) ? copysignf(mn, A) : 0.0f;
+    const float a = fabsf(dl), b = fabsf(dr);
+    const bool al = a < b;
+    const float m = al ? a : b, M = al ? b : a;
+    const float t = fmaf(4.0f, m, -M);
+    const bool same = ((__float_as_int(dl) ^ __float_as_int(dr)) >= 0) && (t > 0.0f);
+    return same ? copysignf(t < m ? t : m, dl) : 0.0f;
 }
 
-__device__ __forceinline__ float mp_clamp_f(float x, float lo, float hi) {
-    const float a = __fsub_rn(lo, x), b = __fsub_rn(hi, x);
-    const float f = __fadd_rn(copysignf(0.5f, a), copysignf(0.5f, b));
-    return __fadd_rn(x, __fmul_rn(f, fminf(fabsf(a), fabsf(b))));
-}
-
-__device__ __forceinline__ void mp_limit_f(const float vm2, const float vm1, const float v0,
-                                           const float vp1, const float vp2, float& L, float& R) {
+__device__ __forceinline__ void mp_limit_f(const float vm2, const float vm1, const float v0, const float vp1,
+                                           const float vp2, float& L, float& R) {
     const float kBetaMP = 4.0f / 3.0f;
-    const float dm1 = __fsub_rn(__fadd_rn(v0, vm2), __fmul_rn(2.0f, vm1));
-    const float d0 = __fsub_rn(__fadd_rn(vp1, vm1), __fmul_rn(2.0f, v0));
-    const float dp1 = __fsub_rn(__fadd_rn(vp2, v0), __fmul_rn(2.0f, vp1));
+    const float dm1 = fmaf(-2.0f, vm1, v0 + vm2);
+    const float d0 = fmaf(-2.0f, v0, vp1 + vm1);
+    const float dp1 = fmaf(-2.0f, vp1, vp2 + v0);
     const float mA = mp_minmod_f(dm1, d0);
     const float mB = mp_minmod_f(d0, dp1);
+    const float dR1 = vp1 - v0, dL1 = v0 - vm1;
+    const bool up_r = __float_as_int(dR1) >= 0, up_l = __float_as_int(dL1) >= 0;
     {
-        const float dR1 = __fsub_rn(vp1, v0);
-        const float UL = __fsub_rn(v0, __fmul_rn(2.0f, dR1));
-        const float MD = __fmul_rn(__fsub_rn(__fadd_rn(v0, vm1), mA), 0.5f);
-        const float LC = __fadd_rn(__fsub_rn(v0, __fmul_rn(dR1, 0.5f)), __fmul_rn(kBetaMP, mB));
-        const float lo = fmaxf(fminf(fminf(v0, vm1), MD), fminf(fminf(v0, UL), LC));
-        const float hi = fminf(fmaxf(fmaxf(v0, vm1), MD), fmaxf(fmaxf(v0, UL), LC));
-        L = mp_clamp_f(L, lo, hi);
+        const float UL = fmaf(-2.0f, dR1, v0);
+        const float MD = ((v0 + vm1) - mA) * 0.5f;
+        const float LC = fmaf(kBetaMP, mB, fmaf(-0.5f, dR1, v0));
+        const float mn1 = up_l ? vm1 : v0, mx1 = up_l ? v0 : vm1;
+        const float mn2 = up_r ? UL : v0, mx2 = up_r ? v0 : UL;
+        L = sclamp(L, smax(smin(mn1, MD), smin(mn2, LC)), smin(smax(mx1, MD), smax(mx2, LC)));
     }
     {
-        const float dL1 = __fsub_rn(v0, vm1);
-        const float UL = __fadd_rn(v0, __fmul_rn(2.0f, dL1));
-        const float MD = __fmul_rn(__fsub_rn(__fadd_rn(v0, vp1), mB), 0.5f);
-        const float LC = __fadd_rn(__fadd_rn(v0, __fmul_rn(dL1, 0.5f)), __fmul_rn(kBetaMP, mA));
-        const float lo = fmaxf(fminf(fminf(v0, vp1), MD), fminf(fminf(v0, UL), LC));
-        const float hi = fminf(fmaxf(fmaxf(v0, vp1), MD), fmaxf(fmaxf(v0, UL), LC));
-        R = mp_clamp_f(R, lo, hi);
+        const float UL = fmaf(2.0f, dL1, v0);
+        const float MD = ((v0 + vp1) - mB) * 0.5f;
+        const float LC = fmaf(kBetaMP, mA, fmaf(0.5f, dL1, v0));
+        const float mn1 = up_r ? v0 : vp1, mx1 = up_r ? vp1 : v0;
+        const float mn2 = up_l ? v0 : UL, mx2 = up_l ? UL : v0;
+        R = sclamp(R, smax(smin(mn1, MD), smin(mn2, LC)), smin(smax(mx1, MD), smax(mx2, LC)));
     }
 }
 

@@ -13,6 +13,8 @@
 #include <mutex>
 #include <string>
 #include <algorithm>
+#include <fstream>
+#include <sstream>
 #include <vector>
 
 #include "weno_sb.h"
@@ -20,6 +22,8 @@
 #include "sweep_generic.cuh"
 #include "sweep_tma.cuh"
 #include "sweep_pipe.cuh"
+#include "weno_adjoint.cuh"
+#include "batched.cuh"
 
 using namespace wsb;
 
@@ -230,27 +234,30 @@ int launch_order1(const Dims& d, int dir, const double* v_vf, T* vL, T* vR, cuda
 
 template <int ORDER, bool MPF, typename T>
 void launch_generic_t(const SweepGeom& g, const T* in, T* vL, T* vR, const CoefPtrs& cp,
-                      const WenoParams& wp, cudaStream_t st) {
+                      const WenoParams& wp, cudaStream_t st, const UniCoefs& uc) {
     const long long nf = (ORDER == 3) ? g.ns : g.nc;
     dim3 blk(128);
     const long long tiles = (nf + 127) / 128;
     const long long want = (long long)num_sms() * 16 / tiles + 1;
     dim3 grid((unsigned)tiles, (unsigned)std::min<long long>(std::min<long long>(g.cols, want * 8), 65535));
-    sweep_generic_kernel<ORDER, MPF, T><<<grid, blk, 0, st>>>(g, in, vL, vR, cp, wp);
+    sweep_generic_kernel<ORDER, MPF, T><<<grid, blk, 0, st>>>(g, in, vL, vR, cp, wp, uc);
 }
 
 template <typename T>
 int launch_generic(const SweepGeom& g, int order, bool mp, const T* in, T* vL, T* vR,
-                   const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st) {
+                   const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st, const double* ucf = nullptr) {
+    UniCoefs uc{};
+    if (ucf)
+        for (int q = 0; q < 56; ++q) uc.v[q] = ucf[q];
     switch (order * 2 + (mp ? 1 : 0)) {
-        case 0: launch_generic_t<0, false, T>(g, in, vL, vR, cp, wp, st); break;
-        case 1: launch_generic_t<0, true, T>(g, in, vL, vR, cp, wp, st); break;
-        case 6: launch_generic_t<3, false, T>(g, in, vL, vR, cp, wp, st); break;
-        case 7: launch_generic_t<3, true, T>(g, in, vL, vR, cp, wp, st); break;
-        case 10: launch_generic_t<5, false, T>(g, in, vL, vR, cp, wp, st); break;
-        case 11: launch_generic_t<5, true, T>(g, in, vL, vR, cp, wp, st); break;
-        case 14: launch_generic_t<7, false, T>(g, in, vL, vR, cp, wp, st); break;
-        case 15: launch_generic_t<7, true, T>(g, in, vL, vR, cp, wp, st); break;
+        case 0: launch_generic_t<0, false, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 1: launch_generic_t<0, true, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 6: launch_generic_t<3, false, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 7: launch_generic_t<3, true, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 10: launch_generic_t<5, false, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 11: launch_generic_t<5, true, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 14: launch_generic_t<7, false, T>(g, in, vL, vR, cp, wp, st, uc); break;
+        case 15: launch_generic_t<7, true, T>(g, in, vL, vR, cp, wp, st, uc); break;
         default: return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
     }
     return cuda_err(cudaGetLastError(), "reconstruction launch");
@@ -267,27 +274,193 @@ int kernel_choice() {
     return 0;
 }
 
+// Coefficients come either per face (cf, device arrays) or, when ucf is
+// non-null, as one face-independent set laid out like Coef<order>.
 template <typename T>
 int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned flags,
-             const T* in, const weno_sb_coefs* cf, T* vL, T* vR, cudaStream_t st) {
+             const T* in, const weno_sb_coefs* cf, T* vL, T* vR, cudaStream_t st,
+             const double* ucf = nullptr) {
     const bool folded = (flags & WENO_SB_F_FOLDED) != 0;
     const bool mp = (flags & WENO_SB_F_MP) != 0;
     SweepGeom g = make_geom(d, dir, folded);
     if (g.nc < 1) return set_err(WENO_SB_ERR_ARG, "sweep has no core faces (Ns=%lld)", g.ns);
-    CoefPtrs cp{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
+    CoefPtrs cp{nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
     if constexpr (sizeof(T) == 8) {
         if (choice == 0) {
-            int rc = launch_pipe_sweep(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st, num_sms());
+            int rc = launch_pipe_sweep(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st, num_sms(), ucf);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "tma sweep launch") : rc;
         }
     }
     if (choice == 0 || choice == 2) {
-        int rc = launch_tma_sweep<T>(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st);
+        int rc = launch_tma_sweep<T>(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st, ucf);
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "cp.async sweep launch") : rc;
     }
-    return launch_generic<T>(g, order, mp, in, vL, vR, cp, wp, st);
+    return launch_generic<T>(g, order, mp, in, vL, vR, cp, wp, st, ucf);
+}
+
+// One face's coefficients (weno_sb_face_coefs, index order [s][r]) laid out
+// as the kernels' Coef<order> register block.
+void build_ucf(int order, const weno_sb_face_coefs* f, double* out) {
+    for (int q = 0; q < 56; ++q) out[q] = 0.0;
+    const int R = (order + 1) / 2;    // stencils
+    const int S = R - 1;              // poly terms per stencil
+    const int B = (order == 7) ? 6 : (order == 5 ? 3 : 1);  // beta terms per stencil
+    int k = 0;
+    for (int r = 0; r < R; ++r)
+        for (int s = 0; s < S; ++s) out[k++] = f->polyL[s][r];
+    for (int r = 0; r < R; ++r)
+        for (int s = 0; s < S; ++s) out[k++] = f->polyR[s][r];
+    for (int r = 0; r < R; ++r) out[k++] = f->dL[r];
+    for (int r = 0; r < R; ++r) out[k++] = f->dR[r];
+    for (int r = 0; r < R; ++r)
+        for (int s = 0; s < B; ++s) out[k++] = f->beta_coef[s][r];
+}
+
+// Adjoint of one sweep (weno_adjoint.cuh).  gv has the layout of v_in.
+int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned flags, const double* v,
+               const CoefPtrs& cp, const double* ucf, const double* gL, const double* gR, double* gv,
+               cudaStream_t st) {
+    const bool folded = (flags & WENO_SB_F_FOLDED) != 0;
+    const bool acc_flag = (flags & WENO_SB_F_ACCUMULATE) != 0;
+    VjpArgs a{};
+    a.g = make_geom(d, dir, folded);
+    if (a.g.nc < 1) return set_err(WENO_SB_ERR_ARG, "sweep has no core faces");
+    a.v = v;
+    a.gL = gL;
+    a.gR = gR;
+    a.gv = gv;
+    a.cp = cp;
+    if (ucf)
+        for (int q = 0; q < 56; ++q) a.uc.v[q] = ucf[q];
+    a.wp = WenoParams{gr->scheme, gr->weno_eps, gr->teno_CT};
+    a.mp = (flags & WENO_SB_F_MP) ? 1 : 0;
+    // the folded layout has cells no sweep touches: clear them once and add
+    a.accumulate = (acc_flag || folded) ? 1 : 0;
+    if (folded && !acc_flag)
+        WSB_CUDA(cudaMemsetAsync(gv, 0, sizeof(double) * d.E[0] * d.E[1] * d.E[2] * d.nv, st));
+    const int threads = 128;
+    a.TC = threads - 6;
+    a.n_ct = (int)((a.g.ns + 6 + a.TC - 1) / a.TC);
+    long long per = ((long long)num_sms() * 12) / a.n_ct;
+    if (per < 1) per = 1;
+    if (per > a.g.cols) per = a.g.cols;
+    const size_t smem = sizeof(double) * 7 * threads;
+    const unsigned grid = (unsigned)(per * a.n_ct);
+    switch (order) {
+        case 3: vjp_kernel<3><<<grid, threads, smem, st>>>(a); break;
+        case 5: vjp_kernel<5><<<grid, threads, smem, st>>>(a); break;
+        case 7: vjp_kernel<7><<<grid, threads, smem, st>>>(a); break;
+        default: return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
+    }
+    return cuda_err(cudaGetLastError(), "vjp launch");
+}
+
+// ----------------------------------------------------------------------
+// Batches of uneven blocks (batched.cuh)
+// ----------------------------------------------------------------------
+struct Batch {
+    std::vector<weno_sb_block> blocks;
+    std::vector<BatchEntry> entries;
+    BatchEntry* d_entries = nullptr;
+    unsigned long long* d_counter = nullptr;
+    long long n_items = 0;
+    int threads = 128;  // face-tile width = CTA size
+    int U = 8;          // columns per work item
+    int grid = 0;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+};
+
+std::mutex g_batch_mu;
+std::vector<Batch*> g_batches;
+
+Batch* get_batch(int b) {
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    if (b < 1 || b > (int)g_batches.size()) return nullptr;
+    return g_batches[b - 1];
+}
+
+void batch_release_graph(Batch* B) {
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    B->exec = nullptr;
+    B->graph = nullptr;
+}
+
+// Cut the entries into work items for tile width `threads` and `U` columns
+// per item, upload the table and size the persistent grid.
+int batch_layout(Batch* B, int threads, int U) {
+    B->threads = threads;
+    B->U = U;
+    long long item = 0;
+    for (auto& e : B->entries) {
+        e.TJ = threads;
+        e.n_jt = (e.nf + threads - 1) / threads;
+        e.n_groups = (e.g.cols + U - 1) / U;
+        e.item0 = item;
+        item += (long long)e.n_jt * e.n_groups;
+    }
+    B->n_items = item;
+    WSB_CUDA(cudaMemcpy(B->d_entries, B->entries.data(), sizeof(BatchEntry) * B->entries.size(),
+                        cudaMemcpyHostToDevice));
+    int occ = 0;
+    WSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, threads, 0));
+    if (occ < 1) occ = 1;
+    B->grid = num_sms() * occ;
+    batch_release_graph(B);
+    return WENO_SB_OK;
+}
+
+int batch_enqueue(Batch* B, cudaStream_t st) {
+    WSB_CUDA(cudaMemsetAsync(B->d_counter, 0, sizeof(unsigned long long), st));
+    batch_kernel<<<B->grid, B->threads, 0, st>>>(B->d_entries, (int)B->entries.size(), B->n_items, B->d_counter,
+                                                 B->U);
+    return cuda_err(cudaGetLastError(), "batch launch");
+}
+
+// Capture the batch (counter reset + persistent kernel) into a CUDA graph.
+int batch_build_graph(Batch* B) {
+    batch_release_graph(B);
+    WSB_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_enqueue(B, B->cap);
+    cudaGraph_t gph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(B->cap, &gph);
+    if (rc) {
+        if (gph) cudaGraphDestroy(gph);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_err(e, "cudaStreamEndCapture");
+    B->graph = gph;
+    WSB_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+    return WENO_SB_OK;
+}
+
+// FNV-1a signature of what the tile choice depends on: per entry the order,
+// v_size, storage, direction, layout and extents in 16-cell buckets.
+unsigned long long batch_signature(const Batch* B) {
+    unsigned long long h = 1469598103934665603ull;
+    auto mix = [&](long long x) {
+        for (int i = 0; i < 8; ++i) {
+            h ^= (unsigned long long)((x >> (8 * i)) & 0xff);
+            h *= 1099511628211ull;
+        }
+    };
+    for (const auto& e : B->entries) {
+        mix(e.order);
+        mix(e.g.nv);
+        mix(e.fp32);
+        mix(e.mp);
+        mix(e.g.sJ == 1 ? 0 : 1);
+        mix(e.g.ns / 16);
+        mix(e.g.c1 / 16);
+        mix(e.g.c2 / 16);
+    }
+    return h;
 }
 
 // ----------------------------------------------------------------------
@@ -303,6 +476,11 @@ struct Handle {
     int dtype[WENO_SB_A_COUNT] = {};
     double* sum_scratch = nullptr;  // kSumBlocks partials + 1 result
     int device = 0;
+    // Per direction: whether each of the five coefficient arrays was last set
+    // by weno_sb_upload with the same values on every face (then the sweeps
+    // take them from kernel parameters), and face 0's values.
+    bool coef_uniform[3][5] = {};
+    weno_sb_face_coefs face0[3] = {};
 };
 
 std::mutex g_mu;
@@ -312,6 +490,35 @@ Handle* get_handle(int h) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (h < 1 || h > (int)g_handles.size()) return nullptr;
     return g_handles[h - 1];
+}
+
+// Record whether an uploaded coefficient array is the same on every face.
+void note_coefficients(Handle* H, int which, const double* host) {
+    const int kind = (which - WENO_SB_A_POLYL(0)) / 3;  // 0 polyL 1 polyR 2 dL 3 dR 4 beta
+    const int dir = (which - WENO_SB_A_POLYL(0)) % 3;
+    long long ns, c1, c2;
+    sweep_ext(H->dims, dir, &ns, &c1, &c2);
+    const long long nc = ns - 6;
+    weno_sb_face_coefs& f = H->face0[dir];
+    bool uni = true;
+    if (kind <= 1 || kind == 4) {  // (nc, 5, S) arrays
+        const int S = (kind == 4) ? 6 : 3;
+        for (int s = 0; s < S; ++s)
+            for (int r = 0; r < 5; ++r) {
+                const double* col = host + nc * (r + 5 * s);
+                for (long long cc = 1; cc < nc && uni; ++cc) uni = (col[cc] == col[0]);
+                if (kind == 0) f.polyL[s][r] = col[0];
+                else if (kind == 1) f.polyR[s][r] = col[0];
+                else f.beta_coef[s][r] = col[0];
+            }
+    } else {  // (5, nc)
+        for (int r = 0; r < 5; ++r) {
+            for (long long cc = 1; cc < nc && uni; ++cc) uni = (host[r + 5 * cc] == host[r]);
+            if (kind == 2) f.dL[r] = host[r];
+            else f.dR[r] = host[r];
+        }
+    }
+    H->coef_uniform[dir][kind] = uni;
 }
 
 void free_handle_arrays(Handle* H) {
@@ -412,6 +619,10 @@ int weno_sb_array_info(int handle, int which, void** dev_ptr, int64_t* n_elem, i
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
     if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
     if (dev_ptr) *dev_ptr = H->arr[which];
+    // the caller may now write the array directly: stop trusting the
+    // uniformity recorded at upload
+    if (dev_ptr && which >= WENO_SB_A_POLYL(0))
+        H->coef_uniform[(which - WENO_SB_A_POLYL(0)) % 3][(which - WENO_SB_A_POLYL(0)) / 3] = false;
     if (n_elem) *n_elem = H->n[which];
     if (dtype) *dtype = H->dtype[which];
     return WENO_SB_OK;
@@ -424,6 +635,7 @@ int weno_sb_upload(int handle, int which, const double* host) {
     if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
     if (!host) return set_err(WENO_SB_ERR_ARG, "host pointer is NULL");
     const long long n = H->n[which];
+    if (which >= WENO_SB_A_POLYL(0)) note_coefficients(H, which, host);
     if (H->dtype[which] == WENO_SB_FP64) {
         WSB_CUDA(cudaMemcpyAsync(H->arr[which], host, sizeof(double) * n, cudaMemcpyHostToDevice, H->stream));
     } else {
@@ -523,6 +735,60 @@ int weno_sb_weno_dev(const weno_sb_grid* g, int dir, int order, unsigned flags, 
     return run_weno<float>(d, g, dir, order, flags, (const float*)v_in, coefs, (float*)vL, (float*)vR, st);
 }
 
+int weno_sb_weno_uniform_dev(const weno_sb_grid* g, int dir, int order, unsigned flags, int dtype,
+                             const void* v_in, const weno_sb_face_coefs* face, void* vL, void* vR, void* stream) {
+    WSB_FAULT("launch");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc || (rc = check_dir(dir)) || (rc = check_dtype(dtype))) return rc;
+    if (order != 3 && order != 5 && order != 7)
+        return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
+    if (flags & ~(WENO_SB_F_SPLIT | WENO_SB_F_SPECIALIZED | WENO_SB_F_MP | WENO_SB_F_FOLDED))
+        return set_err(WENO_SB_ERR_ARG, "unknown flag bits 0x%x", flags);
+    if (!v_in || !vL || !vR || !face) return set_err(WENO_SB_ERR_ARG, "NULL pointer");
+    if ((flags & WENO_SB_F_FOLDED) && dtype != WENO_SB_FP64)
+        return set_err(WENO_SB_ERR_UNSUPPORTED, "the folded form reads the FP64 v_vf; use dtype FP64");
+    double ucf[56];
+    build_ucf(order, face, ucf);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == WENO_SB_FP64)
+        return run_weno<double>(d, g, dir, order, flags, (const double*)v_in, nullptr, (double*)vL, (double*)vR, st,
+                                ucf);
+    return run_weno<float>(d, g, dir, order, flags, (const float*)v_in, nullptr, (float*)vL, (float*)vR, st, ucf);
+}
+
+int weno_sb_vjp_dev(const weno_sb_grid* g, int dir, int order, unsigned flags, const double* v_in,
+                    const weno_sb_coefs* coefs, const weno_sb_face_coefs* face, const double* gL, const double* gR,
+                    double* gv, void* stream) {
+    WSB_FAULT("launch");
+    Dims d;
+    int rc = check_grid(g, &d);
+    if (rc || (rc = check_dir(dir))) return rc;
+    if (order != 3 && order != 5 && order != 7)
+        return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
+    if (flags & ~(WENO_SB_F_SPLIT | WENO_SB_F_SPECIALIZED | WENO_SB_F_MP | WENO_SB_F_FOLDED | WENO_SB_F_ACCUMULATE))
+        return set_err(WENO_SB_ERR_ARG, "unknown flag bits 0x%x", flags);
+    if (g->scheme != WENO_SB_JS && g->scheme != WENO_SB_TENO)
+        return set_err(WENO_SB_ERR_UNSUPPORTED, "the adjoint covers the JS and TENO weights (scheme %d)", g->scheme);
+    if (order == 3 && g->scheme == WENO_SB_TENO)
+        return set_err(WENO_SB_ERR_UNSUPPORTED, "WENO3 has no TENO weights (its forward output is NaN)");
+    if (!v_in || !gL || !gR || !gv) return set_err(WENO_SB_ERR_ARG, "NULL pointer");
+    if ((coefs == nullptr) == (face == nullptr))
+        return set_err(WENO_SB_ERR_ARG, "pass exactly one of coefs (device arrays) and face (host values)");
+    CoefPtrs cp{nullptr, nullptr, nullptr, nullptr, nullptr};
+    double ucf[56];
+    const double* up = nullptr;
+    if (coefs) {
+        if (!coefs->polyL || !coefs->polyR || !coefs->dL || !coefs->dR || !coefs->beta_coef)
+            return set_err(WENO_SB_ERR_ARG, "NULL coefficient pointer");
+        cp = CoefPtrs{coefs->polyL, coefs->polyR, coefs->dL, coefs->dR, coefs->beta_coef};
+    } else {
+        build_ucf(order, face, ucf);
+        up = ucf;
+    }
+    return launch_vjp(d, g, dir, order, flags, v_in, cp, up, gL, gR, gv, (cudaStream_t)stream);
+}
+
 int weno_sb_preserve_monotonicity_dev(const weno_sb_grid* g, int dir, int dtype, const void* v_rs_ws,
                                       void* vL, void* vR, void* stream) {
     WSB_FAULT("launch");
@@ -584,6 +850,11 @@ int weno_sb_weno(int handle, int dir, int order, unsigned flags) {
                      (const double*)H->arr[WENO_SB_A_DL(dir)], (const double*)H->arr[WENO_SB_A_DR(dir)],
                      (const double*)H->arr[WENO_SB_A_BETA(dir)]};
     const void* in = (flags & WENO_SB_F_FOLDED) ? H->arr[WENO_SB_A_V_VF] : H->arr[WENO_SB_A_RS(dir)];
+    bool uni = true;
+    for (int k = 0; k < 5; ++k) uni = uni && H->coef_uniform[dir][k];
+    if (uni && getenv("WENO_SB_PER_FACE") == nullptr)
+        return weno_sb_weno_uniform_dev(&H->grid, dir, order, flags, H->precision, in, &H->face0[dir],
+                                        H->arr[WENO_SB_A_VL(dir)], H->arr[WENO_SB_A_VR(dir)], H->stream);
     return weno_sb_weno_dev(&H->grid, dir, order, flags, H->precision, in, &cf, H->arr[WENO_SB_A_VL(dir)],
                             H->arr[WENO_SB_A_VR(dir)], H->stream);
 }
@@ -662,6 +933,155 @@ int weno_sb_checksum_noalloc(int dtype, const void* const* arrays, const int64_t
         abs_sum_final_kernel<<<1, kSumThreads, 0, st>>>(part, kSumBlocks, d_results + a);
     }
     return cuda_err(cudaGetLastError(), "checksum (no-alloc) launch");
+}
+
+int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
+    WSB_FAULT("init");
+    if (!blocks || n < 1 || !batch) return set_err(WENO_SB_ERR_ARG, "need at least one block and a batch pointer");
+    Batch* B = new Batch;
+    cudaGetDevice(&B->device);
+    for (int i = 0; i < n; ++i) {
+        const weno_sb_block& b = blocks[i];
+        Dims d;
+        int rc = check_grid(&b.grid, &d);
+        if (!rc) rc = check_dir(b.dir);
+        if (!rc) rc = check_dtype(b.dtype);
+        if (!rc && b.order != 3 && b.order != 5 && b.order != 7)
+            rc = set_err(WENO_SB_ERR_ARG, "block %d: order must be 3, 5 or 7", i);
+        if (!rc && (b.flags & ~(WENO_SB_F_MP | WENO_SB_F_FOLDED | WENO_SB_F_SPLIT | WENO_SB_F_SPECIALIZED)))
+            rc = set_err(WENO_SB_ERR_ARG, "block %d: unknown flag bits 0x%x", i, b.flags);
+        if (!rc && (!b.v_in || !b.vL || !b.vR || !b.coefs.polyL || !b.coefs.polyR || !b.coefs.dL ||
+                    !b.coefs.dR || !b.coefs.beta_coef))
+            rc = set_err(WENO_SB_ERR_ARG, "block %d: NULL pointer", i);
+        if (rc) {
+            delete B;
+            return rc;
+        }
+        BatchEntry e{};
+        e.g = make_geom(d, b.dir, (b.flags & WENO_SB_F_FOLDED) != 0);
+        e.in = b.v_in;
+        e.vL = b.vL;
+        e.vR = b.vR;
+        e.cp = CoefPtrs{b.coefs.polyL, b.coefs.polyR, b.coefs.dL, b.coefs.dR, b.coefs.beta_coef};
+        e.wp = WenoParams{b.grid.scheme, b.grid.weno_eps, b.grid.teno_CT};
+        e.order = b.order;
+        e.mp = (b.flags & WENO_SB_F_MP) ? 1 : 0;
+        e.fp32 = b.dtype == WENO_SB_FP32;
+        e.o_first = (b.order == 3) ? 0 : 3;
+        e.nf = (int)((b.order == 3) ? e.g.ns : e.g.nc);
+        B->blocks.push_back(b);
+        B->entries.push_back(e);
+    }
+    int rc = cuda_err(cudaMalloc((void**)&B->d_entries, sizeof(BatchEntry) * n), "cudaMalloc");
+    if (!rc) rc = cuda_err(cudaMalloc((void**)&B->d_counter, sizeof(unsigned long long)), "cudaMalloc");
+    if (!rc) rc = cuda_err(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!rc) rc = batch_layout(B, 128, 8);
+    if (rc) {
+        if (B->d_entries) cudaFree(B->d_entries);
+        if (B->d_counter) cudaFree(B->d_counter);
+        if (B->cap) cudaStreamDestroy(B->cap);
+        delete B;
+        return rc;
+    }
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    g_batches.push_back(B);
+    *batch = (int)g_batches.size();
+    return WENO_SB_OK;
+}
+
+int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_item, double* best_ms) {
+    Batch* B = get_batch(batch);
+    if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned long long sig = batch_signature(B);
+    const char* cache = getenv("WENO_SB_TUNE_CACHE");
+    if (cache && *cache) {
+        std::ifstream f(cache);
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream ls(line);
+            unsigned long long h;
+            int t, u;
+            double ms;
+            if ((ls >> std::hex >> h >> std::dec >> t >> u >> ms) && h == sig) {
+                int rc = batch_layout(B, t, u);
+                if (rc) return rc;
+                if (threads) *threads = t;
+                if (cols_per_item) *cols_per_item = u;
+                if (best_ms) *best_ms = ms;
+                return WENO_SB_OK;
+            }
+        }
+    }
+    static const int cand_t[] = {64, 128, 256};
+    static const int cand_u[] = {4, 8, 16, 32};
+    cudaEvent_t e0, e1;
+    WSB_CUDA(cudaEventCreate(&e0));
+    WSB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bt = 128, bu = 8;
+    for (int t : cand_t) {
+        for (int u : cand_u) {
+            int rc = batch_layout(B, t, u);
+            if (!rc) rc = batch_enqueue(B, st);  // warm-up
+            if (rc) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return rc;
+            }
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < 3; ++r) batch_enqueue(B, st);
+            cudaEventRecord(e1, st);
+            WSB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= 3.f;
+            if (ms < best) {
+                best = ms;
+                bt = t;
+                bu = u;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc = batch_layout(B, bt, bu);
+    if (rc) return rc;
+    if (cache && *cache) {
+        std::ofstream f(cache, std::ios::app);
+        f << std::hex << sig << std::dec << " " << bt << " " << bu << " " << best << "\n";
+    }
+    if (threads) *threads = bt;
+    if (cols_per_item) *cols_per_item = bu;
+    if (best_ms) *best_ms = best;
+    return WENO_SB_OK;
+}
+
+int weno_sb_batch_launch(int batch, void* stream) {
+    WSB_FAULT("launch");
+    Batch* B = get_batch(batch);
+    if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
+    if (!B->exec) {
+        int rc = batch_build_graph(B);
+        if (rc) return rc;
+    }
+    return cuda_err(cudaGraphLaunch(B->exec, (cudaStream_t)stream), "cudaGraphLaunch");
+}
+
+int weno_sb_batch_destroy(int batch) {
+    Batch* B = get_batch(batch);
+    if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
+    cudaStreamSynchronize(B->cap);
+    batch_release_graph(B);
+    cudaFree(B->d_entries);
+    cudaFree(B->d_counter);
+    cudaStreamDestroy(B->cap);
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        g_batches[batch - 1] = nullptr;
+    }
+    delete B;
+    return WENO_SB_OK;
 }
 
 int weno_sb_selftest_rcp(const double* d_x, double* d_fast, double* d_ieee, int64_t n, void* stream) {
