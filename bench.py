@@ -295,6 +295,17 @@ def run_ours(args):
     # end-to-end through the handle API with pinned host buffers
     e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev) if not args.no_extras else None
 
+    # the other workloads of the path (adjoint, batched blocks, mixed precision)
+    adjoint = batched = mixed = None
+    if not args.no_extras and rank == 0:
+        Kx = max(3, min(K, 10))
+        adjoint = measure_adjoint(dev, Kx)
+        torch.cuda.empty_cache()
+        batched = measure_batched(dev, Kx)
+        torch.cuda.empty_cache()
+        mixed = measure_mixed_precision(dev, Kx)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_reference_run(steps=1, warmup=0, sample_nv=1)
@@ -329,6 +340,12 @@ def run_ours(args):
             line["drop_in"] = drop
         if e2e:
             line["e2e"] = e2e
+        if adjoint:
+            line["adjoint"] = adjoint
+        if batched:
+            line["batched"] = batched
+        if mixed:
+            line["mixed_precision"] = mixed
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "face-states/s", "cores": cpu["cores"],
                                     "kind": "port", "sample": cpu["sample"]}
@@ -473,6 +490,193 @@ def measure_e2e(g, vf_host, coefs, K, dev):
     return {"value": fs / dt, "unit": "face-states/s", "h2d_bytes_per_step": int(vf_host.nbytes),
             "d2h_bytes_per_step": int(6 * nface * 8), "ms_per_step": dt * 1e3, "steps": K,
             "path": "weno_sb_upload -> weno_sb_weno x3 (folded, MP) -> weno_sb_download x6, pinned host buffers"}
+
+
+def _time_steps(step, stream, K, warm=3):
+    """Mean device time of `step` over K calls (CUDA events on `stream`)."""
+    import torch
+    for _ in range(warm):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / K
+
+
+def measure_adjoint(dev, K):
+    """Adjoint of FP64 WENO5-JS + MP in x/y/z at 128^3 cells x 5 variables:
+    forward = three folded sweeps; backward = three VJP sweeps accumulating
+    the gradient of v_vf (beta and the weights recomputed, nothing stored).
+    Cotangents N(0,1) from a seeded generator; smooth sinusoidal input."""
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api, fields
+    m, nv = 127, 5
+    g = wsb.Grid(m, m, m, nv, BUFF)
+    stream = torch.cuda.Stream(device=dev)
+    sp = int(stream.cuda_stream)
+    v = fields.sinusoid_shock_field_dev(m, m, m, nv, BUFF, seed=4, shock=False, device=dev)
+    faces = [api.face_coefs(fields.uniform_weno_coefficients(5, g.nc(d))) for d in range(3)]
+    nface = int(np.prod(g.face_shape(0)))
+    gen = torch.Generator(device=dev).manual_seed(8)
+    gs = [(torch.randn(nface, generator=gen, device=dev, dtype=torch.float64),
+           torch.randn(nface, generator=gen, device=dev, dtype=torch.float64)) for _ in range(3)]
+    outs = (torch.empty(nface, dtype=torch.float64, device=dev), torch.empty(nface, dtype=torch.float64, device=dev))
+    gv = torch.empty_like(v)
+    fl = wsb.F_MP | wsb.F_FOLDED
+
+    def fwd():
+        for d in range(3):
+            api.weno_uniform(g, d, 5, v, faces[d], outs[0], outs[1], flags=fl, stream=sp)
+
+    def bwd():
+        for d in range(3):
+            api.vjp(g, d, 5, v, faces[d], gs[d][0], gs[d][1], gv, stream=sp, uniform=True,
+                    flags=fl | (wsb.F_ACCUMULATE if d > 0 else 0))
+
+    f_ms = _time_steps(fwd, stream, K)
+    b_ms = _time_steps(bwd, stream, K)
+    return {"workload": "VJP of FP64 WENO5-JS + MP, x/y/z, 128^3 cells x 5 vars, folded input, "
+                        "uniform coefficients, cotangents N(0,1)",
+            "forward_ms": f_ms, "vjp_ms": b_ms, "vjp_over_forward": b_ms / f_ms, "target_ratio": 2.5}
+
+
+def _batch_blocks(n_blocks=96, seed=96):
+    """Block shapes of the batched workload: cells per axis uniform in
+    16..112, v_size from {5, 8, 10}, order from {3, 5, 7}, JS or TENO."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_blocks):
+        cells = [int(c) for c in rng.integers(16, 113, 3)]
+        nv = int(rng.choice([5, 8, 10]))
+        order = int(rng.choice([3, 5, 7]))
+        scheme = 0 if order == 3 else int(rng.choice([0, 3]))
+        out.append((cells, nv, order, scheme))
+    return out
+
+
+def measure_batched(dev, K):
+    """96 uneven blocks (x/y/z sweeps each, MP fused, folded input) as one
+    persistent launch in a CUDA graph with autotuned tiles, FP64 and
+    FP32-bulk; FP64 also as one launch per sweep for comparison."""
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api, fields
+    stream = torch.cuda.Stream(device=dev)
+    sp = int(stream.cuda_stream)
+    blocks = _batch_blocks()
+    res = {"workload": "96 blocks, cells per axis U{16..112}, v_size {5,8,10}, order {3,5,7}, JS/TENO "
+                       "(teno_CT 1e-5), smooth-plus-jump fields, x/y/z sweeps + MP each = 288 sweeps",
+           "blocks": len(blocks)}
+    for dt_name, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        entries, fs = [], 0
+        for i, (cells, nv, order, scheme) in enumerate(blocks):
+            m, n, p = (c - 1 for c in cells)
+            g = wsb.Grid(m, n, p, nv, BUFF, scheme=scheme)
+            v = fields.smooth_jump_field_dev(m, n, p, nv, BUFF, seed=100 + i, device=dev).to(dt)
+            for d in range(3):
+                cf = tuple(torch.from_numpy(np.ascontiguousarray(c.ravel(order="F"))).to(dev)
+                           for c in fields.uniform_weno_coefficients(order, g.nc(d)))
+                nface = int(np.prod(g.face_shape(d)))
+                L = torch.empty(nface, dtype=dt, device=dev)
+                R = torch.empty(nface, dtype=dt, device=dev)
+                entries.append(dict(grid=g, dir=d, order=order, flags=wsb.F_MP | wsb.F_FOLDED, v_in=v,
+                                    coefs=cf, vL=L, vR=R))
+                ns, c1, c2 = g.extents(d)
+                nf = ns if order == 3 else ns - 6
+                fs += 2 * nf * c1 * c2 * nv
+        b = api.Batch(entries)
+        try:
+            t, u, tune_ms = b.autotune(stream=sp)
+            ms = _time_steps(lambda: b.launch(stream=sp), stream, K)
+        finally:
+            b.close()
+        r = {"ms_per_step": ms, "value": fs / (ms * 1e-3), "face_states": fs, "tile": {"threads": t, "cols": u},
+             "launches_per_step": 1}
+        if dt == torch.float64:
+            structs = [api.coefs_struct(e["coefs"]) for e in entries]
+
+            def seq():
+                for e, cs in zip(entries, structs):
+                    api.weno(e["grid"], e["dir"], e["order"], e["v_in"], cs, e["vL"], e["vR"],
+                             flags=e["flags"], stream=sp)
+            sms = _time_steps(seq, stream, K)
+            r["one_launch_per_sweep"] = {"ms_per_step": sms, "value": fs / (sms * 1e-3),
+                                         "launches_per_step": len(entries)}
+        res[dt_name] = r
+        del entries
+    return res
+
+
+def measure_mixed_precision(dev, K):
+    """FP32-bulk against FP64 on 256^3 cells x 10 variables: WENO5 and WENO7
+    + MP in x/y/z, FP32 fields (FP64-generated sinusoids, modes 1-8, plus a
+    planar shock of jump ratio 5 at a seeded orientation, downcast) and FP32
+    face states.  Error per output array against the FP64 path (which the
+    parity tests hold to 1e-12 of the oracle): max-norm relative and RMS
+    relative over the core faces; smooth (no shock) and shocked data."""
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api, fields
+    m, nv = 255, 10
+    g = wsb.Grid(m, m, m, nv, BUFF)
+    stream = torch.cuda.Stream(device=dev)
+    sp = int(stream.cuda_stream)
+    nface = int(np.prod(g.face_shape(0)))
+    ns = g.extents(0)[0]
+    o64 = (torch.empty(nface, dtype=torch.float64, device=dev), torch.empty(nface, dtype=torch.float64, device=dev))
+    o32 = (torch.empty(nface, dtype=torch.float32, device=dev), torch.empty(nface, dtype=torch.float32, device=dev))
+    rs32 = torch.empty(int(np.prod(g.rs_shape(0))), dtype=torch.float32, device=dev)
+    res = {"workload": "256^3 cells x 10 vars, x/y/z + MP, FP32 fields and face states vs FP64",
+           "error_reference": "FP64 sweeps of the same inputs (held to 1e-12 of the oracle by the tests)"}
+    for order in (5, 7):
+        faces = [api.face_coefs(fields.uniform_weno_coefficients(order, g.nc(d))) for d in range(3)]
+        for shock in (False, True):
+            v = fields.sinusoid_shock_field_dev(m, m, m, nv, BUFF, seed=11, shock=shock, device=dev)
+            arrays = {}
+            for d in range(3):
+                api.weno_uniform(g, d, order, v, faces[d], o64[0], o64[1], flags=wsb.F_MP | wsb.F_FOLDED, stream=sp)
+                api.reshape(g, d, v, rs32, stream=sp)
+                api.weno_uniform(g, d, order, rs32, faces[d], o32[0], o32[1], flags=wsb.F_MP, stream=sp)
+                torch.cuda.synchronize()
+                for nm, a, b in (("vL", o64[0], o32[0]), ("vR", o64[1], o32[1])):
+                    A = a.view(-1, ns)[:, 3:ns - 3]
+                    B = b.view(-1, ns)[:, 3:ns - 3].double()
+                    den = float(A.abs().max())
+                    diff = (A - B)
+                    arrays[f"{nm}_{'xyz'[d]}"] = {
+                        "max_rel": float(diff.abs().max()) / den,
+                        "rms_rel": float(diff.pow(2).mean().sqrt() / A.pow(2).mean().sqrt())}
+            res[f"weno{order}_{'shock' if shock else 'smooth'}"] = {
+                "max_rel_worst": max(x["max_rel"] for x in arrays.values()),
+                "rms_rel_worst": max(x["rms_rel"] for x in arrays.values()), "per_array": arrays}
+            if not shock:
+                def s64():
+                    for d in range(3):
+                        api.weno_uniform(g, d, order, v, faces[d], o64[0], o64[1],
+                                         flags=wsb.F_MP | wsb.F_FOLDED, stream=sp)
+                rsd = [torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float32, device=dev) for d in range(3)]
+                for d in range(3):
+                    api.reshape(g, d, v, rsd[d], stream=sp)
+
+                def s32():
+                    for d in range(3):
+                        api.weno_uniform(g, d, order, rsd[d], faces[d], o32[0], o32[1], flags=wsb.F_MP, stream=sp)
+                t64 = _time_steps(s64, stream, K)
+                t32 = _time_steps(s32, stream, K)
+                fs = 3 * face_states_per_dir(m=m, nv=nv)
+                res[f"weno{order}_speed"] = {"fp64_ms": t64, "fp32_ms": t32, "fp32_over_fp64": t64 / t32,
+                                             "fp64_value": fs / (t64 * 1e-3), "fp32_value": fs / (t32 * 1e-3)}
+                del rsd
+            del v
+    return res
 
 
 def main():

@@ -1,9 +1,10 @@
 """Adjoint (VJP) of the reconstruction sweep through the C ABI.
 
 Checked three ways: against forward-mode dual-number differentiation of the
-reference formulas (oracle/weno_oracle_ad.cpp) at 1e-11 max-norm relative
-error; against central finite differences (step 1e-6, smooth data, JS) to
-1e-6; and with torch.autograd.gradcheck through a ctypes autograd wrapper.
+reference formulas (oracle/weno_oracle_ad.cpp) at 1e-9 max-norm relative (1e-8 for WENO3)
+error; against central finite differences (unit-norm direction, step 1e-4,
+smooth data, JS and TENO, with and without MP, cells near kinks held fixed)
+to 1e-6; and with torch.autograd.gradcheck through a ctypes autograd wrapper.
 """
 import numpy as np
 import pytest
@@ -97,13 +98,11 @@ def test_vjp_folded_accumulates_three_sweeps(wsb, oracle_mod):
     assert rel_err(from_dev(gv, vf.shape), ref) <= TOL_AD
 
 
-def _mp_safe_cells(rs, L, R, margin=1e-3, half_width=2):
-    """Mask rule for the finite-difference check: a core face is safe when
-    its WENO states lie inside the MP bounds (f90:1564-1608) with `margin`
-    to spare on both sides, so a perturbation of size ~1e-6 keeps the limiter
-    on the same (pass-through) branch.  A cell is perturbed only if every
-    face whose stencil (+-half_width: 2 for WENO5, 3 for WENO7) contains it
-    is safe."""
+def _mp_bad_faces(rs, L, R, margin=1e-3):
+    """Faces near a limiter kink: a core face is safe when its WENO states lie
+    inside the MP bounds (f90:1564-1608) with `margin` to spare on both sides,
+    so a perturbation of ~1e-9 per cell keeps the limiter on its pass-through
+    branch.  Returns the unsafe faces as a (ns, c1, c2, V) mask."""
     ns = rs.shape[0] - 6
     o = np.arange(3, ns - 3)
     v = {k: rs[o + 3 + k] for k in range(-2, 3)}
@@ -131,19 +130,34 @@ def _mp_safe_cells(rs, L, R, margin=1e-3, half_width=2):
         safe &= (x - lo > margin) & (hi - x > margin)
     bad_face = np.zeros((ns,) + rs.shape[1:], dtype=bool)
     bad_face[3:ns - 3] = ~safe
-    bad_cell = np.zeros(rs.shape, dtype=bool)
+    return bad_face
+
+
+def _cells_clear_of(bad_face, rs_shape, half_width):
+    """Cells outside every bad face's stencil (+-half_width: 2 for WENO5,
+    3 for WENO7)."""
+    ns = bad_face.shape[0]
+    bad_cell = np.zeros(rs_shape, dtype=bool)
     for k in range(-half_width, half_width + 1):
         bad_cell[3 + k:ns + 3 + k] |= bad_face
     return ~bad_cell
 
 
-@pytest.mark.parametrize("mp", [False, True])
-@pytest.mark.parametrize("order", [5, 7])
-def test_vjp_central_differences(wsb, oracle_mod, order, mp):
+def _mp_safe_cells(rs, L, R, margin=1e-3, half_width=2):
+    return _cells_clear_of(_mp_bad_faces(rs, L, R, margin), rs.shape, half_width)
+
+
+# TENO7 is left out: the reference's beta(4) term (f90:1489-1491) outweighs
+# every stencil, so its faces and their gradient are identically zero.
+@pytest.mark.parametrize("order,scheme,mp", [(5, 0, False), (5, 0, True), (7, 0, False), (7, 0, True),
+                                             (5, 3, False), (5, 3, True)])
+def test_vjp_central_differences(wsb, oracle_mod, order, scheme, mp):
     """<gv, dv> against (F(v+h dv) - F(v-h dv)) . g / 2h with h = 1e-4 along a
     random unit-norm direction dv, on the smooth 128^3-cell, v_size=5 input,
-    JS weights, cotangents N(0,1).  With MP, dv is zero on the cells
-    _mp_safe_cells excludes (limiter kinks).  Bar: 1e-6 relative.
+    cotangents N(0,1), JS or TENO (teno_CT=1e-5) weights.  dv is zero on the
+    cells whose stencils reach a kink: MP faces that _mp_bad_faces flags, and
+    TENO faces whose output changes when teno_CT moves by a factor of 2 (a
+    stencil within reach of the cutoff).  Bar: 1e-6 relative.
 
     h: dv is spread over ~1e7 cells, so a cell moves by ~h * 3e-4, far inside
     the 1e-3 limiter margin, and the O(h^2) truncation stays near 1e-9; the
@@ -152,10 +166,11 @@ def test_vjp_central_differences(wsb, oracle_mod, order, mp):
     import torch
     from wenostandalone_b200 import api, fields
     m = 127
-    g = wsb.Grid(m, m, m, 5, 6)
+    g = wsb.Grid(m, m, m, 5, 6, scheme=scheme)
     vf = fields.sinusoid_shock_field(m, m, m, 5, 6, seed=4, shock=False)
     gen = torch.Generator(device="cuda").manual_seed(8)
     flags = wsb.F_MP if mp else 0
+    hw = (order - 1) // 2
     for d in range(3):
         coefs_np = fields.uniform_weno_coefficients(order, g.nc(d))
         coefs = tuple(to_dev(c) for c in coefs_np)
@@ -167,13 +182,23 @@ def test_vjp_central_differences(wsb, oracle_mod, order, mp):
         gv = torch.empty_like(rs)
         api.vjp(g, d, order, rs, coefs, gL, gR, gv, flags=flags)
         dv = torch.randn(rs.numel(), generator=gen, device="cuda", dtype=torch.float64)
-        if mp:
+
+        def faces(grid):
             Lw = torch.zeros(n, dtype=torch.float64, device="cuda")
             Rw = torch.zeros_like(Lw)
-            api.weno(g, d, order, rs, coefs, Lw, Rw)
-            mask = _mp_safe_cells(rs_np, from_dev(Lw, g.face_shape(d)), from_dev(Rw, g.face_shape(d)),
-                                  half_width=max(2, (order - 1) // 2))
-            assert mask.mean() > 0.3  # most of the smooth field is limiter-free
+            api.weno(grid, d, order, rs, coefs, Lw, Rw)
+            return from_dev(Lw, g.face_shape(d)), from_dev(Rw, g.face_shape(d))
+
+        bad = np.zeros((g.extents(d)[0],) + rs_np.shape[1:], dtype=bool)
+        if scheme == 3:
+            lo = faces(wsb.Grid(m, m, m, 5, 6, scheme=3, teno_CT=g.teno_CT * 0.5))
+            hi = faces(wsb.Grid(m, m, m, 5, 6, scheme=3, teno_CT=g.teno_CT * 2.0))
+            bad |= (lo[0] != hi[0]) | (lo[1] != hi[1])
+        if mp:
+            bad |= _mp_bad_faces(rs_np, *faces(g))
+        if scheme == 3 or mp:
+            mask = _cells_clear_of(bad, rs_np.shape, hw)
+            assert mask.mean() > 0.3  # most of the smooth field is away from kinks
             dv = dv * to_dev(mask.astype(np.float64))
         dv = dv / torch.linalg.vector_norm(dv)
         h = 1e-4

@@ -304,3 +304,64 @@ def uniform_weno_coefficients(order: int, nc: int):
     bca = np.empty((nc, 5, 6), order="F")
     bca[:] = beta[None]
     return polyL, polyR, dLa, dRa, bca
+
+
+# ---------------------------------------------------------------------------
+# Device-side generators (torch) for large benchmark inputs: the same
+# formulas as above, evaluated on the GPU in FP64; the noise comes from a
+# seeded torch generator instead of splitmix64, so values match the numpy
+# generators in distribution, not bit for bit.  Returned flat in Fortran
+# order (x fastest), shape (N1+6)(N2+6)(N3+6)V.
+# ---------------------------------------------------------------------------
+def _centres_t(cells, buff, device):
+    import torch
+    i = torch.arange(-buff - 3, cells + buff + 3, dtype=torch.float64, device=device)
+    return (i + 0.5) / cells
+
+
+def sinusoid_shock_field_dev(m, n, p, nv, buff, seed=0, ratio=5.0, shock=True, device="cuda"):
+    """Device version of sinusoid_shock_field (same modes, directions, phases
+    and shock plane for a given seed)."""
+    import torch
+    x = _centres_t(m + 1, buff, device)
+    y = _centres_t(n + 1, buff, device)
+    z = _centres_t(p + 1, buff, device)
+    Zc, Y, X = torch.meshgrid(z, y, x, indexing="ij")  # C order (z, y, x): x fastest
+    rnd = splitmix64_uniform(seed ^ 0x5EED, 4 * 8 * nv + 3)
+    nrm = rnd[-3:] * 2.0 - 1.0
+    nrm = nrm / max(np.linalg.norm(nrm), 1e-12)
+    out = torch.empty((nv,) + tuple(X.shape), dtype=torch.float64, device=device)
+    side = (float(nrm[0]) * (X - 0.5) + float(nrm[1]) * (Y - 0.5) + float(nrm[2]) * (Zc - 0.5)) > 0.0
+    for q in range(nv):
+        f = torch.zeros_like(X)
+        for k in range(1, 9):
+            base = 4 * (8 * q + (k - 1))
+            c = rnd[base:base + 3] * 2.0 - 1.0
+            c = c / max(np.linalg.norm(c), 1e-12)
+            phi = 2 * np.pi * rnd[base + 3]
+            f += torch.sin(2 * np.pi * k * (float(c[0]) * X + float(c[1]) * Y + float(c[2]) * Zc) + phi)
+        f = 1.0 + 0.5 * f / 8.0
+        if shock:
+            f = torch.where(side, f * ratio, f)
+        out[q] = f
+    return out.reshape(-1)
+
+
+def smooth_jump_field_dev(m, n, p, nv, buff, seed=0, noise=1e-3, jump=1.0, device="cuda"):
+    """Device version of smooth_jump_field (noise from a seeded torch
+    generator)."""
+    import torch
+    x = _centres_t(m + 1, buff, device)
+    y = _centres_t(n + 1, buff, device)
+    z = _centres_t(p + 1, buff, device)
+    gen = torch.Generator(device=device).manual_seed(int(seed))
+    cyz = torch.sin(2 * np.pi * z)[:, None, None] * torch.cos(2 * np.pi * y)[None, :, None]
+    out = torch.empty((nv, z.numel(), y.numel(), x.numel()), dtype=torch.float64, device=device)
+    for q in range(nv):
+        sx = torch.sin(2 * np.pi * (q + 1) * x)[None, None, :]
+        u = torch.rand(out.shape[1:], generator=gen, dtype=torch.float64, device=device)
+        f = 1.0 + 0.5 * sx * cyz + noise * (2.0 * u - 1.0)
+        if q % 2 == 1:
+            f = f + jump * (x > 0.5).to(torch.float64)[None, None, :]
+        out[q] = f
+    return out.reshape(-1)
