@@ -217,12 +217,23 @@ def run_ours(args):
     stream = torch.cuda.Stream(device=dev)
     sp = int(stream.cuda_stream)
     flags = wsb.F_MP | wsb.F_FOLDED
+    fp32_main = args.precision == "fp32"
+    if fp32_main:
+        # FP32-bulk as the timed step: FP32 v_rs_ws per direction (reshaped
+        # once, before timing) and FP32 face states
+        rs32 = [torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float32, device=dev) for d in range(3)]
+        for d in range(3):
+            api.reshape(g, d, v, rs32[d], stream=sp)
+        o32 = [(torch.empty(nface, dtype=torch.float32, device=dev),
+                torch.empty(nface, dtype=torch.float32, device=dev)) for _ in range(3)]
 
     def step(evs=None, per_face=False):
         for d in range(3):
             if evs is not None:
                 evs[d][0].record(stream)
-            if per_face:
+            if fp32_main:
+                api.weno_uniform(g, d, ORDER, rs32[d], faces[d], o32[d][0], o32[d][1], flags=wsb.F_MP, stream=sp)
+            elif per_face:
                 api.weno(g, d, ORDER, v, cstructs[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
             else:
                 api.weno_uniform(g, d, ORDER, v, faces[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
@@ -265,12 +276,12 @@ def run_ours(args):
     dk = int(np.argmax(sums))
     dk_ms = sums[dk] / K
     peak, peak_kind = load_peaks()
-    ab = alg_bytes_per_sweep()
+    ab = alg_bytes_per_sweep(elem=4 if fp32_main else 8)
     achieved = ab / (dk_ms * 1e-3) / 1e9
 
     # the same step with per-face coefficient arrays (stretched-grid form)
     per_face = None
-    if not args.no_extras:
+    if not args.no_extras and not fp32_main:
         for _ in range(3):
             step(per_face=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -286,18 +297,18 @@ def run_ours(args):
 
     # FP32-bulk variant (same sweeps, FP32 v_rs_ws field and face states)
     fp32 = None
-    if not args.no_extras:
+    if not args.no_extras and not fp32_main:
         fp32 = measure_fp32_bulk(g, v, faces, outs, stream, K, dev)
         drop = measure_drop_in(g, v, faces, outs, stream, K, dev)
     else:
         drop = None
 
     # end-to-end through the handle API with pinned host buffers
-    e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev) if not args.no_extras else None
+    e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev) if not (args.no_extras or fp32_main) else None
 
     # the other workloads of the path (adjoint, batched blocks, mixed precision)
     adjoint = batched = mixed = None
-    if not args.no_extras and rank == 0:
+    if not args.no_extras and rank == 0 and not fp32_main:
         Kx = max(3, min(K, 10))
         adjoint = measure_adjoint(dev, Kx)
         torch.cuda.empty_cache()
@@ -307,27 +318,32 @@ def run_ours(args):
         torch.cuda.empty_cache()
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu and not fp32_main:
         cpu = cpu_reference_run(steps=1, warmup=0, sample_nv=1)
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "face-states/s", "n_gpus": ws, "steps": K,
+            "metric": METRIC.replace("FP64", "FP32-bulk") if fp32_main else METRIC, "value": value, "unit": "face-states/s", "n_gpus": ws, "steps": K,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "FP64 WENO5-JS + MP fused, x/y/z sweeps reading v_vf directly "
-                                   "(reshape folded), 200^3 cells x 8 vars, buff_size 6",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-bulk" if fp32_main else "f64",
+            "data": "synthetic",
+            "config": {"workload": ("FP32-bulk WENO5-JS + MP (FP64 beta and weights), x/y/z sweeps of FP32 "
+                                    "v_rs_ws" if fp32_main else
+                                    "FP64 WENO5-JS + MP fused, x/y/z sweeps reading v_vf directly "
+                                    "(reshape folded)") + f", {M + 1}^3 cells x 8 vars, buff_size 6",
                        "m=n=p": M, "v_size": NV, "buff_size": BUFF, "coefficients": "uniform-grid WENO5-JS",
                        "field": "seeded smooth-plus-jump", "l2": "inputs (663 MB) and outputs (3.7 GB) exceed "
                                                                   "the 126 MB L2; no flush",
                        "parallelism": f"{ws} independent blocks (weak scaling, no collective)"},
-            "roofline": {"bound": "hbm", "kernel": f"sweep_pipe_kernel<5,MP,JS,uniform> {'xyz'[dk]} sweep "
-                                                   f"({'row tiles' if dk == 0 else '128B-swizzled column tiles'})",
+            "roofline": {"bound": "hbm", "kernel": (f"sweep_fast_kernel<5,MP,float,JS> {'xyz'[dk]} sweep"
+                                                    if fp32_main else
+                                                    f"sweep_pipe_kernel<5,MP,JS,uniform> {'xyz'[dk]} sweep "
+                                                    f"({'row tiles' if dk == 0 else '128B-swizzled column tiles'})"),
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "alg_bytes_per_launch": ab, "launch_ms": dk_ms,
-                         "traffic": read_traffic()},
+                         "traffic": None if (fp32_main or M != 199) else read_traffic()},
             "per_sweep_ms": [s / K for s in sums],
             "gpu_launches": 3 * K,
             "clocks": clk.summary(),
@@ -688,6 +704,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip FP32/drop-in/e2e side measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--m", type=int, default=199, help="cells per axis minus one (m=n=p); 199 = 200^3")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+                    help="fp32: time the FP32-bulk form as the main step (no extras)")
     args = ap.parse_args()
     global M
     M = args.m

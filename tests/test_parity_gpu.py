@@ -151,7 +151,7 @@ def test_face_varying_coefficients(wsb, oracle_mod, order, folded, mp, kernel):
             assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
 
 
-@pytest.mark.parametrize("kernel", ["auto", "cpasync", "generic"])
+@pytest.mark.parametrize("kernel", ["auto", "march", "tma", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
 @pytest.mark.parametrize("scheme", [0, 3])
@@ -363,7 +363,7 @@ def test_argument_errors(wsb):
     assert rc == L.ERR_ARG and "buff_size" in L.last_error()
 
 
-def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64"):
+def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64", entry="arrays"):
     import torch
     from wenostandalone_b200 import api, fields
     m = 47
@@ -380,7 +380,10 @@ def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64"):
     api.reshape(g, d, v, rs32)
     L = torch.zeros(int(np.prod(g.face_shape(d))), dtype=torch.float32, device="cuda")
     R = torch.zeros_like(L)
-    api.weno(g, d, order, rs32, tuple(to_dev(c) for c in coefs), L, R, flags=wsb.F_MP if mp else 0)
+    if entry == "uniform":
+        api.weno_uniform(g, d, order, rs32, coefs, L, R, flags=wsb.F_MP if mp else 0)
+    else:
+        api.weno(g, d, order, rs32, tuple(to_dev(c) for c in coefs), L, R, flags=wsb.F_MP if mp else 0)
     core = (slice(3, g.extents(d)[0] - 3),)
     out = []
     for got, ref in ((L, Lr), (R, Rr)):
@@ -390,25 +393,28 @@ def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64"):
     return out
 
 
+@pytest.mark.parametrize("entry", ["arrays", "uniform"])
 @pytest.mark.parametrize("order", [5, 7])
 @pytest.mark.parametrize("d", [0, 1, 2])
-def test_fp32_bulk_smooth_error(wsb, oracle_mod, order, d):
+def test_fp32_bulk_smooth_error(wsb, oracle_mod, order, d, entry):
     """FP32-bulk (FP32 fields and face states, FP32 stencil sums, FP64 beta and
     normalisation) on smooth data vs the FP64 oracle on the FP64 field:
-    max-norm relative error <= 1e-6 per array."""
-    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=False):
+    max-norm relative error <= 1e-6 per array (per-face coefficient arrays,
+    and the face-independent entry, which takes the marching kernel for WENO5)."""
+    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=False, entry=entry):
         assert mx <= 1e-6 and rms <= 1e-7, (mx, rms)
 
 
+@pytest.mark.parametrize("entry", ["arrays", "uniform"])
 @pytest.mark.parametrize("order", [5, 7])
 @pytest.mark.parametrize("d", [0, 1, 2])
-def test_fp32_bulk_with_mp_error(wsb, oracle_mod, order, d):
+def test_fp32_bulk_with_mp_error(wsb, oracle_mod, order, d, entry):
     """With the MP limiter the FP32 storage rounding of the field (2^-24) is
     amplified by the limiter's curvature bounds (|4 d0 - d1| has coefficient
     sum 20 over the stencil, times beta_mp = 4/3): against the FP64 field the
     bar is 4e-6 max / 1e-7 RMS.  Against the oracle run on the same
     FP32-rounded field (the arithmetic alone) it is 1e-6."""
-    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=True):
+    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=True, entry=entry):
         assert mx <= 4e-6 and rms <= 1e-7, (mx, rms)
-    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=True, field_for_oracle="fp32"):
+    for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=True, field_for_oracle="fp32", entry=entry):
         assert mx <= 1e-6, (mx, rms)

@@ -155,8 +155,11 @@ struct Swz128Tile {  // TMA box of 128-byte rows in the 128B swizzle pattern
 // case, so the other families' code is not carried); -1 reads it at run time.
 template <int ORDER, bool MPF, typename T, int SCH, typename Tile>
 __device__ __forceinline__ void compute_columns(const FastArgs& a, const Coef<ORDER>& cf, const Tile& t, int kb,
-                                                int ke, long long oidx0, long long o) {
+                                                int ke, long long oidx0, long long o,
+                                                const PolyF<ORDER>* pf = nullptr) {
     const int scheme = (SCH >= 0) ? SCH : a.wp.scheme;
+    // FP32-bulk with JS weights: the conversion-free mixed form
+    constexpr bool MIXED = (sizeof(T) == 4) && SCH == 0 && (ORDER == 5 || ORDER == 7);
     T* __restrict__ vL = (T*)a.vL;
     T* __restrict__ vR = (T*)a.vR;
     long long oidx = oidx0 + (long long)kb * a.o_sU;
@@ -170,20 +173,33 @@ __device__ __forceinline__ void compute_columns(const FastArgs& a, const Coef<OR
             if (MPF && o >= 3 && o <= a.ns - 4) MP<T>::apply(t(-2, k), t(-1, k), t(0, k), t(1, k), t(2, k), Lt, Rt);
         } else if constexpr (ORDER == 5) {
             const T m2 = t(-2, k), m1 = t(-1, k), z0 = t(0, k), p1 = t(1, k), p2 = t(2, k);
-            double L, R;
-            weno5_face<T>((double)m2, (double)m1, (double)z0, (double)p1, (double)p2, cf, scheme, a.wp.eps,
-                          a.wp.teno_ct, L, R);
-            Lt = (T)L;
-            Rt = (T)R;
+            bool done = false;
+            if constexpr (MIXED) done = weno5_js_mixed(m2, m1, z0, p1, p2, cf, *pf, a.wp.eps, Lt, Rt);
+            if (!done) {
+                double L, R;
+                weno5_face<T>((double)m2, (double)m1, (double)z0, (double)p1, (double)p2, cf, scheme, a.wp.eps,
+                              a.wp.teno_ct, L, R);
+                Lt = (T)L;
+                Rt = (T)R;
+            }
             if (MPF) MP<T>::apply(m2, m1, z0, p1, p2, Lt, Rt);
         } else {
-            double s7[7];
+            bool done = false;
+            if constexpr (MIXED) {
+                float s7[7];
 #pragma unroll
-            for (int q = 0; q < 7; ++q) s7[q] = (double)t(q - 3, k);
-            double L, R;
-            weno7_face<T>(s7 + 3, cf, scheme, a.wp.eps, a.wp.teno_ct, L, R);
-            Lt = (T)L;
-            Rt = (T)R;
+                for (int q = 0; q < 7; ++q) s7[q] = t(q - 3, k);
+                done = weno7_js_mixed(s7 + 3, cf, *pf, a.wp.eps, Lt, Rt);
+            }
+            if (!done) {
+                double s7[7];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) s7[q] = (double)t(q - 3, k);
+                double L, R;
+                weno7_face<T>(s7 + 3, cf, scheme, a.wp.eps, a.wp.teno_ct, L, R);
+                Lt = (T)L;
+                Rt = (T)R;
+            }
             if (MPF) MP<T>::apply(t(-2, k), t(-1, k), t(0, k), t(1, k), t(2, k), Lt, Rt);
         }
         vL[oidx] = Lt;
@@ -253,6 +269,8 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(c
         if (a.cp.polyL) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, cidx);
         else cf = *reinterpret_cast<const Coef<ORDER>*>(a.ucf);  // face-independent coefficients
     }
+    PolyF<ORDER> pf;  // float polynomial coefficients of the FP32-bulk form
+    if constexpr (sizeof(T) == 4) pf.from(cf);
 
     const int js = (KIND == 0) ? 1 : a.pitch;     // smem stride along the sweep
     const int ks = (KIND == 0) ? a.pitch : 1;     // smem stride between columns
@@ -276,7 +294,7 @@ __global__ void __launch_bounds__(256, (ORDER == 7 ? 1 : 2)) sweep_fast_kernel(c
         if (!active) continue;
         const GroupInfo gi = group_info(a, grp);
         const LinearTile<T> tile{smem + (it % STAGES) * stage_elems + (f + H) * js, js, ks};
-        compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, 0, gi.ucnt, gi.out0 + o, o);
+        compute_columns<ORDER, MPF, T, SCH>(a, cf, tile, 0, gi.ucnt, gi.out0 + o, o, &pf);
     }
     cp_async_wait<0>();
 }

@@ -100,28 +100,34 @@ __device__ __forceinline__ double mp_side_vjp(bool left, const double* v, double
     const double UL = left ? fma(-2.0, dF, v0) : fma(2.0, dF, v0);
     const double MD = ((v0 + vn) - mMD) * 0.5;
     const double LC = left ? fma(kBetaMP, mLC, fma(-0.5, dF, v0)) : fma(kBetaMP, mLC, fma(0.5, dF, v0));
-    // candidates: 0 v0, 1 vn, 2 MD, 3 UL, 4 LC
-    const double cand[5] = {v0, vn, MD, UL, LC};
-    const double dN = left ? v0 - vn : vn - v0;   // >= 0 <=> vn <= v0 (left)
-    const bool n_low = left ? (__double2hiint(dN) >= 0) : !(__double2hiint(dN) >= 0);
-    // min/max(v0, vn)
-    const int mn1 = (left ? __double2hiint(dN) >= 0 : __double2hiint(dN) < 0) ? 1 : 0;
-    (void)n_low;
-    const int mx1 = 1 - mn1;
+    // candidates: 0 v0, 1 vn, 2 MD, 3 UL, 4 LC, carried as (value, code)
+    // pairs through the min/max selections (no indexed array, so nothing
+    // goes to local memory)
+    const double dN = left ? v0 - vn : vn - v0;
+    const bool vn_low = left ? (__double2hiint(dN) >= 0) : (__double2hiint(dN) < 0);  // vn <= v0
+    const double vmn1 = vn_low ? vn : v0, vmx1 = vn_low ? v0 : vn;
+    const int cmn1 = vn_low ? 1 : 0, cmx1 = vn_low ? 0 : 1;
     // min/max(v0, UL): UL <= v0 iff dF >= 0 (left), UL >= v0 iff dF >= 0 (right)
     const bool f_up = __double2hiint(dF) >= 0;
-    const int mn2 = left ? (f_up ? 3 : 0) : (f_up ? 0 : 3);
-    const int mx2 = (mn2 == 3) ? 0 : 3;
-    auto mnsel = [&](int a, int b) { return (cand[b] < cand[a]) ? b : a; };
-    auto mxsel = [&](int a, int b) { return (cand[a] < cand[b]) ? b : a; };
-    const int lo_a = mnsel(mn1, 2), lo_b = mnsel(mn2, 4);
-    const int lo = mxsel(lo_a, lo_b);
-    const int hi_a = mxsel(mx1, 2), hi_b = mxsel(mx2, 4);
-    const int hi = (cand[hi_b] < cand[hi_a]) ? hi_b : hi_a;
+    const bool ul_low = left ? f_up : !f_up;
+    const double vmn2 = ul_low ? UL : v0, vmx2 = ul_low ? v0 : UL;
+    const int cmn2 = ul_low ? 3 : 0, cmx2 = ul_low ? 0 : 3;
+    const bool la = MD < vmn1, lb = LC < vmn2;
+    const double lo_av = la ? MD : vmn1, lo_bv = lb ? LC : vmn2;
+    const int lo_ac = la ? 2 : cmn1, lo_bc = lb ? 4 : cmn2;
+    const bool lsel = lo_av < lo_bv;  // max(lo_a, lo_b)
+    const double lo_v = lsel ? lo_bv : lo_av;
+    const int lo_c = lsel ? lo_bc : lo_ac;
+    const bool ha = vmx1 < MD, hb = vmx2 < LC;
+    const double hi_av = ha ? MD : vmx1, hi_bv = hb ? LC : vmx2;
+    const int hi_ac = ha ? 2 : cmx1, hi_bc = hb ? 4 : cmx2;
+    const bool hsel = hi_bv < hi_av;  // min(hi_a, hi_b)
+    const double hi_v = hsel ? hi_bv : hi_av;
+    const int hi_c = hsel ? hi_bc : hi_ac;
     // median(in, lo, hi) with lo <= hi: the input passes through unless it
     // lies outside the bounds
-    if (!(in < cand[lo]) && !(cand[hi] < in)) return 1.0;
-    const int pick = (in < cand[lo]) ? lo : hi;
+    if (!(in < lo_v) && !(hi_v < in)) return 1.0;
+    const int pick = (in < lo_v) ? lo_c : hi_c;
     // stencil weights of the picked expression, times g
     switch (pick) {
         case 0: acc.g[2] += g; break;
@@ -181,65 +187,111 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
         pL[r] = l;
         pR[r] = rr;
     }
-    // weights (faithful JS / TENO) for both sides
-    double aL[R + 1], aR[R + 1], SL = 0.0, SR = 0.0;
+    // weights for both sides: wL[r], wR[r] are the normalised weights
+    double wL[R], wR[R];
     double a4 = 0.0, tau4 = 0.0;  // WENO7 TENO extra alpha (f90:1491-1506)
-    double delta[R];
-    if (scheme == TENO) {
-        // cutoff exactly as the forward sweep decides it
-        double al[R + 1], s = 0.0, tau;
-        if (ORDER == 7) {
-            tau4 = fabs(eps - beta[0]);  // beta(3) of the reference is row 0 here
-            tau = tau4;
-        } else {
-            tau = fabs(beta[R - 1] - beta[0]);
+    double SL4 = 1.0, SR4 = 1.0;  // WENO7 TENO: the sums that include a4
+    bool js_fast = false;
+    // WENO3 keeps the reference's division form: its two-stencil weights
+    // amplify the few-ulp rounding change of the one-reciprocal form.
+    if (ORDER != 3 && scheme == JS) {
+        // one-reciprocal form: w_r = d_r P_r / sum_m d_m P_m, P_r = prod_{m != r} beta_m^2
+        double qq[R], P[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) qq[r] = beta[r] * beta[r];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double p = 1.0;
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                if (m != r) p *= qq[m];
+            P[r] = p;
+        }
+        double aL[R], aR[R], SL = 0.0, SR = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int q = Sh::q_of(r);
+            aL[r] = cf_d<ORDER>(cf, true, q) * P[r];
+            aR[r] = cf_d<ORDER>(cf, false, q) * P[r];
+            SL += aL[r];
+            SR += aR[r];
+        }
+        if (mid_range(SL) && mid_range(SR)) {
+            const double rr = nr_rcp(SL * SR), gSL = SR * rr, gSR = SL * rr;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                wL[r] = aL[r] * gSL;
+                wR[r] = aR[r] * gSR;
+            }
+            js_fast = true;
+        }
+    }
+    if (!js_fast) {
+        double aL[R], aR[R], SL = 0.0, SR = 0.0;
+        double delta[R];
+        if (scheme == TENO) {
+            // cutoff exactly as the forward sweep decides it
+            double al[R], s = 0.0, tau;
+            if (ORDER == 7) {
+                tau4 = fabs(eps - beta[0]);  // beta(3) of the reference is row 0 here
+                tau = tau4;
+            } else {
+                tau = fabs(beta[R - 1] - beta[0]);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (ORDER == 7) {
+                    const double a3 = pow(1.0 + tau / beta[r], 3.0);
+                    al[r] = a3 * a3;
+                } else {
+                    al[r] = pow(1.0 + tau / beta[r], 6.0);
+                }
+            }
+            if (ORDER == 7) {
+                const double a3 = pow(1.0 + tau / eps, 3.0);
+                a4 = a3 * a3;
+            }
+            // reference sums in weight order q = 0..
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                int r = q;
+                if (ORDER == 7) r = 3 - q;
+                s += al[r];
+            }
+            if (ORDER == 7) s += a4;
+#pragma unroll
+            for (int r = 0; r < R; ++r) delta[r] = (al[r] / s < teno_ct) ? 0.0 : 1.0;
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            if (ORDER == 7) {
-                const double a3 = pow(1.0 + tau / beta[r], 3.0);
-                al[r] = a3 * a3;
+            const int q = Sh::q_of(r);
+            if (scheme == TENO) {
+                aL[r] = delta[r] * cf_d<ORDER>(cf, true, q);
+                aR[r] = delta[r] * cf_d<ORDER>(cf, false, q);
             } else {
-                al[r] = pow(1.0 + tau / beta[r], 6.0);
+                aL[r] = cf_d<ORDER>(cf, true, q) / (beta[r] * beta[r]);
+                aR[r] = cf_d<ORDER>(cf, false, q) / (beta[r] * beta[r]);
             }
+            SL += aL[r];
+            SR += aR[r];
         }
-        if (ORDER == 7) {
-            const double a3 = pow(1.0 + tau / eps, 3.0);
-            a4 = a3 * a3;
+        if (ORDER == 7 && scheme == TENO) {
+            SL += a4;
+            SR += a4;
         }
-        // reference sums in weight order q = 0..
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-            int r = q;
-            if (ORDER == 7) r = 3 - q;
-            s += al[r];
+        for (int r = 0; r < R; ++r) {
+            wL[r] = aL[r] / SL;
+            wR[r] = aR[r] / SR;
         }
-        if (ORDER == 7) s += a4;
-#pragma unroll
-        for (int r = 0; r < R; ++r) delta[r] = (al[r] / s < teno_ct) ? 0.0 : 1.0;
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int q = Sh::q_of(r);
-        if (scheme == TENO) {
-            aL[r] = delta[r] * cf_d<ORDER>(cf, true, q);
-            aR[r] = delta[r] * cf_d<ORDER>(cf, false, q);
-        } else {
-            aL[r] = cf_d<ORDER>(cf, true, q) / (beta[r] * beta[r]);
-            aR[r] = cf_d<ORDER>(cf, false, q) / (beta[r] * beta[r]);
-        }
-        SL += aL[r];
-        SR += aR[r];
-    }
-    if (ORDER == 7 && scheme == TENO) {
-        SL += a4;
-        SR += a4;
+        SL4 = SL;
+        SR4 = SR;
     }
     double Lw = 0.0, Rw = 0.0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        Lw += aL[r] / SL * pL[r];
-        Rw += aR[r] / SR * pR[r];
+        Lw += wL[r] * pL[r];
+        Rw += wR[r] * pR[r];
     }
 
     // ---- MP (core faces only), pulled back first ----
@@ -264,22 +316,43 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
     }
 
     // ---- weights and candidates ----
+    // d out / d p_r = w_r;  d out / d beta_r = -2 w_r (p_r - out) / beta_r (JS)
+    double inv_beta[R];
+    if (scheme != TENO) {
+        double B = 1.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) B *= beta[r];
+        if (mid_range(B)) {
+            const double rB = nr_rcp(B);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                double p = rB;
+#pragma unroll
+                for (int m = 0; m < R; ++m)
+                    if (m != r) p *= beta[m];
+                inv_beta[r] = p;
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) inv_beta[r] = 1.0 / beta[r];
+        }
+    }
     double gD[6] = {0, 0, 0, 0, 0, 0};
     double gv0 = 0.0;
     double gbeta[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const double gpL = gLw * aL[r] / SL, gpR = gRw * aR[r] / SR;
+        const double gpL = gLw * wL[r], gpR = gRw * wR[r];
         gv0 += gpL + gpR;
 #pragma unroll
         for (int s = 0; s < S; ++s)
             gD[Sh::dk(r, s) + 3] += cf_poly<ORDER>(cf, true, r, s) * gpL + cf_poly<ORDER>(cf, false, r, s) * gpR;
-        const double gaL = gLw * (pL[r] - Lw) / SL, gaR = gRw * (pR[r] - Rw) / SR;
-        gbeta[r] = (scheme == TENO) ? 0.0 : -2.0 * (gaL * aL[r] + gaR * aR[r]) / beta[r];
+        gbeta[r] = (scheme == TENO) ? 0.0
+                                    : -2.0 * (gpL * (pL[r] - Lw) + gpR * (pR[r] - Rw)) * inv_beta[r];
     }
     if (ORDER == 7 && scheme == TENO) {
         // alpha(4) = (1 + |eps - beta(3)|/eps)^6 sits in both sums
-        const double ga4 = gLw * (0.0 - Lw) / SL + gRw * (0.0 - Rw) / SR;
+        const double ga4 = gLw * (0.0 - Lw) / SL4 + gRw * (0.0 - Rw) / SR4;
         const double base = 1.0 + tau4 / eps;
         const double da4 = 6.0 * pow(base, 5.0) / eps;   // d a4 / d tau
         const double sgn = (beta[0] - eps) >= 0.0 ? 1.0 : -1.0;
@@ -309,10 +382,16 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
 }
 
 // ---------------------------------------------------------------------
-// Kernel: a CTA owns TC consecutive cells of one column at a time; its
-// TC + 6 threads first compute the contributions of faces [Ja-6, Ja+TC)
-// (the faces whose stencils can reach the tile) into shared memory, then
-// the first TC threads gather them into their cells.
+// Kernel: one thread per column (a, b, v) of the sweep, marching along it.
+// Face o reads cells o..o+6 of the column (sweep index J = o + 3 + q,
+// q = -3..3) and contributes to the same cells; a cell has all its
+// contributions once face o = J is done.  The thread keeps the 7-cell
+// stencil window and the 7 pending cell sums in registers, so each step
+// loads one new cell and the two cotangents and writes one finished cell:
+// no shared memory, no barriers, no atomics.  Consecutive threads take
+// consecutive columns, i.e. consecutive x for the folded y/z sweeps
+// (coalesced); for sweeps along the contiguous axis the warp's 32 rows are
+// read through L1, each 32-byte sector serving four consecutive steps.
 // ---------------------------------------------------------------------
 struct VjpArgs {
     SweepGeom g;
@@ -325,60 +404,63 @@ struct VjpArgs {
     WenoParams wp;
     int mp;
     int accumulate;
-    int TC;
-    int n_ct;  // cell tiles per column
 };
 
-template <int ORDER>
+// UNI: face-independent coefficients, read from the kernel-parameter bank.
+template <int ORDER, bool UNI>
 __global__ void __launch_bounds__(128) vjp_kernel(const VjpArgs a) {
-    extern __shared__ double contrib[];  // [7][blockDim.x]
-    const int t = threadIdx.x;
-    const int nt = blockDim.x;
-    const int ct = blockIdx.x % a.n_ct;
-    const long long c0 = blockIdx.x / a.n_ct;
-    const long long cstep = gridDim.x / a.n_ct;
-    const long long Ja = (long long)ct * a.TC;
-    const long long o = Ja - 6 + t;  // this thread's face
     const long long ns = a.g.ns;
-    const bool face_ok = (ORDER == 3) ? (o >= 0 && o < ns) : (o >= 3 && o <= ns - 4);
-    const bool core = (o >= 3 && o <= ns - 4);
-    long long c = o - 3;
-    c = c < 0 ? 0 : (c > a.g.nc - 1 ? a.g.nc - 1 : c);
-    Coef<ORDER> cf;
-    if (face_ok) {
-        if (a.cp.polyL) cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.g.nc, c);
-        else cf = *reinterpret_cast<const Coef<ORDER>*>(a.uc.v);
-    }
-    const long long J = Ja + t;  // this thread's cell (t < TC)
-    for (long long col = c0; col < a.g.cols; col += cstep) {
+    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < a.g.cols;
+         col += (long long)gridDim.x * blockDim.x) {
         const long long av = col % a.g.c1;
         const long long tt = col / a.g.c1;
         const long long bv = tt % a.g.c2;
         const long long vv = tt / a.g.c2;
-        const long long base = a.g.in_off + av * a.g.sA + bv * a.g.sB + vv * a.g.sV;
-        double cq[7] = {0, 0, 0, 0, 0, 0, 0};
-        if (face_ok) {
-            double w[7];
+        const double* __restrict__ vin = a.v + a.g.in_off + av * a.g.sA + bv * a.g.sB + vv * a.g.sV;
+        double* __restrict__ gout = a.gv + a.g.in_off + av * a.g.sA + bv * a.g.sB + vv * a.g.sV;
+        const double* __restrict__ gLc = a.gL + ns * col;
+        const double* __restrict__ gRc = a.gR + ns * col;
+        const long long sJ = a.g.sJ;
+        double w[7], acc[7];
 #pragma unroll
-            for (int q = -3; q <= 3; ++q) {
-                const long long Jq = o + 3 + q;
-                w[q + 3] = (Jq >= 0 && Jq < ns + 6) ? __ldg(a.v + base + Jq * a.g.sJ) : 0.0;
+        for (int q = 0; q < 6; ++q) w[q] = __ldg(vin + q * sJ);
+#pragma unroll
+        for (int q = 0; q < 7; ++q) acc[q] = 0.0;
+        for (long long o = 0; o < ns; ++o) {
+            w[6] = __ldg(vin + (o + 6) * sJ);
+            const bool face_ok = (ORDER == 3) || (o >= 3 && o <= ns - 4);
+            if (face_ok) {
+                const bool core = (o >= 3 && o <= ns - 4);
+                if constexpr (UNI) {
+                    face_vjp<ORDER>(w + 3, *reinterpret_cast<const Coef<ORDER>*>(a.uc.v), a.wp.scheme, a.wp.eps,
+                                    a.wp.teno_ct, a.mp && core, __ldg(gLc + o), __ldg(gRc + o), acc);
+                } else {
+                    long long c = o - 3;
+                    c = c < 0 ? 0 : (c > a.g.nc - 1 ? a.g.nc - 1 : c);
+                    Coef<ORDER> cf;
+                    cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.g.nc, c);
+                    face_vjp<ORDER>(w + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, a.mp && core, __ldg(gLc + o),
+                                    __ldg(gRc + o), acc);
+                }
             }
-            const double gl = __ldg(a.gL + o + ns * col), gr = __ldg(a.gR + o + ns * col);
-            face_vjp<ORDER>(w + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, a.mp && core, gl, gr, cq);
-        }
+            // cell J = o is complete
+            double* dst = gout + o * sJ;
+            if (a.accumulate) *dst += acc[0];
+            else *dst = acc[0];
 #pragma unroll
-        for (int q = 0; q < 7; ++q) contrib[q * nt + t] = cq[q];
-        __syncthreads();
-        if (t < a.TC && J < ns + 6) {
-            double s = 0.0;
-#pragma unroll
-            for (int q = -3; q <= 3; ++q) s += contrib[(q + 3) * nt + (t + 3 - q)];
-            double* dst = a.gv + base + J * a.g.sJ;
-            if (a.accumulate) *dst += s;
-            else *dst = s;
+            for (int q = 0; q < 6; ++q) {
+                acc[q] = acc[q + 1];
+                w[q] = w[q + 1];
+            }
+            acc[6] = 0.0;
         }
-        __syncthreads();
+        // cells ns .. ns+5
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            double* dst = gout + (ns + q) * sJ;
+            if (a.accumulate) *dst += acc[q];
+            else *dst = acc[q];
+        }
     }
 }
 

@@ -436,6 +436,128 @@ __device__ __forceinline__ void weno7_face(const double* v /* v[-3..3] */, const
 }
 
 // ---------------------------------------------------------------------
+// FP32-bulk WENO-JS without FP32 <-> FP64 conversion instructions.
+//
+// On B200 a conversion between float and double issues at a quarter of the
+// FP64 FMA rate, so a per-face path that widens its stencil and narrows its
+// weights with cvt instructions spends more on conversions than on the
+// WENO arithmetic.  Here:
+//  * the stencil values are widened by bit manipulation on the integer
+//    pipe (f2d_bits): exact for normal floats; zero and subnormal floats
+//    become values below 2^-126 in magnitude (immaterial next to eps in
+//    beta), Inf/NaN become large finite values -- the float stencil sums
+//    below still carry the Inf/NaN into the face state;
+//  * the differences, beta (with eps) and the weight normalisation are
+//    FP64, as in the FP64 path;
+//  * the normalised weights (in [0, 1]) are narrowed by bit manipulation
+//    with truncation (unit_d2f, relative error < 2^-23);
+//  * the candidate polynomials and the weighted sum are FP32, written as
+//    v0 + (small corrections): L = v0 + e1 + w0 (e0 - e1) + w2 (e2 - e1)
+//    with e_k = p_k - v0 (and the WENO7 analogue), so the weights'
+//    truncation multiplies only the small differences e_k - e1 and the
+//    face state is rounded once, at the final add.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ double f2d_bits(float x) {
+    const unsigned u = __float_as_uint(x);
+    const unsigned hi = ((((u & 0x7FFFFFFFu) >> 3) | (u & 0x80000000u)) + 0x38000000u);
+    return __hiloint2double((int)hi, (int)(u << 29));
+}
+
+// w in [0, 1] (or NaN-free non-negative) to float, truncating; values below
+// 2^-126 become 0.
+__device__ __forceinline__ float unit_d2f(double w) {
+    const unsigned hi = (unsigned)__double2hiint(w), lo = (unsigned)__double2loint(w);
+    const unsigned t = __funnelshift_l(lo, hi, 3) + 0x40000000u;
+    return (hi < 0x38100000u) ? 0.0f : __uint_as_float(t);
+}
+
+// Float copies of one face's polynomial coefficients (layout of Coef<ORDER>).
+template <int ORDER>
+struct PolyF {
+    static constexpr int N = (ORDER == 7) ? 12 : (ORDER == 5 ? 6 : 2);
+    float L[N], R[N];
+    __device__ __forceinline__ void from(const Coef<ORDER>& c) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            L[i] = (float)c.pL[i];
+            R[i] = (float)c.pR[i];
+        }
+    }
+};
+
+// WENO5-JS, FP32 in and out.  Returns false when a normalisation sum left
+// the one-reciprocal range; the caller then redoes the face in FP64.
+__device__ __forceinline__ bool weno5_js_mixed(float m2, float m1, float z0, float p1, float p2,
+                                               const Coef<5>& c, const PolyF<5>& pf, double eps, float& L,
+                                               float& R) {
+    const double Dm2 = f2d_bits(m2), Dm1 = f2d_bits(m1), D0 = f2d_bits(z0), Dp1 = f2d_bits(p1),
+                 Dp2 = f2d_bits(p2);
+    const double dvd_p1 = Dp2 - Dp1, dvd_0 = Dp1 - D0, dvd_m1 = D0 - Dm1, dvd_m2 = Dm1 - Dm2;
+    const double beta0 = c.b[0] * dvd_p1 * dvd_p1 + c.b[1] * dvd_p1 * dvd_0 + c.b[2] * dvd_0 * dvd_0 + eps;
+    const double beta1 = c.b[3] * dvd_0 * dvd_0 + c.b[4] * dvd_0 * dvd_m1 + c.b[5] * dvd_m1 * dvd_m1 + eps;
+    const double beta2 = c.b[6] * dvd_m1 * dvd_m1 + c.b[7] * dvd_m1 * dvd_m2 + c.b[8] * dvd_m2 * dvd_m2 + eps;
+    const double q0 = beta0 * beta0, q1 = beta1 * beta1, q2 = beta2 * beta2;
+    const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+    const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2;
+    const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2;
+    const double SL = aL0 + aL1 + aL2, SR = aR0 + aR1 + aR2;
+    const bool ok = mid_range(SL) && mid_range(SR);
+    const double r = nr_rcp(SL * SR), gL = SR * r, gR = SL * r;
+    const float wL0 = unit_d2f(aL0 * gL), wL2 = unit_d2f(aL2 * gL);
+    const float wR0 = unit_d2f(aR0 * gR), wR2 = unit_d2f(aR2 * gR);
+    const float fp1 = p2 - p1, f0 = p1 - z0, fm1 = z0 - m1, fm2 = m1 - m2;
+    const float eL0 = fmaf(pf.L[0], fp1, pf.L[1] * f0), eL1 = fmaf(pf.L[2], f0, pf.L[3] * fm1),
+                eL2 = fmaf(pf.L[4], fm1, pf.L[5] * fm2);
+    const float eR0 = fmaf(pf.R[0], fp1, pf.R[1] * f0), eR1 = fmaf(pf.R[2], f0, pf.R[3] * fm1),
+                eR2 = fmaf(pf.R[4], fm1, pf.R[5] * fm2);
+    L = z0 + fmaf(wL0, eL0 - eL1, fmaf(wL2, eL2 - eL1, eL1));
+    R = z0 + fmaf(wR0, eR0 - eR1, fmaf(wR2, eR2 - eR1, eR1));
+    return ok;
+}
+
+// WENO7-JS, FP32 in and out (v[-3..3]); same contract as weno5_js_mixed.
+__device__ __forceinline__ bool weno7_js_mixed(const float* v, const Coef<7>& c, const PolyF<7>& pf, double eps,
+                                               float& L, float& R) {
+    double V[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) V[q] = f2d_bits(v[q - 3]);
+    double D[6];  // D[k+3] = dvd(k), k = -3..2
+#pragma unroll
+    for (int k = 0; k < 6; ++k) D[k] = V[k + 1] - V[k];
+    double beta[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const double a = D[5 - r], b = D[4 - r], e = D[3 - r];
+        beta[3 - r] = c.b[6 * r + 0] * a * a + c.b[6 * r + 1] * a * b + c.b[6 * r + 2] * a * e +
+                      c.b[6 * r + 3] * b * b + c.b[6 * r + 4] * b * e + c.b[6 * r + 5] * e * e + eps;
+    }
+    const double q0 = beta[0] * beta[0], q1 = beta[1] * beta[1], q2 = beta[2] * beta[2], q3 = beta[3] * beta[3];
+    const double q01 = q0 * q1, q23 = q2 * q3;
+    const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
+    const double aL0 = c.dL[0] * P0, aL1 = c.dL[1] * P1, aL2 = c.dL[2] * P2, aL3 = c.dL[3] * P3;
+    const double aR0 = c.dR[0] * P0, aR1 = c.dR[1] * P1, aR2 = c.dR[2] * P2, aR3 = c.dR[3] * P3;
+    const double SL = aL0 + aL1 + aL2 + aL3, SR = aR0 + aR1 + aR2 + aR3;
+    const bool ok = mid_range(SL) && mid_range(SR);
+    const double r = nr_rcp(SL * SR), gL = SR * r, gR = SL * r;
+    // stencil 3 - r uses float differences F[5-r], F[4-r], F[3-r]
+    float F[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) F[k] = v[k - 2] - v[k - 3];
+    float eL[4], eR[4];
+#pragma unroll
+    for (int r2 = 0; r2 < 4; ++r2) {
+        eL[3 - r2] = fmaf(pf.L[3 * r2], F[5 - r2], fmaf(pf.L[3 * r2 + 1], F[4 - r2], pf.L[3 * r2 + 2] * F[3 - r2]));
+        eR[3 - r2] = fmaf(pf.R[3 * r2], F[5 - r2], fmaf(pf.R[3 * r2 + 1], F[4 - r2], pf.R[3 * r2 + 2] * F[3 - r2]));
+    }
+    // pivot on stencil 1: L = v0 + e1 + sum_{k != 1} w_k (e_k - e1)
+    const float wL0 = unit_d2f(aL0 * gL), wL2 = unit_d2f(aL2 * gL), wL3 = unit_d2f(aL3 * gL);
+    const float wR0 = unit_d2f(aR0 * gR), wR2 = unit_d2f(aR2 * gR), wR3 = unit_d2f(aR3 * gR);
+    L = v[0] + fmaf(wL0, eL[0] - eL[1], fmaf(wL2, eL[2] - eL[1], fmaf(wL3, eL[3] - eL[1], eL[1])));
+    R = v[0] + fmaf(wR0, eR[0] - eR[1], fmaf(wR2, eR[2] - eR[1], fmaf(wR3, eR[3] - eR[1], eR[1])));
+    return ok;
+}
+
+// ---------------------------------------------------------------------
 // MP limiter (f90:1564-1608), rounding exactly as the reference.
 // ---------------------------------------------------------------------
 // 4-argument minmod of (4dl-dr, dl, 4dr-dl, dr) (f90:1568-1571).  The
@@ -518,31 +640,35 @@ __device__ __forceinline__ float mp_minmod_f(float dl, float dr) {
     return same ? copysignf(t < m ? t : m, dl) : 0.0f;
 }
 
+// The same limiter for FP32-bulk, on the FP32 field, with every bound
+// carried as an offset from v0: the first differences a, b, c, e of
+// neighbouring values are exact for values within a factor of two of each
+// other, the bounds minus v0 are sums of small terms, and the state is
+// rounded once when v0 is added back.  In exact arithmetic this is the
+// reference's median(x, lo, hi) shifted by v0.
 __device__ __forceinline__ void mp_limit_f(const float vm2, const float vm1, const float v0, const float vp1,
                                            const float vp2, float& L, float& R) {
     const float kBetaMP = 4.0f / 3.0f;
-    const float dm1 = fmaf(-2.0f, vm1, v0 + vm2);
-    const float d0 = fmaf(-2.0f, v0, vp1 + vm1);
-    const float dp1 = fmaf(-2.0f, vp1, vp2 + v0);
-    const float mA = mp_minmod_f(dm1, d0);
-    const float mB = mp_minmod_f(d0, dp1);
-    const float dR1 = vp1 - v0, dL1 = v0 - vm1;
-    const bool up_r = __float_as_int(dR1) >= 0, up_l = __float_as_int(dL1) >= 0;
+    const float a = vm1 - vm2, b = v0 - vm1, c = vp1 - v0, e = vp2 - vp1;
+    const float mA = mp_minmod_f(b - a, c - b);  // minmod(d_{j-1}, d_j)
+    const float mB = mp_minmod_f(c - b, e - c);  // minmod(d_j, d_{j+1})
     {
-        const float UL = fmaf(-2.0f, dR1, v0);
-        const float MD = ((v0 + vm1) - mA) * 0.5f;
-        const float LC = fmaf(kBetaMP, mB, fmaf(-0.5f, dR1, v0));
-        const float mn1 = up_l ? vm1 : v0, mx1 = up_l ? v0 : vm1;
-        const float mn2 = up_r ? UL : v0, mx2 = up_r ? v0 : UL;
-        L = sclamp(L, smax(smin(mn1, MD), smin(mn2, LC)), smin(smax(mx1, MD), smax(mx2, LC)));
+        const float x = L - v0;
+        const float oMD = -0.5f * (b + mA);           // (v0 + vm1 - mA)/2 - v0
+        const float oLC = fmaf(kBetaMP, mB, -0.5f * c);  // v0 - c/2 + 4/3 mB - v0
+        const float ul = -2.0f * c;                   // UL - v0
+        const float lo = fmaxf(fminf(fminf(0.0f, -b), oMD), fminf(fminf(0.0f, ul), oLC));
+        const float hi = fminf(fmaxf(fmaxf(0.0f, -b), oMD), fmaxf(fmaxf(0.0f, ul), oLC));
+        L = v0 + sclamp(x, lo, hi);
     }
     {
-        const float UL = fmaf(2.0f, dL1, v0);
-        const float MD = ((v0 + vp1) - mB) * 0.5f;
-        const float LC = fmaf(kBetaMP, mA, fmaf(0.5f, dL1, v0));
-        const float mn1 = up_r ? v0 : vp1, mx1 = up_r ? vp1 : v0;
-        const float mn2 = up_l ? v0 : UL, mx2 = up_l ? UL : v0;
-        R = sclamp(R, smax(smin(mn1, MD), smin(mn2, LC)), smin(smax(mx1, MD), smax(mx2, LC)));
+        const float x = R - v0;
+        const float oMD = 0.5f * (c - mB);            // (v0 + vp1 - mB)/2 - v0
+        const float oLC = fmaf(kBetaMP, mA, 0.5f * b);   // v0 + b/2 + 4/3 mA - v0
+        const float ul = 2.0f * b;                    // UL - v0
+        const float lo = fmaxf(fminf(fminf(0.0f, c), oMD), fminf(fminf(0.0f, ul), oLC));
+        const float hi = fminf(fmaxf(fmaxf(0.0f, c), oMD), fmaxf(fmaxf(0.0f, ul), oLC));
+        R = v0 + sclamp(x, lo, hi);
     }
 }
 

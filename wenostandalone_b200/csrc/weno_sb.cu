@@ -22,6 +22,7 @@
 #include "sweep_generic.cuh"
 #include "sweep_tma.cuh"
 #include "sweep_pipe.cuh"
+#include "sweep_march.cuh"
 #include "weno_adjoint.cuh"
 #include "batched.cuh"
 
@@ -267,10 +268,15 @@ int launch_generic(const SweepGeom& g, int order, bool mp, const T* in, T* vL, T
 // (read per call): "auto" (default: TMA pipeline for FP64 when the layout
 // allows it, else the cp.async pipeline, else the general-stride kernel),
 // "tma", "cpasync" or "generic" to pin one for testing.
+// WENO_SB_KERNEL: auto (0), generic (1), cpasync (2), march (3), tma (4).
+// A forced kernel that does not cover the case falls through to the next
+// one in the auto order (march, tma, cp.async, generic).
 int kernel_choice() {
     const char* e = getenv("WENO_SB_KERNEL");
     if (e && strcmp(e, "generic") == 0) return 1;
     if (e && strcmp(e, "cpasync") == 0) return 2;
+    if (e && strcmp(e, "march") == 0) return 3;
+    if (e && strcmp(e, "tma") == 0) return 4;
     return 0;
 }
 
@@ -288,13 +294,17 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
+    if ((choice == 0 || choice == 3) && ucf && order == 5 && gr->scheme == WENO_SB_JS) {
+        int rc = launch_march_sweep<T>(g, mp, in, vL, vR, wp, ucf, st, num_sms());
+        if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
+    }
     if constexpr (sizeof(T) == 8) {
-        if (choice == 0) {
+        if (choice == 0 || choice == 3 || choice == 4) {
             int rc = launch_pipe_sweep(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st, num_sms(), ucf);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "tma sweep launch") : rc;
         }
     }
-    if (choice == 0 || choice == 2) {
+    if (choice != 1) {
         int rc = launch_tma_sweep<T>(d.E, g, dir, folded, order, mp, in, vL, vR, cp, wp, st, ucf);
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "cp.async sweep launch") : rc;
     }
@@ -342,17 +352,18 @@ int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsign
     if (folded && !acc_flag)
         WSB_CUDA(cudaMemsetAsync(gv, 0, sizeof(double) * d.E[0] * d.E[1] * d.E[2] * d.nv, st));
     const int threads = 128;
-    a.TC = threads - 6;
-    a.n_ct = (int)((a.g.ns + 6 + a.TC - 1) / a.TC);
-    long long per = ((long long)num_sms() * 12) / a.n_ct;
-    if (per < 1) per = 1;
-    if (per > a.g.cols) per = a.g.cols;
-    const size_t smem = sizeof(double) * 7 * threads;
-    const unsigned grid = (unsigned)(per * a.n_ct);
-    switch (order) {
-        case 3: vjp_kernel<3><<<grid, threads, smem, st>>>(a); break;
-        case 5: vjp_kernel<5><<<grid, threads, smem, st>>>(a); break;
-        case 7: vjp_kernel<7><<<grid, threads, smem, st>>>(a); break;
+    long long blocks = (a.g.cols + threads - 1) / threads;
+    if (blocks < 1) blocks = 1;
+    if (blocks > (1LL << 30)) blocks = 1LL << 30;
+    const unsigned grid = (unsigned)blocks;
+    const bool uni = ucf != nullptr;
+    switch (order * 2 + (uni ? 1 : 0)) {
+        case 6: vjp_kernel<3, false><<<grid, threads, 0, st>>>(a); break;
+        case 7: vjp_kernel<3, true><<<grid, threads, 0, st>>>(a); break;
+        case 10: vjp_kernel<5, false><<<grid, threads, 0, st>>>(a); break;
+        case 11: vjp_kernel<5, true><<<grid, threads, 0, st>>>(a); break;
+        case 14: vjp_kernel<7, false><<<grid, threads, 0, st>>>(a); break;
+        case 15: vjp_kernel<7, true><<<grid, threads, 0, st>>>(a); break;
         default: return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
     }
     return cuda_err(cudaGetLastError(), "vjp launch");
