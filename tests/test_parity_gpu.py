@@ -151,7 +151,7 @@ def test_face_varying_coefficients(wsb, oracle_mod, order, folded, mp, kernel):
             assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
 
 
-@pytest.mark.parametrize("kernel", ["auto", "march", "tma", "cpasync", "generic"])
+@pytest.mark.parametrize("kernel", ["auto", "march", "march_ldg", "tma", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
 @pytest.mark.parametrize("scheme", [0, 3])
@@ -315,9 +315,12 @@ def test_handle_all_mode_matches_oracle(wsb, oracle_mod):
         assert abs(a - e) / e <= 1e-12
 
 
-def test_full_size_weno5_mp(wsb, oracle_mod):
+@pytest.mark.parametrize("entry", ["arrays", "uniform"])
+def test_full_size_weno5_mp(wsb, oracle_mod, entry):
     """200^3 x 8, seeded smooth-plus-jump field, WENO5-JS + MP, every direction,
-    drop-in and folded forms, against the oracle at 1e-12 per array."""
+    drop-in and folded forms, against the oracle at 1e-12 per array; through
+    the per-face coefficient arrays and through the face-independent entry
+    (the marching kernels)."""
     import torch
     from wenostandalone_b200 import api, fields
     m = 199
@@ -338,7 +341,11 @@ def test_full_size_weno5_mp(wsb, oracle_mod):
             if not folded:
                 src = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float64, device="cuda")
                 api.reshape(g, d, v, src)
-            api.weno(g, d, 5, src, dc, L, R, flags=wsb.F_MP | (wsb.F_FOLDED if folded else 0))
+            fl = wsb.F_MP | (wsb.F_FOLDED if folded else 0)
+            if entry == "uniform":
+                api.weno_uniform(g, d, 5, src, coefs, L, R, flags=fl)
+            else:
+                api.weno(g, d, 5, src, dc, L, R, flags=fl)
             eL = rel_err(from_dev(L, g.face_shape(d)), Lr)
             eR = rel_err(from_dev(R, g.face_shape(d)), Rr)
             assert eL <= TOL64 and eR <= TOL64, (d, folded, eL, eR)

@@ -50,6 +50,9 @@ struct MarchArgs {
     long long n_items;
     double ucf[56];  // Coef<5> layout
     float ucf32[12]; // float copies of polyL[0..5], polyR[0..5]
+    // FP64 kernel: candidate-polynomial coefficients scaled by the ideal
+    // weights, kL[2r+s] = dL[r] * polyL[s][r] (and kR likewise)
+    double kL[6], kR[6];
 };
 
 // Second-order minmod of the MP limiter (same decisions as mp_minmod /
@@ -296,12 +299,287 @@ __global__ void __launch_bounds__(128) sweep_march_kernel(const MarchArgs a) {
     }
 }
 
-// Launch for face-independent WENO5-JS coefficients.  Returns 1003 when
-// the sweep has too few faces for the window.
-template <typename T>
-int launch_march_sweep(const SweepGeom& g, bool mp, const T* in, T* vL, T* vR, const WenoParams& wp,
-                       const double* ucf, cudaStream_t st, int sms) {
-    if (g.nc < 1 || !ucf) return 1003;
+// ---------------------------------------------------------------------
+// FP64 marching sweep with a branch-free face body.
+//
+// Per face the FP64 issue slots are the bound (a B200 SM retires 64 FP64
+// lanes per clock against 128 for FP32 and integer work), so the body is
+// arranged to spend as few as the arithmetic allows while keeping FP64
+// throughout:
+//  * each new difference pair (d[k], d[k+1]) enters beta_0 of face k,
+//    beta_1 of face k+1 and beta_2 of face k+2 (three FMA chains of the
+//    reference's form, so the beta are the ones the per-face kernels
+//    compute) and the pending beta_1 / beta_2 ride along with the window;
+//  * the ideal weights are folded into the candidate polynomials on the
+//    host, kL[2r+s] = dL[r] polyL[s][r], so with P_k = prod_{m!=k} beta_m^2
+//    the state is v0 + E_L / S_L, E_L = sum_k P_k (kL . differences),
+//    S_L = sum_k dL[k] P_k: the weights' rounding multiplies only the
+//    offset from v0, and one Newton step on the hardware reciprocal seed
+//    of S_L S_R leaves a relative error near 2^-46 in that offset;
+//  * the MP limiter takes the curvature minmod of the newest pair only
+//    (the other one slides along), the half-sums (v[j-1]+v[j])/2 slide
+//    too, and since lo <= v0 <= hi, median(L, lo, hi) is min(L, hi) when
+//    L >= v0 and max(L, lo) otherwise: one bound per state, with min or
+//    max picked by the sign of the offset.  Values and roundings are those
+//    of mp_core.
+// A face whose normalisation sums leave the range of the one-reciprocal
+// form is flagged and redone after its chunk with the reference sequence
+// (weno5_face, then mp_limit), so the common path has no branch.
+// ---------------------------------------------------------------------
+// min (up = false) or max (up = true) of two doubles: one comparison and a
+// select, no NaN special-casing (the CUDA fmin/fmax handle NaN operands and
+// cost several more instructions each).
+__device__ __forceinline__ double mm_sel(double a, double b, bool up) { return ((a < b) != up) ? a : b; }
+
+// minmod of the MP limiter: the value of mp_minmod (up to the sign of a
+// zero result), with the "signs differ or 4m - M < 0" test on sign bits.
+__device__ __forceinline__ double mm64(double dl, double dr) {
+    const double a = fabs(dl), b = fabs(dr);
+    const bool al = a < b;
+    const double m = al ? a : b, M = al ? b : a;
+    const double t = fma(4.0, m, -M);
+    const double u = (t < m) ? t : m;
+    const int hl = __double2hiint(dl), hu = __double2hiint(u);
+    const int kill = ((hl ^ __double2hiint(dr)) | hu) >> 31;
+    const int hi = (hu & ~kill) | (hl & (int)0x80000000);
+    const int lo = __double2loint(u) & ~kill;
+    return __hiloint2double(hi, lo);
+}
+
+// Reciprocal of a positive normal double: hardware seed and one Newton step.
+__device__ __forceinline__ double rcp1(double s) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
+    return fma(r, fma(-s, r, 1.0), r);
+}
+
+struct March64 {
+    double vm1, v0, vp1, vp2;   // cells J-1 .. J+2
+    double dm2, dm1, d0, dp1;   // d[k] = v[k+1] - v[k], k = J-2 .. J+1
+    double s1;                  // d[J+1]^2
+    double b0, b1, b2;          // beta_0, beta_1, beta_2 of face J
+    double b1n, b2n, b2nn;      // beta_1(J+1), beta_2(J+1), beta_2(J+2)
+    double e2;                  // curvature d[J+1] - d[J]
+    double mA, mB;              // minmod(e2[J-1], e2[J]), minmod(e2[J], e2[J+1])
+    double hL, hR;              // (v[J-1] + v[J]) / 2, (v[J] + v[J+1]) / 2
+
+    // beta of the three stencils that pair (x, y) = (d[k], d[k+1]) enters
+    __device__ __forceinline__ static void betas(const MarchArgs& a, double sx, double cxy, double sy, double& g0,
+                                                 double& g1, double& g2) {
+        const double eps = a.wp.eps;
+        g0 = fma(a.ucf[18], sy, fma(a.ucf[19], cxy, fma(a.ucf[20], sx, eps)));
+        g1 = fma(a.ucf[21], sy, fma(a.ucf[22], cxy, fma(a.ucf[23], sx, eps)));
+        g2 = fma(a.ucf[24], sy, fma(a.ucf[25], cxy, fma(a.ucf[26], sx, eps)));
+    }
+
+    // Window of face J from cells J-2 .. J+2.
+    __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3,
+                                         double c4) {
+        vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
+        dm2 = c1 - c0; dm1 = c2 - c1; d0 = c3 - c2; dp1 = c4 - c3;
+        const double sm2 = dm2 * dm2, sm1 = dm1 * dm1, s0 = d0 * d0;
+        s1 = dp1 * dp1;
+        double g0, g1, g2, u;
+        betas(a, sm2, dm2 * dm1, sm1, u, u, b2);      // pair (d[J-2], d[J-1])
+        betas(a, sm1, dm1 * d0, s0, u, b1, b2n);      // pair (d[J-1], d[J])
+        betas(a, s0, d0 * dp1, s1, g0, g1, g2);       // pair (d[J], d[J+1])
+        b0 = g0; b1n = g1; b2nn = g2;
+        const double em = dm1 - dm2, ez = d0 - dm1;
+        e2 = dp1 - d0;
+        mA = mm64(em, ez);
+        mB = mm64(ez, e2);
+        hL = (vm1 + v0) * 0.5;
+        hR = (v0 + vp1) * 0.5;
+    }
+
+    // Advance to face J+1; n is cell J+3.
+    __device__ __forceinline__ void push(const MarchArgs& a, double n) {
+        const double dn = n - vp2;
+        const double sn = dn * dn;
+        double g0, g1, g2;
+        betas(a, s1, dp1 * dn, sn, g0, g1, g2);
+        const double ne2 = dn - dp1;
+        const double nmB = mm64(e2, ne2);
+        const double nhR = (vp1 + vp2) * 0.5;
+        vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
+        dm2 = dm1; dm1 = d0; d0 = dp1; dp1 = dn;
+        s1 = sn;
+        b0 = g0; b1 = b1n; b2 = b2n;
+        b1n = g1; b2n = b2nn; b2nn = g2;
+        e2 = ne2; mA = mB; mB = nmB;
+        hL = hR; hR = nhR;
+    }
+
+    // WENO5-JS (+ MP) state of face J; false when the one-reciprocal form
+    // is out of range (the caller redoes the face).
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+        const double q0 = b0 * b0, q1 = b1 * b1, q2 = b2 * b2;
+        const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+        const double SL = fma(a.ucf[12], P0, fma(a.ucf[13], P1, a.ucf[14] * P2));
+        const double SR = fma(a.ucf[15], P0, fma(a.ucf[16], P1, a.ucf[17] * P2));
+        const double eL0 = fma(a.kL[1], d0, a.kL[0] * dp1), eL1 = fma(a.kL[3], dm1, a.kL[2] * d0),
+                     eL2 = fma(a.kL[5], dm2, a.kL[4] * dm1);
+        const double eR0 = fma(a.kR[1], d0, a.kR[0] * dp1), eR1 = fma(a.kR[3], dm1, a.kR[2] * d0),
+                     eR2 = fma(a.kR[5], dm2, a.kR[4] * dm1);
+        const double EL = fma(P0, eL0, fma(P1, eL1, P2 * eL2));
+        const double ER = fma(P0, eR0, fma(P1, eR1, P2 * eR2));
+        const bool ok = mid_range(SL) && mid_range(SR);
+        const double r = rcp1(SL * SR);
+        L = fma(EL * SR, r, v0);
+        R = fma(ER * SL, r, v0);
+        if constexpr (MPF) {
+            // median(L, lo, hi) with lo <= v0 <= hi: for L >= v0 (E_L >= 0)
+            // it is min(L, hi) and otherwise max(L, lo), so only one bound
+            // is formed, with min/max chosen by that sign.
+            const double kBetaMP = 4.0 / 3.0;
+            const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
+            {
+                const bool pos = sign_clear(EL);
+                const double UL = fma(-2.0, d0, v0);
+                const double MD = fma(-0.5, mA, hL);
+                const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
+                const double P1 = (pos == up_l) ? v0 : vm1;  // max / min of (v0, vm1)
+                const double P2 = (pos == up_r) ? v0 : UL;   // max / min of (v0, UL)
+                const double A = mm_sel(P1, MD, pos), B = mm_sel(P2, LC, pos);
+                L = mm_sel(mm_sel(L, A, !pos), B, !pos);
+            }
+            {
+                const bool pos = sign_clear(ER);
+                const double UL = fma(2.0, dm1, v0);
+                const double MD = fma(-0.5, mB, hR);
+                const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
+                const double P1 = (pos == up_r) ? vp1 : v0;  // max / min of (v0, vp1)
+                const double P2 = (pos == up_l) ? UL : v0;   // max / min of (v0, UL)
+                const double A = mm_sel(P1, MD, pos), B = mm_sel(P2, LC, pos);
+                R = mm_sel(mm_sel(R, A, !pos), B, !pos);
+            }
+        }
+        return ok;
+    }
+};
+
+// The reference sequence for one face (cells o+1 .. o+5 of the column).
+template <bool MPF>
+__device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __restrict__ col, long long o,
+                                          double& L, double& R) {
+    Coef<5> c;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        c.pL[q] = a.ucf[q];
+        c.pR[q] = a.ucf[6 + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        c.dL[q] = a.ucf[12 + q];
+        c.dR[q] = a.ucf[15 + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) c.b[q] = a.ucf[18 + q];
+    const double* p = col + (o + 1) * a.sJ;
+    const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
+                 vp2 = __ldg(p + 4 * a.sJ);
+    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, JS, a.wp.eps, 0.0, L, R);
+    if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
+}
+
+#ifndef WSB_MARCH64_MIN_BLOCKS
+#define WSB_MARCH64_MIN_BLOCKS 3
+#endif
+#ifndef WSB_MARCH64_GROUP
+#define WSB_MARCH64_GROUP 8
+#endif
+constexpr int kMarch64F = 16;                  // faces per chunk (and per shared-memory flush)
+constexpr int kMarch64H = WSB_MARCH64_GROUP;   // cells per prefetch group
+static_assert(kMarch64F % (2 * kMarch64H) == 0, "an even number of prefetch groups per chunk");
+
+template <bool MPF>
+__global__ void __launch_bounds__(128, WSB_MARCH64_MIN_BLOCKS)
+    sweep_march64_kernel(const __grid_constant__ MarchArgs a) {
+    constexpr int F = kMarch64F, H = kMarch64H;
+    __shared__ double tile[4][2][F][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double* __restrict__ in = (const double*)a.in;
+    double* __restrict__ outL = (double*)a.vL;
+    double* __restrict__ outR = (double*)a.vR;
+    double(*tl)[F][33] = tile[warp];
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long ncell = a.ns + 6;
+    for (long long item = (long long)blockIdx.x * (blockDim.x >> 5) + warp; item < a.n_items; item += nwarps) {
+        const int sg = (int)(item % a.n_seg);
+        long long t = item / a.n_seg;
+        const int ut = (int)(t % a.n_ut);
+        t /= a.n_ut;
+        const int wv = (int)(t % a.Nw);
+        const int vv = (int)(t / a.Nw);
+        const int u = ut * 32 + lane;
+        const int uc = u < a.Nu ? u : a.Nu - 1;  // idle lanes shadow a valid column
+        const double* __restrict__ col = in + a.in_off + uc * a.sU + wv * a.sW + vv * a.sV;
+        const long long o_begin = 3 + (long long)sg * a.seg;
+        long long o_end = o_begin + a.seg;
+        if (o_end > a.ns - 3) o_end = a.ns - 3;
+        // face o: centre cell o + 3, cells o+1 .. o+5; after face o the
+        // window takes cell o + 6
+        March64 w;
+        {
+            const double* p = col + (o_begin + 1) * a.sJ;
+            w.init(a, __ldg(p), __ldg(p + a.sJ), __ldg(p + 2 * a.sJ), __ldg(p + 3 * a.sJ), __ldg(p + 4 * a.sJ));
+        }
+        const long long obase = (long long)ut * 32 * a.oU + wv * a.oW + vv * a.oV;
+        // cells arrive H at a time, one group ahead of their use
+        double buf[2][H];
+        auto load = [&](double* dst, long long J0) {
+#pragma unroll
+            for (int i = 0; i < H; ++i) {
+                const long long J = J0 + i;
+                dst[i] = (J < ncell) ? __ldg(col + J * a.sJ) : 0.0;
+            }
+        };
+        load(buf[0], o_begin + 6);
+        for (long long f0 = o_begin; f0 < o_end; f0 += F) {
+            const int nF = (int)min((long long)F, o_end - f0);
+            unsigned bad = 0;
+#pragma unroll
+            for (int gi = 0; gi < F / H; ++gi) {
+                load(buf[(gi + 1) & 1], f0 + 6 + (gi + 1) * H);
+#pragma unroll
+                for (int i = 0; i < H; ++i) {
+                    double L, R;
+                    if (!w.face<MPF>(a, L, R)) bad |= 1u << (gi * H + i);
+                    tl[0][gi * H + i][lane] = L;
+                    tl[1][gi * H + i][lane] = R;
+                    w.push(a, buf[gi & 1][i]);
+                }
+            }
+            bad &= (nF >= 32) ? ~0u : ((1u << nF) - 1u);
+            while (bad) {
+                const int i = __ffs(bad) - 1;
+                bad &= bad - 1;
+                double L, R;
+                march64_redo<MPF>(a, col, f0 + i, L, R);
+                tl[0][i][lane] = L;
+                tl[1][i][lane] = R;
+            }
+            __syncwarp();
+            // lanes take faces, the warp walks the columns (two per store)
+            const int fi = lane & (F - 1), cj = lane / F;
+#pragma unroll 4
+            for (int c = cj; c < 32; c += 32 / F) {
+                if (ut * 32 + c < a.Nu && fi < nF) {
+                    const long long oi = obase + c * a.oU + f0 + fi;
+                    outL[oi] = tl[0][fi][c];
+                    outR[oi] = tl[1][fi][c];
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Arguments of a marching sweep for face-independent WENO5-JS coefficients
+// (everything but the segmentation).
+inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, void* vR, const WenoParams& wp,
+                                 const double* ucf) {
     MarchArgs a{};
     a.in = in; a.vL = vL; a.vR = vR; a.wp = wp;
     a.ns = g.ns; a.nc = g.nc;
@@ -322,6 +600,21 @@ int launch_march_sweep(const SweepGeom& g, bool mp, const T* in, T* vL, T* vR, c
         a.ucf32[q] = (float)ucf[q];          // polyL (Coef<5>::pL)
         a.ucf32[6 + q] = (float)ucf[6 + q];  // polyR
     }
+    for (int r = 0; r < 3; ++r)
+        for (int s = 0; s < 2; ++s) {
+            a.kL[2 * r + s] = ucf[12 + r] * ucf[2 * r + s];
+            a.kR[2 * r + s] = ucf[15 + r] * ucf[6 + 2 * r + s];
+        }
+    return a;
+}
+
+// Launch for face-independent WENO5-JS coefficients.  Returns 1003 when
+// the sweep has too few faces for the window.
+template <typename T>
+int launch_march_sweep(const SweepGeom& g, bool mp, const T* in, T* vL, T* vR, const WenoParams& wp,
+                       const double* ucf, cudaStream_t st, int sms) {
+    if (g.nc < 1 || !ucf) return 1003;
+    MarchArgs a = make_march_args(g, in, vL, vR, wp, ucf);
     // segments: enough warps to fill the GPU about four times over
     constexpr int F = MarchFlush<T>::F;
     const long long cols = (long long)a.n_ut * a.Nw * a.NV;
@@ -340,8 +633,14 @@ int launch_march_sweep(const SweepGeom& g, bool mp, const T* in, T* vL, T* vR, c
     const long long cap = (long long)sms * 64;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    if (mp) sweep_march_kernel<true, T><<<(unsigned)blocks, 128, 0, st>>>(a);
-    else sweep_march_kernel<false, T><<<(unsigned)blocks, 128, 0, st>>>(a);
+    if constexpr (sizeof(T) == 8) {
+        static_assert(MarchFlush<double>::F == kMarch64F, "FP64 segment rounding");
+        if (mp) sweep_march64_kernel<true><<<(unsigned)blocks, 128, 0, st>>>(a);
+        else sweep_march64_kernel<false><<<(unsigned)blocks, 128, 0, st>>>(a);
+    } else {
+        if (mp) sweep_march_kernel<true, T><<<(unsigned)blocks, 128, 0, st>>>(a);
+        else sweep_march_kernel<false, T><<<(unsigned)blocks, 128, 0, st>>>(a);
+    }
     return 0;
 }
 

@@ -23,6 +23,7 @@
 #include "sweep_tma.cuh"
 #include "sweep_pipe.cuh"
 #include "sweep_march.cuh"
+#include "sweep_march_tma.cuh"
 #include "weno_adjoint.cuh"
 #include "batched.cuh"
 
@@ -268,7 +269,8 @@ int launch_generic(const SweepGeom& g, int order, bool mp, const T* in, T* vL, T
 // (read per call): "auto" (default: TMA pipeline for FP64 when the layout
 // allows it, else the cp.async pipeline, else the general-stride kernel),
 // "tma", "cpasync" or "generic" to pin one for testing.
-// WENO_SB_KERNEL: auto (0), generic (1), cpasync (2), march (3), tma (4).
+// WENO_SB_KERNEL: auto (0), generic (1), cpasync (2), march (3), tma (4),
+// march_ldg (5: the marching kernel with per-lane loads, no TMA staging).
 // A forced kernel that does not cover the case falls through to the next
 // one in the auto order (march, tma, cp.async, generic).
 int kernel_choice() {
@@ -277,6 +279,7 @@ int kernel_choice() {
     if (e && strcmp(e, "cpasync") == 0) return 2;
     if (e && strcmp(e, "march") == 0) return 3;
     if (e && strcmp(e, "tma") == 0) return 4;
+    if (e && strcmp(e, "march_ldg") == 0) return 5;
     return 0;
 }
 
@@ -294,7 +297,15 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
-    if ((choice == 0 || choice == 3) && ucf && order == 5 && gr->scheme == WENO_SB_JS) {
+    if ((choice == 0 || choice == 3 || choice == 5) && ucf && order == 5 && gr->scheme == WENO_SB_JS) {
+        if constexpr (sizeof(T) == 8) {
+            if (choice != 5 && g.nc >= 1) {
+                const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
+                int rc = launch_march_tma(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
+                if (rc != WENO_SB_ERR_UNSUPPORTED)
+                    return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch") : rc;
+            }
+        }
         int rc = launch_march_sweep<T>(g, mp, in, vL, vR, wp, ucf, st, num_sms());
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
     }
