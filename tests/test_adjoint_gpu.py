@@ -235,8 +235,9 @@ def test_vjp_rejects_unsupported(wsb):
     import torch
     from wenostandalone_b200 import _lib as L, api, fields
     g = wsb.Grid(7, 7, 7, 1, 6, scheme=1)
-    t = torch.zeros(10, dtype=torch.float64, device="cuda")
+    t = torch.zeros(int(np.prod(g.rs_shape(0))), dtype=torch.float64, device="cuda")
+    f = torch.zeros(int(np.prod(g.face_shape(0))), dtype=torch.float64, device="cuda")
     coefs = fields.uniform_weno_coefficients(5, g.nc(0))
     with pytest.raises(L.WenoError) as e:
-        api.vjp(g, 0, 5, t, coefs, t, t, t, uniform=True)
+        api.vjp(g, 0, 5, t, coefs, f, f, torch.zeros_like(t), uniform=True)
     assert e.value.code == L.ERR_UNSUPPORTED

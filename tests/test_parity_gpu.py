@@ -370,6 +370,25 @@ def test_argument_errors(wsb):
     assert rc == L.ERR_ARG and "buff_size" in L.last_error()
 
 
+def test_device_api_refuses_mismatched_arrays(wsb):
+    """The device-pointer calls take bare pointers: a float32 v_vf where the
+    library reads FP64, or an array shorter than the call's extent, is
+    refused on the host before any kernel runs."""
+    import torch
+    from wenostandalone_b200 import api, fields
+    g = wsb.Grid(9, 9, 9, 2, 6)
+    v64 = to_dev(fields.smooth_jump_field(9, 9, 9, 2, 6, seed=1))
+    rs = torch.empty(int(np.prod(g.rs_shape(0))), dtype=torch.float32, device="cuda")
+    with pytest.raises(TypeError):
+        api.reshape(g, 0, v64.to(torch.float32), rs)
+    api.reshape(g, 0, v64, rs)
+    L = torch.empty(int(np.prod(g.face_shape(0))), dtype=torch.float32, device="cuda")
+    with pytest.raises(ValueError):
+        api.weno_uniform(g, 0, 5, rs[:-1], fields.uniform_weno_coefficients(5, g.nc(0)), L, L.clone())
+    with pytest.raises(TypeError):
+        api.weno_uniform(g, 0, 5, rs, fields.uniform_weno_coefficients(5, g.nc(0)), L, L.double())
+
+
 def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64", entry="arrays"):
     import torch
     from wenostandalone_b200 import api, fields
@@ -391,10 +410,14 @@ def _fp32_case(wsb, oracle_mod, order, d, mp, field_for_oracle="fp64", entry="ar
         api.weno_uniform(g, d, order, rs32, coefs, L, R, flags=wsb.F_MP if mp else 0)
     else:
         api.weno(g, d, order, rs32, tuple(to_dev(c) for c in coefs), L, R, flags=wsb.F_MP if mp else 0)
-    core = (slice(3, g.extents(d)[0] - 3),)
+    ns = g.extents(d)[0]
+    core = (slice(3, ns - 3),)
     out = []
     for got, ref in ((L, Lr), (R, Rr)):
-        got = from_dev(got, g.face_shape(d))[core]
+        full = from_dev(got, g.face_shape(d))
+        # faces outside the core keep what the caller put there (zeros)
+        assert not np.any(full[:3]) and not np.any(full[ns - 3:])
+        got = full[core]
         ref = ref[core]
         out.append((rel_err(got, ref), float(np.sqrt(np.mean((got - ref) ** 2)) / np.abs(ref).max())))
     return out

@@ -199,12 +199,58 @@ def _dtype_of(t) -> int:
     return L.FP32 if t.dtype == torch.float32 else L.FP64
 
 
+def _need(name: str, t, n: int, dtypes) -> None:
+    """Refuse a tensor the C call would read or write out of its bounds: the
+    device-pointer entries take bare pointers, so the element type and count
+    are checked here (a float32 array where FP64 is read, or a short array,
+    would otherwise make the kernel access memory it does not own)."""
+    import torch
+    if t is None:
+        raise ValueError(f"{name} is missing")
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype not in dtypes:
+        raise TypeError(f"{name} has dtype {t.dtype}; expected {' or '.join(str(x) for x in dtypes)}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if t.numel() < n:
+        raise ValueError(f"{name} has {t.numel()} elements; the call accesses {n}")
+
+
+def _f64():
+    import torch
+    return (torch.float64,)
+
+
+def _same(t):
+    return (t.dtype,) if t is not None else _f64()
+
+
+def _check_sweep(grid: Grid, d: int, v_in, vL, vR, folded: bool) -> None:
+    """Sizes of a sweep's arrays; an invalid direction is left for the
+    library to report (WENO_SB_ERR_ARG)."""
+    import torch
+    if d not in (0, 1, 2):
+        return
+    _need("vL", vL, int(np.prod(grid.face_shape(d))), (torch.float64, torch.float32))
+    _need("vR", vR, int(np.prod(grid.face_shape(d))), _same(vL))
+    n_in = int(np.prod(grid.vf_shape() if folded else grid.rs_shape(d)))
+    _need("v_in", v_in, n_in, _same(vL))
+
+
 def reshape(grid: Grid, d: int, v_vf, out, stream=None) -> None:
+    import torch
+    _need("v_vf", v_vf, int(np.prod(grid.vf_shape())), _f64())
+    _need("out", out, int(np.prod(grid.rs_shape(d))), (torch.float64, torch.float32))
     check(lib().weno_sb_reshape_dev(ctypes.byref(grid.c()), d, _dtype_of(out), _ptr(v_vf), _ptr(out),
                                     _stream(stream)))
 
 
 def order1_copy(grid: Grid, d: int, v_vf, vL, vR, stream=None) -> None:
+    import torch
+    _need("v_vf", v_vf, int(np.prod(grid.vf_shape())), _f64())
+    _need("vL", vL, int(np.prod(grid.face_shape(d))), (torch.float64, torch.float32))
+    _need("vR", vR, int(np.prod(grid.face_shape(d))), _same(vL))
     check(lib().weno_sb_order1_dev(ctypes.byref(grid.c()), d, _dtype_of(vL), _ptr(v_vf), _ptr(vL), _ptr(vR),
                                    _stream(stream)))
 
@@ -216,6 +262,8 @@ def coefs_struct(coefs) -> L.WenoCoefs:
 
 def weno(grid: Grid, d: int, order: int, v_in, coefs, vL, vR, flags: int = 0, stream=None) -> None:
     cs = coefs if isinstance(coefs, L.WenoCoefs) else coefs_struct(coefs)
+    if order in (1, 3, 5, 7):
+        _check_sweep(grid, d, v_in, vL, vR, bool(flags & L.F_FOLDED))
     check(lib().weno_sb_weno_dev(ctypes.byref(grid.c()), d, order, flags, _dtype_of(vL), _ptr(v_in),
                                  ctypes.byref(cs), _ptr(vL), _ptr(vR), _stream(stream)))
 
@@ -242,6 +290,8 @@ def weno_uniform(grid: Grid, d: int, order: int, v_in, face, vL, vR, flags: int 
     """Reconstruction with face-independent coefficients (`face`: a
     WenoFaceCoefs, or numpy coefficient arrays whose face 0 is used)."""
     f = face if isinstance(face, L.WenoFaceCoefs) else face_coefs(face)
+    if order in (1, 3, 5, 7):
+        _check_sweep(grid, d, v_in, vL, vR, bool(flags & L.F_FOLDED))
     check(lib().weno_sb_weno_uniform_dev(ctypes.byref(grid.c()), d, order, flags, _dtype_of(vL), _ptr(v_in),
                                          ctypes.byref(f), _ptr(vL), _ptr(vR), _stream(stream)))
 
@@ -257,11 +307,18 @@ def vjp(grid: Grid, d: int, order: int, v_in, coefs, gL, gR, gv, flags: int = 0,
     else:
         cs = coefs if isinstance(coefs, L.WenoCoefs) else coefs_struct(coefs)
         cs, fp = ctypes.byref(cs), None
+    if d in (0, 1, 2) and order in (3, 5, 7):
+        n_in = int(np.prod(grid.vf_shape() if flags & L.F_FOLDED else grid.rs_shape(d)))
+        _need("v_in", v_in, n_in, _f64())
+        _need("gv", gv, n_in, _f64())
+        _need("gL", gL, int(np.prod(grid.face_shape(d))), _f64())
+        _need("gR", gR, int(np.prod(grid.face_shape(d))), _f64())
     check(lib().weno_sb_vjp_dev(ctypes.byref(grid.c()), d, order, flags, _ptr(v_in), cs, fp, _ptr(gL), _ptr(gR),
                                 _ptr(gv), _stream(stream)))
 
 
 def preserve_monotonicity(grid: Grid, d: int, v_rs_ws, vL, vR, stream=None) -> None:
+    _check_sweep(grid, d, v_rs_ws, vL, vR, False)
     check(lib().weno_sb_preserve_monotonicity_dev(ctypes.byref(grid.c()), d, _dtype_of(vL), _ptr(v_rs_ws),
                                                   _ptr(vL), _ptr(vR), _stream(stream)))
 

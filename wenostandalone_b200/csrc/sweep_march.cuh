@@ -53,6 +53,8 @@ struct MarchArgs {
     // FP64 kernel: candidate-polynomial coefficients scaled by the ideal
     // weights, kL[2r+s] = dL[r] * polyL[s][r] (and kR likewise)
     double kL[6], kR[6];
+    // FP32-bulk engine: (polyL, polyR) float pairs, Coef<5>::pL index order
+    float2 pf2[6];
 };
 
 // Second-order minmod of the MP limiter (same decisions as mp_minmod /
@@ -483,6 +485,156 @@ __device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __re
     if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
 }
 
+// ---------------------------------------------------------------------
+// FP32-bulk marching engine: FP32 cells and face states; FP64 differences,
+// beta and weight normalisation (the parts that cancel or need eps = 1e-16),
+// as weno5_js_mixed; FP32 candidate offsets and MP limiter, with the left
+// and right states carried as float pairs (sm_100 paired FP32 arithmetic).
+// ---------------------------------------------------------------------
+// FP32 minmod of the MP limiter (the value of mp_minmod_f up to the sign of
+// a zero result).
+__device__ __forceinline__ float mm32(float dl, float dr) {
+    const float m = fminf(fabsf(dl), fabsf(dr)), M = fmaxf(fabsf(dl), fabsf(dr));
+    const float u = fminf(fmaf(4.0f, m, -M), m);
+    const int hl = __float_as_int(dl), hu = __float_as_int(u);
+    const int kill = ((hl ^ __float_as_int(dr)) | hu) >> 31;
+    return __int_as_float((hu & ~kill) | (hl & (int)0x80000000));
+}
+
+// A weight w in [0, 2) to float through 2 + w, whose exponent is fixed:
+// the float mantissa is read off the double's bits and 2 is taken back off
+// exactly.  Truncation, absolute error below 2^-22; the weights only scale
+// differences of candidate offsets, so an absolute bound is what matters.
+__device__ __forceinline__ float w2f(double w) {
+    const double s = 2.0 + w;
+    const unsigned t = __funnelshift_l((unsigned)__double2loint(s), (unsigned)__double2hiint(s), 3);
+    return __uint_as_float((t & 0x007FFFFFu) | 0x40000000u) - 2.0f;
+}
+
+// +-1 with the sign of x.
+__device__ __forceinline__ float sign1(float x) {
+    return __int_as_float((__float_as_int(x) & (int)0x80000000) | 0x3F800000);
+}
+
+struct March32 {
+    float vm1, v0, vp1, vp2;    // cells J-1 .. J+2
+    float fm2, fm1, f0, fp1;    // FP32 differences v[k+1] - v[k], k = J-2 .. J+1
+    double Dp2;                 // vp2, widened
+    double dp1;                 // FP64 d[J+1]
+    double s1;                  // d[J+1]^2
+    double b0, b1, b2;          // beta_0, beta_1, beta_2 of face J
+    double b1n, b2n, b2nn;      // beta_1(J+1), beta_2(J+1), beta_2(J+2)
+    float e2;                   // curvature fp1 - f0
+    float mA, mB;               // minmod(e2[J-1], e2[J]), minmod(e2[J], e2[J+1])
+
+    __device__ __forceinline__ void init(const MarchArgs& a, float c0, float c1, float c2, float c3, float c4) {
+        vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
+        fm2 = c1 - c0; fm1 = c2 - c1; f0 = c3 - c2; fp1 = c4 - c3;
+        const double D0 = f2d_bits(c0), D1 = f2d_bits(c1), D2 = f2d_bits(c2), D3 = f2d_bits(c3);
+        Dp2 = f2d_bits(c4);
+        const double dm2 = D1 - D0, dm1 = D2 - D1, d0 = D3 - D2;
+        dp1 = Dp2 - D3;
+        const double sm2 = dm2 * dm2, sm1 = dm1 * dm1, s0 = d0 * d0;
+        s1 = dp1 * dp1;
+        double g0, g1, g2, u;
+        March64::betas(a, sm2, dm2 * dm1, sm1, u, u, b2);
+        March64::betas(a, sm1, dm1 * d0, s0, u, b1, b2n);
+        March64::betas(a, s0, d0 * dp1, s1, g0, g1, g2);
+        b0 = g0; b1n = g1; b2nn = g2;
+        const float em = fm1 - fm2, ez = f0 - fm1;
+        e2 = fp1 - f0;
+        mA = mm32(em, ez);
+        mB = mm32(ez, e2);
+    }
+
+    __device__ __forceinline__ void push(const MarchArgs& a, float n) {
+        const double Dn = f2d_bits(n);
+        const double dn = Dn - Dp2;
+        const double sn = dn * dn;
+        double g0, g1, g2;
+        March64::betas(a, s1, dp1 * dn, sn, g0, g1, g2);
+        const float fn = n - vp2;
+        const float ne2 = fn - fp1;
+        const float nmB = mm32(e2, ne2);
+        vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
+        fm2 = fm1; fm1 = f0; f0 = fp1; fp1 = fn;
+        Dp2 = Dn; dp1 = dn; s1 = sn;
+        b0 = g0; b1 = b1n; b2 = b2n;
+        b1n = g1; b2n = b2nn; b2nn = g2;
+        e2 = ne2; mA = mB; mB = nmB;
+    }
+
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, float& L, float& R) const {
+        const double q0 = b0 * b0, q1 = b1 * b1, q2 = b2 * b2;
+        const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+        const double aL0 = a.ucf[12] * P0, aL2 = a.ucf[14] * P2, aR0 = a.ucf[15] * P0, aR2 = a.ucf[17] * P2;
+        const double SL = fma(a.ucf[13], P1, aL0 + aL2), SR = fma(a.ucf[16], P1, aR0 + aR2);
+        const bool ok = mid_range(SL) && mid_range(SR);
+        const double r = rcp1(SL * SR), gL = SR * r, gR = SL * r;
+        const float2 W0 = make_float2(w2f(aL0 * gL), w2f(aR0 * gR));
+        const float2 W2 = make_float2(w2f(aL2 * gL), w2f(aR2 * gR));
+        // candidate offsets e_k = p_k - v0, (left, right) pairs
+        const float2 E0 = __ffma2_rn(a.pf2[0], make_float2(fp1, fp1), __fmul2_rn(a.pf2[1], make_float2(f0, f0)));
+        const float2 E1 = __ffma2_rn(a.pf2[2], make_float2(f0, f0), __fmul2_rn(a.pf2[3], make_float2(fm1, fm1)));
+        const float2 E2 = __ffma2_rn(a.pf2[4], make_float2(fm1, fm1), __fmul2_rn(a.pf2[5], make_float2(fm2, fm2)));
+        const float2 m1 = make_float2(-1.0f, -1.0f);
+        // x = e1 + w0 (e0 - e1) + w2 (e2 - e1)
+        float2 x = __ffma2_rn(W0, __ffma2_rn(E1, m1, E0), __ffma2_rn(W2, __ffma2_rn(E1, m1, E2), E1));
+        if constexpr (MPF) {
+            // one-sided median in offset space (see March64::face): with
+            // s = sign(x), s * result = min(s x, max(max(0, -s b), s MD),
+            // max(max(0, s UL), s LC)); the right state is the left formula
+            // with (b, c, mA, mB) -> (-c, -b, mB, mA), b = v0 - vm1, c = vp1 - v0
+            const float2 s = make_float2(sign1(x.x), sign1(x.y));
+            const float2 bb = make_float2(fm1, -f0), cc = make_float2(f0, -fm1);
+            const float2 mmA = make_float2(mA, mB), mmB = make_float2(mB, mA);
+            const float2 h = make_float2(-0.5f, -0.5f);
+            const float2 sMD = __fmul2_rn(__fmul2_rn(s, h), __fadd2_rn(bb, mmA));
+            const float2 sLC = __fmul2_rn(s, __ffma2_rn(make_float2(4.0f / 3.0f, 4.0f / 3.0f), mmB, __fmul2_rn(h, cc)));
+            const float2 sUL = __fmul2_rn(s, __fmul2_rn(make_float2(-2.0f, -2.0f), cc));
+            const float2 sNB = __fmul2_rn(s, __fmul2_rn(m1, bb));
+            const float2 sx = __fmul2_rn(s, x);
+            float2 T;
+            T.x = fminf(fminf(sx.x, fmaxf(fmaxf(0.0f, sNB.x), sMD.x)), fmaxf(fmaxf(0.0f, sUL.x), sLC.x));
+            T.y = fminf(fminf(sx.y, fmaxf(fmaxf(0.0f, sNB.y), sMD.y)), fmaxf(fmaxf(0.0f, sUL.y), sLC.y));
+            x = __fmul2_rn(s, T);
+        }
+        const float2 o = __fadd2_rn(make_float2(v0, v0), x);
+        L = o.x;
+        R = o.y;
+        return ok;
+    }
+};
+
+// The reference sequence for one FP32-bulk face (cells o+1 .. o+5).
+template <bool MPF>
+__device__ __noinline__ void march32_redo(const MarchArgs& a, const float* __restrict__ col, long long o, float& L,
+                                          float& R) {
+    Coef<5> c;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        c.pL[q] = a.ucf[q];
+        c.pR[q] = a.ucf[6 + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        c.dL[q] = a.ucf[12 + q];
+        c.dR[q] = a.ucf[15 + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) c.b[q] = a.ucf[18 + q];
+    const float* p = col + (o + 1) * a.sJ;
+    const float vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
+                vp2 = __ldg(p + 4 * a.sJ);
+    double Ld, Rd;
+    weno5_face<float>(f2d_bits(vm2), f2d_bits(vm1), f2d_bits(v0), f2d_bits(vp1), f2d_bits(vp2), c, JS, a.wp.eps, 0.0,
+                      Ld, Rd);
+    L = (float)Ld;
+    R = (float)Rd;
+    if (MPF) MP<float>::apply(vm2, vm1, v0, vp1, vp2, L, R);
+}
+
 #ifndef WSB_MARCH64_MIN_BLOCKS
 #define WSB_MARCH64_MIN_BLOCKS 3
 #endif
@@ -605,6 +757,7 @@ inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, v
             a.kL[2 * r + s] = ucf[12 + r] * ucf[2 * r + s];
             a.kR[2 * r + s] = ucf[15 + r] * ucf[6 + 2 * r + s];
         }
+    for (int q = 0; q < 6; ++q) a.pf2[q] = make_float2((float)ucf[q], (float)ucf[6 + q]);
     return a;
 }
 

@@ -36,14 +36,30 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "sweep_march.cuh"
 #include "sweep_pipe.cuh"
 
 namespace wsb {
 
+#ifndef WSB_MTMA_MIN_BLOCKS
+#define WSB_MTMA_MIN_BLOCKS 3   // CTAs per SM the kernel is register-capped for
+#endif
+#ifndef WSB_MTMA_STAGES
+#define WSB_MTMA_STAGES 4       // input tiles per warp
+#endif
+#ifndef WSB_MTMA_OUTBUF
+#define WSB_MTMA_OUTBUF 2       // output tiles per warp (1: each store is waited before the next chunk)
+#endif
 constexpr int kTmaF = 8;        // faces per chunk = cells per input tile
-constexpr int kTmaStages = 4;   // input tiles per warp
-constexpr int kTmaWarps = 4;    // warps per CTA
+constexpr int kTmaStages = WSB_MTMA_STAGES;
+constexpr int kTmaOut = WSB_MTMA_OUTBUF;
+#ifndef WSB_MTMA_WARPS
+#define WSB_MTMA_WARPS 4        // warps per CTA (each with its own pipeline)
+#endif
+constexpr int kTmaWarps = WSB_MTMA_WARPS;
+static_assert(WSB_MTMA_STAGES <= 4, "the per-lane copy loader waits with at most 3 groups in flight");
 
 struct MarchTmaArgs {
     int kind;          // 0: sweep axis innermost (row tiles), 1: cross axis innermost
@@ -52,6 +68,7 @@ struct MarchTmaArgs {
     int odimU, odimW;  // output map dimension of the lane / outer cross axis
     int stage_bytes;   // one input tile (KIND 0: 2048, KIND 1: 8 rows x 34 cells)
     int warp_bytes;    // shared memory per warp, a multiple of 1024
+    int ring_off;      // byte offset of the input ring within a warp's area
     unsigned box_bytes;
 };
 
@@ -63,30 +80,55 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void*
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-// Byte offset of element (row, i) of a tile of 64-byte rows under the
-// 64-byte swizzle (16-byte chunk index XOR row bits 1..2).
-__device__ __forceinline__ unsigned sw64(unsigned row, unsigned i) {
-    const unsigned off = row * 64u + i * 8u;
-    return off ^ ((off >> 3) & 0x30u);
+// Byte offset of element (row, i) of a tile with rows of 8 elements of T
+// under the TMA swizzle of that row width: 64-byte rows (double) swap
+// 16-byte chunks by row bits 1..2, 32-byte rows (float) by row bit 2.
+template <typename T>
+__device__ __forceinline__ unsigned swz(unsigned row, unsigned i) {
+    if constexpr (sizeof(T) == 8) {
+        const unsigned off = row * 64u + i * 8u;
+        return off ^ ((off >> 3) & 0x30u);
+    } else {
+        const unsigned off = row * 32u + i * 4u;
+        return off ^ ((off >> 3) & 0x10u);
+    }
 }
 
-template <bool MPF, int KIND>
-__global__ void __launch_bounds__(kTmaWarps * 32, 3)
+template <typename T> struct MarchEngine;
+template <> struct MarchEngine<double> { using type = March64; };
+template <> struct MarchEngine<float> { using type = March32; };
+
+template <bool MPF>
+__device__ __forceinline__ void march_redo(const MarchArgs& a, const double* col, long long o, double& L, double& R) {
+    march64_redo<MPF>(a, col, o, L, R);
+}
+template <bool MPF>
+__device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col, long long o, float& L, float& R) {
+    march32_redo<MPF>(a, col, o, L, R);
+}
+
+template <bool MPF, int KIND, typename T, int LDR>
+__global__ void __launch_bounds__(kTmaWarps * 32, WSB_MTMA_MIN_BLOCKS)
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
                            const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
                            const MarchTmaArgs t) {
     constexpr int F = kTmaF, S = kTmaStages;
+    constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
+    constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
+    constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
+    using Engine = typename MarchEngine<T>::type;
     extern __shared__ __align__(1024) unsigned char smem_mt[];
     unsigned char* base = smem_mt + ((1024u - (smem_u32(smem_mt) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // per warp: 2 output buffers x (vL, vR) x 2048 bytes, then S input tiles
+    // per warp: kTmaOut output buffers x (vL, vR), then S input tiles
     const int warp_bytes = t.warp_bytes;
     unsigned char* wbase = base + (size_t)warp * warp_bytes;
     unsigned char* obuf = wbase;
-    unsigned char* ring = wbase + 4 * 2048;
+    unsigned char* ring = wbase + t.ring_off;
     unsigned long long* bars = (unsigned long long*)(base + (size_t)kTmaWarps * warp_bytes) + warp * S;
     if (lane == 0) {
         for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
@@ -94,38 +136,71 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 3)
     }
     __syncwarp();
 
-    double* __restrict__ outL = (double*)a.vL;
-    double* __restrict__ outR = (double*)a.vR;
+    T* __restrict__ outL = (T*)a.vL;
+    T* __restrict__ outR = (T*)a.vR;
     const long long nwarps = (long long)gridDim.x * kTmaWarps;
     const int o_last = (int)a.ns - 3;         // one past the last core face
-    unsigned long long n_issued = 0, n_waited = 0;  // tiles requested / completed (waited on) by this warp
+    unsigned n_issued = 0, n_waited = 0;      // tiles requested / completed (waited on) by this warp
     unsigned n_chunks = 0;                    // output chunks stored by this warp
     bool failed = false;
 
-    auto tile_ptr = [&](unsigned long long k) { return ring + (size_t)(k % S) * t.stage_bytes; };
+    auto tile_ptr = [&](unsigned k) { return ring + (size_t)(k % S) * t.stage_bytes; };
+    // byte offset in a tile of position p (0..7) of this lane's column
+    auto cell_off = [&](int p) -> unsigned {
+        if constexpr (KIND == 0) return swz<T>((unsigned)lane, (unsigned)p);
+        else return (unsigned)((p * XW + lane + XS) * sizeof(T));
+    };
+    auto column = [&](int u0, int wv, int vv) {
+        const int uc = u0 + lane < a.Nu ? u0 + lane : a.Nu - 1;
+        return (const T*)a.in + a.in_off + uc * a.sU + wv * a.sW + vv * a.sV;
+    };
     // request tile k (cells J0 .. J0+7) of the column group (u0, w, v)
-    auto issue = [&](unsigned long long k, int J0, int u0, int w, int v) {
-        if (lane == 0) {
-            unsigned long long* bar = &bars[k % S];
-            const int cU = t.uoff + u0, cW = t.woff + w;
-            const int c0 = t.dimJ == 0 ? J0 : (t.dimU == 0 ? cU : cW);
-            const int c1 = t.dimJ == 1 ? J0 : (t.dimU == 1 ? cU : cW);
-            const int c2 = t.dimJ == 2 ? J0 : (t.dimU == 2 ? cU : cW);
-            mbar_arrive_expect_tx(bar, t.box_bytes);
-            tma_load_4d(tile_ptr(k), &tin, bar, c0, c1, c2, v);
+    auto issue = [&](unsigned k, int J0, int u0, int w, int v) {
+        if constexpr (LDR == 0) {
+            if (lane == 0) {
+                unsigned long long* bar = &bars[k % S];
+                const int cU = t.uoff + u0, cW = t.woff + w;
+                const int c0 = t.dimJ == 0 ? J0 : (t.dimU == 0 ? cU : cW);
+                const int c1 = t.dimJ == 1 ? J0 : (t.dimU == 1 ? cU : cW);
+                const int c2 = t.dimJ == 2 ? J0 : (t.dimU == 2 ? cU : cW);
+                mbar_arrive_expect_tx(bar, t.box_bytes);
+                tma_load_4d(tile_ptr(k), &tin, bar, c0, c1, c2, v);
+            }
+        } else {
+            // each lane copies its own column's cells; cells past the end of
+            // the column are zero-filled without being read
+            unsigned char* tp = tile_ptr(k);
+            const T* col = column(u0, w, v);
+            const long long ncell = a.ns + 6;
+#pragma unroll
+            for (int p = 0; p < F; ++p) {
+                const long long J = (long long)J0 + p;
+                const bool inb = J < ncell;
+                const T* src = col + (inb ? J : 0) * a.sJ;
+                const unsigned dst = smem_u32(tp + cell_off(p));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src), "n"(sizeof(T)),
+                             "r"(inb ? (unsigned)sizeof(T) : 0u)
+                             : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
     };
-    auto wait_tile = [&](unsigned long long k) -> bool {
-        if (!mbar_wait(&bars[k % S], (unsigned)((k / S) & 1ull))) return false;
+    auto wait_tile = [&](unsigned k) -> bool {
+        if constexpr (LDR == 0) {
+            if (!mbar_wait(&bars[k % S], (k / S) & 1u)) return false;
+        } else {
+            // copy groups issued after tile k may stay in flight
+            const unsigned after = n_issued - (k + 1);
+            if (after >= 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+            else if (after == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+            else if (after == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
         n_waited = k + 1;
         return true;
     };
     // cell at position p (0..7) of tile k for this lane's column
-    auto cell = [&](unsigned long long k, int p) -> double {
-        const unsigned char* tp = tile_ptr(k);
-        if constexpr (KIND == 0) return *(const double*)(tp + sw64((unsigned)lane, (unsigned)p));
-        else return *(const double*)(tp + p * (34 * 8) + (lane + 1) * 8);
-    };
+    auto cell = [&](unsigned k, int p) -> T { return *(const T*)(tile_ptr(k) + cell_off(p)); };
 
     for (long long item = (long long)blockIdx.x * kTmaWarps + warp; item < a.n_items && !failed; item += nwarps) {
         const int sg = (int)(item % a.n_seg);
@@ -135,26 +210,22 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 3)
         const int wv = (int)(tt % a.Nw);
         const int vv = (int)(tt / a.Nw);
         const int u0 = ut * 32;
-        const int f_start = 4 + sg * a.seg;                       // even
+        const int f_start = 4 + sg * a.seg;                       // 4 mod 8
         int f_end = f_start + a.seg;
         if (f_end > o_last) f_end = o_last;
         const int nch = f_end > f_start ? (f_end - f_start + F - 1) / F : 0;
         const int ntiles = nch + 1;                               // tiles 0 .. nch
-        const unsigned long long k0 = n_issued;                   // first tile of this item
+        const unsigned k0 = n_issued;                             // first tile of this item
         for (int k = 0; k < ntiles && k < S; ++k) issue(k0 + k, f_start + F * k, u0, wv, vv);
         n_issued += (ntiles < S ? ntiles : S);
         if (!wait_tile(k0)) { failed = true; break; }
 
-        March64 w;
+        Engine w;
         if (sg == 0) {
             // face 3 (cells 4..8 = tile positions 0..4), plain stores
             w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
-            double L, R;
-            if (!w.face<MPF>(a, L, R)) {
-                const int uc = u0 + lane < a.Nu ? u0 + lane : a.Nu - 1;
-                const double* col = (const double*)a.in + a.in_off + uc * a.sU + wv * a.sW + vv * a.sV;
-                march64_redo<MPF>(a, col, 3, L, R);
-            }
+            T L, R;
+            if (!w.template face<MPF>(a, L, R)) march_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
             if (u0 + lane < a.Nu) {
                 const long long oi = 3 + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
                 outL[oi] = L;
@@ -167,50 +238,53 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 3)
         // chunk c: faces f0 .. f0+7 (f0 = f_start + 8c), pushes cells
         // f0+6 .. f0+13 = positions 6, 7 of tile c and 0 .. 5 of tile c+1
         for (int c = 0; c < nch; ++c) {
-            const unsigned long long kc = k0 + c;
+            const unsigned kc = k0 + c;
             if (!wait_tile(kc + 1)) { failed = true; break; }
             const int f0 = f_start + F * c;
-            unsigned char* ob = obuf + (size_t)(n_chunks & 1u) * 4096;
-            if (n_chunks >= 2) {
-                if (lane == 0) bulk_wait_read1();  // the store issued from this buffer two chunks ago has read it
+            unsigned char* ob = obuf + (size_t)(n_chunks % kTmaOut) * (2 * OB);
+            if (n_chunks >= (unsigned)kTmaOut) {
+                // the store issued from this buffer kTmaOut chunks ago has read it
+                if (lane == 0) {
+                    if constexpr (kTmaOut == 1) bulk_wait_read0();
+                    else bulk_wait_read1();
+                }
                 __syncwarp();
             }
             unsigned bad = 0;
 #pragma unroll
             for (int i = 0; i < F; ++i) {
-                double L, R;
-                if (!w.face<MPF>(a, L, R)) bad |= 1u << i;
-                *(double*)(ob + sw64((unsigned)lane, (unsigned)i)) = L;
-                *(double*)(ob + 2048 + sw64((unsigned)lane, (unsigned)i)) = R;
+                T L, R;
+                if (!w.template face<MPF>(a, L, R)) bad |= 1u << i;
+                *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
+                *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 w.push(a, (i < 2) ? cell(kc, 6 + i) : cell(kc + 1, i - 2));
             }
             const int nF = f_end - f0 < F ? f_end - f0 : F;
             bad &= (1u << nF) - 1u;
-            const int i_last = o_last - 1 - f0;  // the last core face, when in this chunk
             if (bad) {
-                const int uc = u0 + lane < a.Nu ? u0 + lane : a.Nu - 1;
-                const double* col = (const double*)a.in + a.in_off + uc * a.sU + wv * a.sW + vv * a.sV;
+                const T* col = column(u0, wv, vv);
                 while (bad) {
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
-                    double L, R;
-                    march64_redo<MPF>(a, col, f0 + i, L, R);
-                    *(double*)(ob + sw64((unsigned)lane, (unsigned)i)) = L;
-                    *(double*)(ob + 2048 + sw64((unsigned)lane, (unsigned)i)) = R;
+                    T L, R;
+                    march_redo<MPF>(a, col, f0 + i, L, R);
+                    *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
+                    *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
             }
+            const int i_last = o_last - 1 - f0;  // the last core face, when in this chunk
             if (i_last >= 0 && i_last < F && u0 + lane < a.Nu) {
                 // outside the store map's extent (see launch_march_tma)
                 const long long oi = (o_last - 1) + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
-                outL[oi] = *(const double*)(ob + sw64((unsigned)lane, (unsigned)i_last));
-                outR[oi] = *(const double*)(ob + 2048 + sw64((unsigned)lane, (unsigned)i_last));
+                outL[oi] = *(const T*)(ob + swz<T>((unsigned)lane, (unsigned)i_last));
+                outR[oi] = *(const T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i_last));
             }
             fence_async_shared();
             __syncwarp();
             if (lane == 0) {
                 const int c1 = t.odimU == 1 ? u0 : wv, c2 = t.odimU == 2 ? u0 : wv;
                 tma_store_4d(&toutL, ob, f0, c1, c2, vv);
-                tma_store_4d(&toutR, ob + 2048, f0, c1, c2, vv);
+                tma_store_4d(&toutR, ob + OB, f0, c1, c2, vv);
                 bulk_commit();
             }
             ++n_chunks;
@@ -227,22 +301,28 @@ __global__ void __launch_bounds__(kTmaWarps * 32, 3)
         // let the tiles still in flight land before the CTA's shared memory
         // is released (bounded, as every wait here); tiles are waited in
         // order, so those past the last completed one are the ones in flight
-        for (unsigned long long k = n_waited; k < n_issued; ++k)
-            mbar_wait(&bars[k % S], (unsigned)((k / S) & 1ull));
+        for (unsigned k = n_waited; k < n_issued; ++k) mbar_wait(&bars[k % S], (k / S) & 1u);
     }
+    if constexpr (LDR == 1) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (lane == 0) bulk_wait_all();
     __syncwarp();
 }
 
 // Host side.  Returns 1003 (unsupported) when the layout does not meet the
 // TMA rules (16-byte aligned bases, strides that are multiples of 16 bytes)
-// or the driver entry point is missing; the caller then uses sweep_march64.
-inline int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const double* in,
-                     double* vL, double* vR, const MarchArgs& a0, cudaStream_t st, int sms) {
+// or the driver entry point is missing; the caller then uses the marching
+// kernel with per-lane loads.
+template <typename T>
+int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const T* in, T* vL,
+                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms) {
+    constexpr int ES = (int)sizeof(T);
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return 1003;
-    if ((((uintptr_t)in) | ((uintptr_t)vL) | ((uintptr_t)vR)) & 15) return 1003;
-    if (g.ns < 7 || (g.ns & 1)) return 1003;
+    if ((((uintptr_t)vL) | ((uintptr_t)vR)) & 15) return 1003;
+    if (((uintptr_t)in) & (ES - 1)) return 1003;
+    // face rows of the outputs must be 16-byte multiples (ns even for FP64,
+    // a multiple of 4 for FP32); then ns - 4 faces is one too
+    if (g.ns < 8 || ((g.ns * ES) & 15)) return 1003;
     MarchArgs a = a0;
     MarchTmaArgs t{};
     const bool kind1 = folded && dir != 0;
@@ -250,74 +330,87 @@ inline int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, b
     cuuint64_t dims[4], strides[3];
     cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
     CUtensorMapSwizzle swz;
+    const int xw = ES == 8 ? 34 : 36;  // column-tile width: starts 16-byte aligned, left of column 0
     if (!folded) {
         // v_rs_ws (ns+6, c1, c2, V): lanes along c1
         dims[0] = g.ns + 6; dims[1] = g.c1; dims[2] = g.c2; dims[3] = g.nv;
         t.dimJ = 0; t.dimU = 1; t.dimW = 2; t.uoff = 0; t.woff = 0;
     } else {
+        // v_vf: column u, w sit at pad + 3; the column tile starts xw - 32 - 1 cells left of column 0
         dims[0] = E[0]; dims[1] = E[1]; dims[2] = E[2]; dims[3] = g.nv;
+        const int xo = 3 - (xw - 32 - 1);
         if (dir == 0) { t.dimJ = 0; t.dimU = 1; t.dimW = 2; t.uoff = 3; t.woff = 3; }
-        else if (dir == 1) { t.dimJ = 1; t.dimU = 0; t.dimW = 2; t.uoff = 2; t.woff = 3; }
-        else { t.dimJ = 2; t.dimU = 0; t.dimW = 1; t.uoff = 2; t.woff = 3; }
+        else if (dir == 1) { t.dimJ = 1; t.dimU = 0; t.dimW = 2; t.uoff = xo; t.woff = 3; }
+        else { t.dimJ = 2; t.dimU = 0; t.dimW = 1; t.uoff = xo; t.woff = 3; }
     }
     if (!kind1) {
         box[0] = kTmaF; box[1] = 32; box[2] = 1; box[3] = 1;
-        swz = CU_TENSOR_MAP_SWIZZLE_64B;
-        t.stage_bytes = 2048;
+        swz = ES == 8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+        t.stage_bytes = kTmaF * 32 * ES;
     } else {
-        box[0] = 34; box[1] = 1; box[2] = 1; box[3] = 1;
+        box[0] = xw; box[1] = 1; box[2] = 1; box[3] = 1;
         box[t.dimJ] = kTmaF;
         swz = CU_TENSOR_MAP_SWIZZLE_NONE;
-        t.stage_bytes = kTmaF * 34 * 8;  // 2176, a multiple of 128
+        t.stage_bytes = ((kTmaF * xw * ES + 127) / 128) * 128;
     }
-    t.box_bytes = (unsigned)(box[0] * box[1] * box[2] * box[3] * 8);
-    strides[0] = dims[0] * 8;
-    strides[1] = dims[0] * dims[1] * 8;
-    strides[2] = dims[0] * dims[1] * dims[2] * 8;
-    if (strides[0] % 16) return 1003;
+    t.box_bytes = (unsigned)(box[0] * box[1] * box[2] * box[3] * ES);
+    strides[0] = dims[0] * ES;
+    strides[1] = dims[0] * dims[1] * ES;
+    strides[2] = dims[0] * dims[1] * dims[2] * ES;
+    const CUtensorMapDataType dt = ES == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     CUtensorMap mi, mL, mR;
-    if (enc(&mi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)in, dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return 1003;
+    // input tiles by TMA when the field's rows are 16-byte multiples and its
+    // base is 16-byte aligned; otherwise (e.g. FP32 rows of 218 cells) each
+    // lane stages its own cells with cp.async into the same tile layout
+    int ldr = 1;
+    std::memset(&mi, 0, sizeof(mi));
+    if (strides[0] % 16 == 0 && (((uintptr_t)in) & 15) == 0 &&
+        enc(&mi, dt, 4, (void*)in, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+        ldr = 0;
     // outputs (ns, c1, c2, V).  The store unit clips the innermost axis in
-    // 16-byte steps, so the face extent is ns - 4 (even): faces up to ns-5
-    // are stored by the TMA unit, the last core face ns-4 with plain stores,
-    // and the non-core faces ns-3 .. ns-1 are never written.
+    // 16-byte steps, so the face extent is ns - 4 (a 16-byte multiple):
+    // faces up to ns-5 are stored by the TMA unit, the last core face ns-4
+    // with plain stores, and the non-core faces ns-3 .. ns-1 are never written.
     cuuint64_t od[4] = {(cuuint64_t)(g.ns - 4), (cuuint64_t)g.c1, (cuuint64_t)g.c2, (cuuint64_t)g.nv};
-    cuuint64_t os[3] = {(cuuint64_t)g.ns * 8, (cuuint64_t)(g.ns * g.c1) * 8, (cuuint64_t)(g.ns * g.c1 * g.c2) * 8};
+    cuuint64_t os[3] = {(cuuint64_t)g.ns * ES, (cuuint64_t)(g.ns * g.c1) * ES, (cuuint64_t)(g.ns * g.c1 * g.c2) * ES};
     cuuint32_t ob[4] = {kTmaF, 1, 1, 1};
-    // lanes run along the output axis with the smaller stride of the two
-    // cross axes the march launcher picked (a.oU == ns: c1, else c2)
+    // lanes run along the output axis the march arguments chose (oU == ns: c1, else c2)
     if (a.oU == g.ns) { t.odimU = 1; t.odimW = 2; }
     else { t.odimU = 2; t.odimW = 1; }
     ob[t.odimU] = 32;
-    if (enc(&mL, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)vL, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
-            CUDA_SUCCESS ||
-        enc(&mR, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)vR, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
-            CUDA_SUCCESS)
+    const CUtensorMapSwizzle oswz = ES == 8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    if (enc(&mL, dt, 4, (void*)vL, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, oswz,
+            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+        enc(&mR, dt, 4, (void*)vR, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, oswz,
+            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return 1003;
-    // lane axis must be the one the march launcher chose
+    // the lane axis must be the one the march arguments chose
     if ((t.kind == 1) != (a.sU == 1)) return 1003;
     // segments over faces [4, ns-3), a multiple of 8 faces each
-    const long long nf4 = g.ns - 3 - 4 > 0 ? g.ns - 3 - 4 : 0;
+    const long long nf4 = g.ns - 7;
     const long long cols = (long long)a.n_ut * a.Nw * a.NV;
     const long long want = (long long)sms * kTmaWarps * 3 * 2;
     long long nseg = (want + cols - 1) / cols;
-    const long long max_seg = nf4 > 0 ? (nf4 + kTmaF - 1) / kTmaF : 1;
+    const long long max_seg = (nf4 + kTmaF - 1) / kTmaF;
     if (nseg > max_seg) nseg = max_seg;
     if (nseg < 1) nseg = 1;
-    long long seg = nf4 > 0 ? (nf4 + nseg - 1) / nseg : kTmaF;
+    long long seg = (nf4 + nseg - 1) / nseg;
     seg = ((seg + kTmaF - 1) / kTmaF) * kTmaF;
     a.seg = (int)seg;
-    a.n_seg = nf4 > 0 ? (int)((nf4 + seg - 1) / seg) : 1;
+    a.n_seg = (int)((nf4 + seg - 1) / seg);
     a.n_items = cols * a.n_seg;
-    t.warp_bytes = ((4 * 2048 + kTmaStages * t.stage_bytes + 1023) / 1024) * 1024;
+    const int out_bytes = kTmaOut * 2 * 32 * kTmaF * ES;
+    t.ring_off = out_bytes;
+    t.warp_bytes = ((out_bytes + kTmaStages * t.stage_bytes + 1023) / 1024) * 1024;
     const size_t smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * kTmaStages * 8;
-    auto kfn = mp ? (kind1 ? sweep_march_tma_kernel<true, 1> : sweep_march_tma_kernel<true, 0>)
-                  : (kind1 ? sweep_march_tma_kernel<false, 1> : sweep_march_tma_kernel<false, 0>);
+    using KFn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, MarchArgs, MarchTmaArgs);
+    static const KFn table[2][2][2] = {
+        {{sweep_march_tma_kernel<false, 0, T, 0>, sweep_march_tma_kernel<false, 0, T, 1>},
+         {sweep_march_tma_kernel<false, 1, T, 0>, sweep_march_tma_kernel<false, 1, T, 1>}},
+        {{sweep_march_tma_kernel<true, 0, T, 0>, sweep_march_tma_kernel<true, 0, T, 1>},
+         {sweep_march_tma_kernel<true, 1, T, 0>, sweep_march_tma_kernel<true, 1, T, 1>}}};
+    const KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kTmaWarps * 32, smem);

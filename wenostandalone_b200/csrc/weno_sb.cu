@@ -298,13 +298,11 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
     if ((choice == 0 || choice == 3 || choice == 5) && ucf && order == 5 && gr->scheme == WENO_SB_JS) {
-        if constexpr (sizeof(T) == 8) {
-            if (choice != 5 && g.nc >= 1) {
-                const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
-                int rc = launch_march_tma(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
-                if (rc != WENO_SB_ERR_UNSUPPORTED)
-                    return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch") : rc;
-            }
+        if (choice != 5 && g.nc >= 1) {
+            const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
+            int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
+            if (rc != WENO_SB_ERR_UNSUPPORTED)
+                return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch") : rc;
         }
         int rc = launch_march_sweep<T>(g, mp, in, vL, vR, wp, ucf, st, num_sms());
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
