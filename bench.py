@@ -335,10 +335,10 @@ def run_ours(args):
                        "field": "seeded smooth-plus-jump", "l2": "inputs (663 MB) and outputs (3.7 GB) exceed "
                                                                   "the 126 MB L2; no flush",
                        "parallelism": f"{ws} independent blocks (weak scaling, no collective)"},
-            "roofline": {"bound": "hbm", "kernel": (f"sweep_fast_kernel<5,MP,float,JS> {'xyz'[dk]} sweep"
-                                                    if fp32_main else
-                                                    f"sweep_pipe_kernel<5,MP,JS,uniform> {'xyz'[dk]} sweep "
-                                                    f"({'row tiles' if dk == 0 else '128B-swizzled column tiles'})"),
+            "roofline": {"bound": "hbm", "kernel": (f"sweep_march_tma_kernel<MP,row tiles,float,cp.async loader> "
+                                                    f"{'xyz'[dk]} sweep" if fp32_main else
+                                                    f"sweep_march_tma_kernel<MP,{'row' if dk == 0 else 'column'} "
+                                                    f"tiles,double,TMA loader> {'xyz'[dk]} sweep"),
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
@@ -375,7 +375,7 @@ def run_ours(args):
 def read_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (line 'traffic_bytes_per_launch: <int>'), else None."""
-    p = os.path.join(ROOT, "profiles", "sweep_weno5_mp_fp64_200cubed.md")
+    p = os.path.join(ROOT, "profiles", "sweep_march_tma_fp64_200cubed.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
