@@ -74,9 +74,12 @@ def _scatter_to_vf(oracle_mod, shape_vf, m, n, p, buff, d, g_rs):
     return out.reshape(shape_vf, order="F")
 
 
-def test_vjp_folded_accumulates_three_sweeps(wsb, oracle_mod):
+@pytest.mark.parametrize("entry", ["arrays", "uniform"])
+def test_vjp_folded_accumulates_three_sweeps(wsb, oracle_mod, entry):
     """Folded sweeps read v_vf directly; with ACCUMULATE the x, y and z
-    adjoints sum into one gradient of v_vf."""
+    adjoints sum into one gradient of v_vf (per-face coefficient arrays, and
+    the face-independent entry, which takes the marching adjoint where the
+    face count is even)."""
     import torch
     from wenostandalone_b200 import api, fields
     m, n, p, nv = 21, 14, 11, 2
@@ -93,8 +96,11 @@ def test_vjp_folded_accumulates_three_sweeps(wsb, oracle_mod):
         gR = np.asfortranarray(rng.standard_normal(g.face_shape(d)))
         ref += _scatter_to_vf(oracle_mod, vf.shape, m, n, p, 6, d,
                               oracle_mod.vjp(rs, coefs, 5, gL, gR, mp=True))
-        api.vjp(g, d, 5, v, tuple(to_dev(c) for c in coefs), to_dev(gL), to_dev(gR), gv,
-                flags=wsb.F_MP | wsb.F_FOLDED | (wsb.F_ACCUMULATE if d > 0 else 0))
+        fl = wsb.F_MP | wsb.F_FOLDED | (wsb.F_ACCUMULATE if d > 0 else 0)
+        if entry == "uniform":
+            api.vjp(g, d, 5, v, coefs, to_dev(gL), to_dev(gR), gv, flags=fl, uniform=True)
+        else:
+            api.vjp(g, d, 5, v, tuple(to_dev(c) for c in coefs), to_dev(gL), to_dev(gR), gv, flags=fl)
     assert rel_err(from_dev(gv, vf.shape), ref) <= TOL_AD
 
 

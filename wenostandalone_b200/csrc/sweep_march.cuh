@@ -488,8 +488,10 @@ __device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __re
 // ---------------------------------------------------------------------
 // FP32-bulk marching engine: FP32 cells and face states; FP64 differences,
 // beta and weight normalisation (the parts that cancel or need eps = 1e-16),
-// as weno5_js_mixed; FP32 candidate offsets and MP limiter, with the left
-// and right states carried as float pairs (sm_100 paired FP32 arithmetic).
+// as weno5_js_mixed; FP32 candidate offsets and MP limiter.  (Written with
+// scalar FP32 arithmetic: the sm_100 paired FP32 instructions need both
+// halves in a register pair, and broadcasting the shared differences into
+// pairs cost more moves than the pairing saved.)
 // ---------------------------------------------------------------------
 // FP32 minmod of the MP limiter (the value of mp_minmod_f up to the sign of
 // a zero result).
@@ -572,37 +574,41 @@ struct March32 {
         const double SL = fma(a.ucf[13], P1, aL0 + aL2), SR = fma(a.ucf[16], P1, aR0 + aR2);
         const bool ok = mid_range(SL) && mid_range(SR);
         const double r = rcp1(SL * SR), gL = SR * r, gR = SL * r;
-        const float2 W0 = make_float2(w2f(aL0 * gL), w2f(aR0 * gR));
-        const float2 W2 = make_float2(w2f(aL2 * gL), w2f(aR2 * gR));
-        // candidate offsets e_k = p_k - v0, (left, right) pairs
-        const float2 E0 = __ffma2_rn(a.pf2[0], make_float2(fp1, fp1), __fmul2_rn(a.pf2[1], make_float2(f0, f0)));
-        const float2 E1 = __ffma2_rn(a.pf2[2], make_float2(f0, f0), __fmul2_rn(a.pf2[3], make_float2(fm1, fm1)));
-        const float2 E2 = __ffma2_rn(a.pf2[4], make_float2(fm1, fm1), __fmul2_rn(a.pf2[5], make_float2(fm2, fm2)));
-        const float2 m1 = make_float2(-1.0f, -1.0f);
+        const float wL0 = w2f(aL0 * gL), wL2 = w2f(aL2 * gL), wR0 = w2f(aR0 * gR), wR2 = w2f(aR2 * gR);
+        // candidate offsets e_k = p_k - v0; pf2[q] = (polyL, polyR) of Coef<5> index q
+        const float eL0 = fmaf(a.pf2[0].x, fp1, a.pf2[1].x * f0), eR0 = fmaf(a.pf2[0].y, fp1, a.pf2[1].y * f0);
+        const float eL1 = fmaf(a.pf2[2].x, f0, a.pf2[3].x * fm1), eR1 = fmaf(a.pf2[2].y, f0, a.pf2[3].y * fm1);
+        const float eL2 = fmaf(a.pf2[4].x, fm1, a.pf2[5].x * fm2), eR2 = fmaf(a.pf2[4].y, fm1, a.pf2[5].y * fm2);
         // x = e1 + w0 (e0 - e1) + w2 (e2 - e1)
-        float2 x = __ffma2_rn(W0, __ffma2_rn(E1, m1, E0), __ffma2_rn(W2, __ffma2_rn(E1, m1, E2), E1));
+        float xL = fmaf(wL0, eL0 - eL1, fmaf(wL2, eL2 - eL1, eL1));
+        float xR = fmaf(wR0, eR0 - eR1, fmaf(wR2, eR2 - eR1, eR1));
         if constexpr (MPF) {
             // one-sided median in offset space (see March64::face): with
             // s = sign(x), s * result = min(s x, max(max(0, -s b), s MD),
-            // max(max(0, s UL), s LC)); the right state is the left formula
-            // with (b, c, mA, mB) -> (-c, -b, mB, mA), b = v0 - vm1, c = vp1 - v0
-            const float2 s = make_float2(sign1(x.x), sign1(x.y));
-            const float2 bb = make_float2(fm1, -f0), cc = make_float2(f0, -fm1);
-            const float2 mmA = make_float2(mA, mB), mmB = make_float2(mB, mA);
-            const float2 h = make_float2(-0.5f, -0.5f);
-            const float2 sMD = __fmul2_rn(__fmul2_rn(s, h), __fadd2_rn(bb, mmA));
-            const float2 sLC = __fmul2_rn(s, __ffma2_rn(make_float2(4.0f / 3.0f, 4.0f / 3.0f), mmB, __fmul2_rn(h, cc)));
-            const float2 sUL = __fmul2_rn(s, __fmul2_rn(make_float2(-2.0f, -2.0f), cc));
-            const float2 sNB = __fmul2_rn(s, __fmul2_rn(m1, bb));
-            const float2 sx = __fmul2_rn(s, x);
-            float2 T;
-            T.x = fminf(fminf(sx.x, fmaxf(fmaxf(0.0f, sNB.x), sMD.x)), fmaxf(fmaxf(0.0f, sUL.x), sLC.x));
-            T.y = fminf(fminf(sx.y, fmaxf(fmaxf(0.0f, sNB.y), sMD.y)), fmaxf(fmaxf(0.0f, sUL.y), sLC.y));
-            x = __fmul2_rn(s, T);
+            // max(max(0, s UL), s LC)), b = v0 - vm1, c = vp1 - v0; the
+            // right state is the same formula with (b, c, mA, mB) -> (-c, -b, mB, mA)
+            const float kB = 4.0f / 3.0f;
+            {
+                const float sg = sign1(xL);
+                const float sMD = (-0.5f * sg) * (fm1 + mA);
+                const float sLC = sg * fmaf(kB, mB, -0.5f * f0);
+                const float sUL = (-2.0f * sg) * f0;
+                const float sNB = -sg * fm1;
+                const float T = fminf(fminf(sg * xL, fmaxf(fmaxf(0.0f, sNB), sMD)), fmaxf(fmaxf(0.0f, sUL), sLC));
+                xL = sg * T;
+            }
+            {
+                const float sg = sign1(xR);
+                const float sMD = (-0.5f * sg) * (mB - f0);
+                const float sLC = sg * fmaf(kB, mA, 0.5f * fm1);
+                const float sUL = (2.0f * sg) * fm1;
+                const float sNB = sg * f0;
+                const float T = fminf(fminf(sg * xR, fmaxf(fmaxf(0.0f, sNB), sMD)), fmaxf(fmaxf(0.0f, sUL), sLC));
+                xR = sg * T;
+            }
         }
-        const float2 o = __fadd2_rn(make_float2(v0, v0), x);
-        L = o.x;
-        R = o.y;
+        L = v0 + xL;
+        R = v0 + xR;
         return ok;
     }
 };

@@ -24,6 +24,7 @@
 #include "sweep_pipe.cuh"
 #include "sweep_march.cuh"
 #include "sweep_march_tma.cuh"
+#include "vjp_march.cuh"
 #include "weno_adjoint.cuh"
 #include "batched.cuh"
 
@@ -360,12 +361,17 @@ int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsign
     a.accumulate = (acc_flag || folded) ? 1 : 0;
     if (folded && !acc_flag)
         WSB_CUDA(cudaMemsetAsync(gv, 0, sizeof(double) * d.E[0] * d.E[1] * d.E[2] * d.nv, st));
+    const bool uni = ucf != nullptr;
+    if (uni && order == 5 && gr->scheme == WENO_SB_JS && kernel_choice() != 1) {
+        int rc = launch_vjp_march(d.E, a.g, dir, folded, a.mp != 0, a.accumulate != 0, v, ucf, a.wp, gL, gR, gv, st,
+                                  num_sms());
+        if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "vjp march launch") : rc;
+    }
     const int threads = 128;
     long long blocks = (a.g.cols + threads - 1) / threads;
     if (blocks < 1) blocks = 1;
     if (blocks > (1LL << 30)) blocks = 1LL << 30;
     const unsigned grid = (unsigned)blocks;
-    const bool uni = ucf != nullptr;
     switch (order * 2 + (uni ? 1 : 0)) {
         case 6: vjp_kernel<3, false><<<grid, threads, 0, st>>>(a); break;
         case 7: vjp_kernel<3, true><<<grid, threads, 0, st>>>(a); break;
