@@ -94,7 +94,10 @@ __device__ __forceinline__ void batch_item(const BatchEntry& e, long long grp, i
 }
 
 // Persistent kernel: CTAs take items from *counter until n_items.
-__global__ void __launch_bounds__(256, 1)
+#ifndef WSB_BATCH_MIN_BLOCKS
+#define WSB_BATCH_MIN_BLOCKS 2  // 2 CTAs of 256 per SM (128 registers; the WENO7 paths spill a little, still faster)
+#endif
+__global__ void __launch_bounds__(256, WSB_BATCH_MIN_BLOCKS)
     batch_kernel(const BatchEntry* __restrict__ entries, int n_entries, long long n_items,
                  unsigned long long* __restrict__ counter, int U) {
     __shared__ long long s_item;

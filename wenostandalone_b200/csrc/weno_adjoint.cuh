@@ -241,14 +241,14 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (ORDER == 7) {
-                    const double a3 = pow(1.0 + tau / beta[r], 3.0);
+                    const double a3 = ipow3(1.0 + tau / beta[r]);
                     al[r] = a3 * a3;
                 } else {
-                    al[r] = pow(1.0 + tau / beta[r], 6.0);
+                    al[r] = ipow6(1.0 + tau / beta[r]);
                 }
             }
             if (ORDER == 7) {
-                const double a3 = pow(1.0 + tau / eps, 3.0);
+                const double a3 = ipow3(1.0 + tau / eps);
                 a4 = a3 * a3;
             }
             // reference sums in weight order q = 0..
@@ -354,7 +354,8 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
         // alpha(4) = (1 + |eps - beta(3)|/eps)^6 sits in both sums
         const double ga4 = gLw * (0.0 - Lw) / SL4 + gRw * (0.0 - Rw) / SR4;
         const double base = 1.0 + tau4 / eps;
-        const double da4 = 6.0 * pow(base, 5.0) / eps;   // d a4 / d tau
+        const double b2 = base * base;
+        const double da4 = 6.0 * (b2 * b2 * base) / eps;   // d a4 / d tau
         const double sgn = (beta[0] - eps) >= 0.0 ? 1.0 : -1.0;
         gbeta[0] += ga4 * da4 * sgn;
     }

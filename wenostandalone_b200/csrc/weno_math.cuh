@@ -127,6 +127,17 @@ __device__ __forceinline__ double nr_rcp(double s) {
     return fma(r, e, r);
 }
 
+// The TENO weights' powers (f90:580-582: (1 + tau/beta)**6._wp; f90:1492:
+// (alpha**3._wp)**2._wp) as products: x^6 = (x^2)^3, x^3 = x^2 x.  A double
+// pow() with a real exponent goes through a logarithm and an exponential in
+// extended precision (on the order of a hundred instructions); the products
+// round differently by a few ulp, which moves the weights by as much.
+__device__ __forceinline__ double ipow6(double x) {
+    const double x2 = x * x;
+    return x2 * x2 * x2;
+}
+__device__ __forceinline__ double ipow3(double x) { return x * x * x; }
+
 // Mapped-WENO transform (f90:419-423, 557-568).
 __device__ __forceinline__ double mapw(double d, double w) {
     return (d * (1.0 + d - 3.0 * w) + w * w) * (w / (d * d + w * (1.0 - 2.0 * d)));
@@ -257,9 +268,9 @@ __device__ __forceinline__ void weno5_face(const double vm2, const double vm1, c
         a2 = c.dL[2] * (1.0 + (tau / beta2));
     } else if (scheme == TENO) {
         tau = fabs(beta2 - beta0);
-        a0 = pow(1.0 + tau / beta0, 6.0);
-        a1 = pow(1.0 + tau / beta1, 6.0);
-        a2 = pow(1.0 + tau / beta2, 6.0);
+        a0 = ipow6(1.0 + tau / beta0);
+        a1 = ipow6(1.0 + tau / beta1);
+        a2 = ipow6(1.0 + tau / beta2);
         s = a0 + a1 + a2;
         de0 = (a0 / s < teno_ct) ? 0.0 : 1.0;
         de1 = (a1 / s < teno_ct) ? 0.0 : 1.0;
@@ -401,7 +412,7 @@ __device__ __forceinline__ void weno7_face(const double* v /* v[-3..3] */, const
         tau = fabs(beta[4] - beta[3]);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            const double a3 = pow(1.0 + tau / beta[q], 3.0);
+            const double a3 = ipow3(1.0 + tau / beta[q]);
             alpha[q] = a3 * a3;
         }
         s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
