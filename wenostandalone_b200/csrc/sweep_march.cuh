@@ -363,7 +363,6 @@ struct March64 {
     double b1n, b2n, b2nn;      // beta_1(J+1), beta_2(J+1), beta_2(J+2)
     double e2;                  // curvature d[J+1] - d[J]
     double mA, mB;              // minmod(e2[J-1], e2[J]), minmod(e2[J], e2[J+1])
-    double hL, hR;              // (v[J-1] + v[J]) / 2, (v[J] + v[J+1]) / 2
 
     // beta of the three stencils that pair (x, y) = (d[k], d[k+1]) enters
     __device__ __forceinline__ static void betas(const MarchArgs& a, double sx, double cxy, double sy, double& g0,
@@ -390,8 +389,6 @@ struct March64 {
         e2 = dp1 - d0;
         mA = mm64(em, ez);
         mB = mm64(ez, e2);
-        hL = (vm1 + v0) * 0.5;
-        hR = (v0 + vp1) * 0.5;
     }
 
     // Advance to face J+1; n is cell J+3.
@@ -402,14 +399,12 @@ struct March64 {
         betas(a, s1, dp1 * dn, sn, g0, g1, g2);
         const double ne2 = dn - dp1;
         const double nmB = mm64(e2, ne2);
-        const double nhR = (vp1 + vp2) * 0.5;
         vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
         dm2 = dm1; dm1 = d0; d0 = dp1; dp1 = dn;
         s1 = sn;
         b0 = g0; b1 = b1n; b2 = b2n;
         b1n = g1; b2n = b2nn; b2nn = g2;
         e2 = ne2; mA = mB; mB = nmB;
-        hL = hR; hR = nhR;
     }
 
     // WENO5-JS (+ MP) state of face J; false when the one-reciprocal form
@@ -426,8 +421,11 @@ struct March64 {
                      eR2 = fma(a.kR[5], dm2, a.kR[4] * dm1);
         const double EL = fma(P0, eL0, fma(P1, eL1, P2 * eL2));
         const double ER = fma(P0, eR0, fma(P1, eR1, P2 * eR2));
-        const bool ok = mid_range(SL) && mid_range(SR);
-        const double r = rcp1(SL * SR);
+        // one range test on S_L S_R: the two sums share the P_k, so they are
+        // within the ratio of the ideal weights of each other
+        const double p = SL * SR;
+        const bool ok = mid_range_prod(p);
+        const double r = rcp1(p);
         L = fma(EL * SR, r, v0);
         R = fma(ER * SL, r, v0);
         if constexpr (MPF) {
@@ -439,7 +437,7 @@ struct March64 {
             {
                 const bool pos = sign_clear(EL);
                 const double UL = fma(-2.0, d0, v0);
-                const double MD = fma(-0.5, mA, hL);
+                const double MD = fma(-0.5, dm1 + mA, v0);   // ((v0 + vm1) - mA) / 2
                 const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
                 const double P1 = (pos == up_l) ? v0 : vm1;  // max / min of (v0, vm1)
                 const double P2 = (pos == up_r) ? v0 : UL;   // max / min of (v0, UL)
@@ -449,7 +447,7 @@ struct March64 {
             {
                 const bool pos = sign_clear(ER);
                 const double UL = fma(2.0, dm1, v0);
-                const double MD = fma(-0.5, mB, hR);
+                const double MD = fma(0.5, d0 - mB, v0);     // ((v0 + vp1) - mB) / 2
                 const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
                 const double P1 = (pos == up_r) ? vp1 : v0;  // max / min of (v0, vp1)
                 const double P2 = (pos == up_l) ? UL : v0;   // max / min of (v0, UL)

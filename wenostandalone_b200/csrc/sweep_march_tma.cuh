@@ -111,8 +111,11 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col,
     march32_redo<MPF>(a, col, o, L, R);
 }
 
+#ifndef WSB_MTMA_MIN_BLOCKS_F32
+#define WSB_MTMA_MIN_BLOCKS_F32 3
+#endif
 template <bool MPF, int KIND, typename T, int LDR>
-__global__ void __launch_bounds__(kTmaWarps * 32, WSB_MTMA_MIN_BLOCKS)
+__global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32)
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
                            const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
                            const MarchTmaArgs t) {
@@ -251,13 +254,45 @@ __global__ void __launch_bounds__(kTmaWarps * 32, WSB_MTMA_MIN_BLOCKS)
                 __syncwarp();
             }
             unsigned bad = 0;
+            // face states leave as 16-byte groups (G faces) of the lane's
+            // row; row-tile cells arrive as 16-byte groups too (the swizzle
+            // moves whole 16-byte chunks), column-tile cells one by one
+            constexpr int G = 16 / (int)sizeof(T);
+            T Lg[G], Rg[G], cg[G];
 #pragma unroll
             for (int i = 0; i < F; ++i) {
+                const int q = 6 + i;                      // position of the pushed cell, tiles c / c+1
+                const unsigned kq = q < 8 ? kc : kc + 1;
+                const int pq = q & 7;
+                if constexpr (KIND == 0) {
+                    if (i == 0 || pq % G == 0) {
+                        const int p0 = pq - pq % G;
+                        const unsigned char* src = tile_ptr(kq) + swz<T>((unsigned)lane, (unsigned)p0);
+                        if constexpr (sizeof(T) == 8) {
+                            const double2 v2 = *(const double2*)src;
+                            cg[0] = v2.x; cg[1] = v2.y;
+                        } else {
+                            const float4 v4 = *(const float4*)src;
+                            cg[0] = v4.x; cg[1] = v4.y; cg[2] = v4.z; cg[3] = v4.w;
+                        }
+                    }
+                }
                 T L, R;
                 if (!w.template face<MPF>(a, L, R)) bad |= 1u << i;
-                *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
-                *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
-                w.push(a, (i < 2) ? cell(kc, 6 + i) : cell(kc + 1, i - 2));
+                Lg[i % G] = L;
+                Rg[i % G] = R;
+                if (i % G == G - 1) {
+                    unsigned char* dL = ob + swz<T>((unsigned)lane, (unsigned)(i - G + 1));
+                    if constexpr (sizeof(T) == 8) {
+                        *(double2*)dL = make_double2(Lg[0], Lg[1]);
+                        *(double2*)(dL + OB) = make_double2(Rg[0], Rg[1]);
+                    } else {
+                        *(float4*)dL = make_float4(Lg[0], Lg[1], Lg[2], Lg[3]);
+                        *(float4*)(dL + OB) = make_float4(Rg[0], Rg[1], Rg[2], Rg[3]);
+                    }
+                }
+                if constexpr (KIND == 0) w.push(a, cg[pq % G]);
+                else w.push(a, cell(kq, pq));
             }
             const int nF = f_end - f0 < F ? f_end - f0 : F;
             bad &= (1u << nF) - 1u;
@@ -390,7 +425,10 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     // segments over faces [4, ns-3), a multiple of 8 faces each
     const long long nf4 = g.ns - 7;
     const long long cols = (long long)a.n_ut * a.Nw * a.NV;
-    const long long want = (long long)sms * kTmaWarps * 3 * 2;
+#ifndef WSB_MTMA_ITEMS_PER_WARP
+#define WSB_MTMA_ITEMS_PER_WARP 8  // target work items per resident warp (200^3: two segments per column)
+#endif
+    const long long want = (long long)sms * kTmaWarps * 3 * WSB_MTMA_ITEMS_PER_WARP;
     long long nseg = (want + cols - 1) / cols;
     const long long max_seg = (nf4 + kTmaF - 1) / kTmaF;
     if (nseg > max_seg) nseg = max_seg;

@@ -155,14 +155,14 @@ struct MarchVjp {
             {
                 const bool pos = sign_clear(xL);
                 const double UL = fma(-2.0, w.d0, v0);
-                const double MD = fma(-0.5, w.mA, w.hL);
+                const double MD = fma(-0.5, w.dm1 + w.mA, v0);
                 const double LC = fma(kBetaMP, w.mB, fma(-0.5, w.d0, v0));
                 mp_pick(v0 + xL, v0, w.vm1, UL, MD, LC, pos, pos != up_l, pos != up_r, cl);
             }
             {
                 const bool pos = sign_clear(xR);
                 const double UL = fma(2.0, w.dm1, v0);
-                const double MD = fma(-0.5, w.mB, w.hR);
+                const double MD = fma(0.5, w.d0 - w.mB, v0);
                 const double LC = fma(kBetaMP, w.mA, fma(0.5, w.dm1, v0));
                 mp_pick(v0 + xR, v0, w.vp1, UL, MD, LC, pos, pos == up_r, pos == up_l, cr);
             }

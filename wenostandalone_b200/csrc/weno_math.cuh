@@ -113,6 +113,14 @@ __device__ __forceinline__ bool mid_range(double s) {
     return (hi - (525u << 20)) < (996u << 20);
 }
 
+// True when p is positive with 2^-996 <= p < 2^996: the product of two
+// normalisation sums whose reciprocal and whose products with either sum
+// stay normal.
+__device__ __forceinline__ bool mid_range_prod(double p) {
+    const unsigned hi = (unsigned)__double2hiint(p);
+    return (hi - (27u << 20)) < (1992u << 20);
+}
+
 // Reciprocal of a normal positive double by Newton-Raphson refinement of the
 // hardware seed (PTX rcp.approx.ftz.f64): r <- r + r (1 - s r), twice.  Each
 // step squares the relative error, so any seed better than 2^-14 ends below
