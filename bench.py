@@ -304,10 +304,13 @@ def run_ours(args):
         drop = None
 
     # end-to-end through the handle API with pinned host buffers
-    e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev) if not (args.no_extras or fp32_main) else None
+    e2e = e2e_full = None
+    if not (args.no_extras or fp32_main):
+        e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev)
+        e2e_full = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev, full_download=True)
 
     # the other workloads of the path (adjoint, batched blocks, mixed precision)
-    adjoint = batched = mixed = None
+    adjoint = batched = mixed = families = None
     if not args.no_extras and rank == 0 and not fp32_main:
         Kx = max(3, min(K, 10))
         adjoint = measure_adjoint(dev, Kx)
@@ -315,6 +318,8 @@ def run_ours(args):
         batched = measure_batched(dev, Kx)
         torch.cuda.empty_cache()
         mixed = measure_mixed_precision(dev, Kx)
+        torch.cuda.empty_cache()
+        families = measure_families(g, v, stream, Kx, dev)
         torch.cuda.empty_cache()
 
     cpu = None
@@ -356,12 +361,16 @@ def run_ours(args):
             line["drop_in"] = drop
         if e2e:
             line["e2e"] = e2e
+        if e2e_full:
+            line["e2e_full_face_states"] = e2e_full
         if adjoint:
             line["adjoint"] = adjoint
         if batched:
             line["batched"] = batched
         if mixed:
             line["mixed_precision"] = mixed
+        if families:
+            line["families_200cubed"] = families
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "face-states/s", "cores": cpu["cores"],
                                     "kind": "port", "sample": cpu["sample"]}
@@ -466,10 +475,14 @@ def measure_drop_in(g, v, faces, outs, stream, K, dev):
     return res
 
 
-def measure_e2e(g, vf_host, coefs, K, dev):
-    """End to end through the C-ABI handle API (what a Fortran caller does):
-    upload v_vf from pinned host memory, x/y/z folded WENO5 + MP, download all
-    six face-state arrays into pinned host memory; wall clock around it."""
+def measure_e2e(g, vf_host, coefs, K, dev, full_download=False):
+    """End to end through the C-ABI handle API (what a Fortran caller of the
+    harness does): upload v_vf from pinned host memory, x/y/z folded WENO5 +
+    MP, then read the step's result back to the host -- the harness's result
+    is its checksum lines (f_checksum of each face-state array, f90:1617-1620,
+    1836-1844), so by default the six checksums, summed on the device; with
+    full_download the six face-state arrays themselves (3.66 GB) into pinned
+    host memory.  Wall clock around each step."""
     import ctypes
 
     import torch
@@ -484,7 +497,8 @@ def measure_e2e(g, vf_host, coefs, K, dev):
                                                      (5, g.nc(d)), (g.nc(d), 5, 6)])])
         src = torch.from_numpy(vf_host.ravel(order="F")).pin_memory()
         nface = int(np.prod(g.face_shape(0)))
-        dst = [torch.empty(nface, dtype=torch.float64).pin_memory() for _ in range(6)]
+        dst = [torch.empty(nface, dtype=torch.float64).pin_memory() for _ in range(6)] if full_download else []
+        sums = (ctypes.c_double * 6)()
         lib = L.lib()
 
         def step():
@@ -492,8 +506,12 @@ def measure_e2e(g, vf_host, coefs, K, dev):
             for d in range(3):
                 L.check(lib.weno_sb_weno(h.handle, d, 5, wsb.F_MP | wsb.F_FOLDED))
             for d in range(3):
-                L.check(lib.weno_sb_download(h.handle, L.A_VL(d), dst[2 * d].data_ptr()))
-                L.check(lib.weno_sb_download(h.handle, L.A_VR(d), dst[2 * d + 1].data_ptr()))
+                if full_download:
+                    L.check(lib.weno_sb_download(h.handle, L.A_VL(d), dst[2 * d].data_ptr()))
+                    L.check(lib.weno_sb_download(h.handle, L.A_VR(d), dst[2 * d + 1].data_ptr()))
+                else:
+                    L.check(lib.weno_sb_checksum(h.handle, L.A_VL(d), ctypes.byref(sums, 16 * d)))
+                    L.check(lib.weno_sb_checksum(h.handle, L.A_VR(d), ctypes.byref(sums, 16 * d + 8)))
 
         step()
         t0 = time.perf_counter()
@@ -503,9 +521,13 @@ def measure_e2e(g, vf_host, coefs, K, dev):
     finally:
         h.close()
     fs = 3 * face_states_per_dir()
-    return {"value": fs / dt, "unit": "face-states/s", "h2d_bytes_per_step": int(vf_host.nbytes),
-            "d2h_bytes_per_step": int(6 * nface * 8), "ms_per_step": dt * 1e3, "steps": K,
-            "path": "weno_sb_upload -> weno_sb_weno x3 (folded, MP) -> weno_sb_download x6, pinned host buffers"}
+    out = {"value": fs / dt, "unit": "face-states/s", "h2d_bytes_per_step": int(vf_host.nbytes),
+           "d2h_bytes_per_step": int(6 * nface * 8) if full_download else 6 * 8, "ms_per_step": dt * 1e3,
+           "steps": K}
+    out["path"] = ("weno_sb_upload -> weno_sb_weno x3 (folded, MP) -> " +
+                   ("weno_sb_download x6 (all face states), pinned host buffers" if full_download else
+                    "weno_sb_checksum x6 (the harness's result: f_checksum of every face-state array)"))
+    return out
 
 
 def _time_steps(step, stream, K, warm=3):
@@ -627,6 +649,54 @@ def measure_batched(dev, K):
                                          "launches_per_step": len(entries)}
         res[dt_name] = r
         del entries
+    return res
+
+
+def measure_families(g, v, stream, K, dev):
+    """Every kernel family of the path at 200^3 x 8 (FP64, x/y/z each):
+    reshape (s_initialize_weno), order-1 copy, WENO3 / WENO5 / WENO7 with
+    JS weights and MP fused, the standalone MP limiter, and WENO5 with TENO
+    weights (teno_CT 1e-5); the harness's per-face coefficient arrays
+    (face-dependent, as s_fill_coefficients makes them) for WENO5, true
+    uniform-grid coefficients for the rest.  ms per three sweeps."""
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api, fields
+    sp = int(stream.cuda_stream)
+    nface = int(np.prod(g.face_shape(0)))
+    L = torch.empty(nface, dtype=torch.float64, device=dev)
+    R = torch.empty(nface, dtype=torch.float64, device=dev)
+    rs = [torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float64, device=dev) for d in range(3)]
+    for d in range(3):
+        api.reshape(g, d, v, rs[d], stream=sp)
+    gt = wsb.Grid(M, M, M, NV, BUFF, scheme=wsb.TENO)
+    res = {}
+
+    def coefs(order, d, harness=False):
+        c = (fields.harness_coefficients(g.nc(d), (0.03, 0.05, 0.07)[d]) if harness
+             else fields.uniform_weno_coefficients(order, g.nc(d)))
+        return tuple(torch.from_numpy(np.ascontiguousarray(x.ravel(order="F"))).to(dev) for x in c)
+
+    def timed(name, fn):
+        res[name] = {"ms_per_step": _time_steps(fn, stream, K)}
+        res[name]["value"] = 3 * face_states_per_dir() / (res[name]["ms_per_step"] * 1e-3)
+
+    timed("reshape", lambda: [api.reshape(g, d, v, rs[d], stream=sp) for d in range(3)])
+    timed("order1_copy", lambda: [api.order1_copy(g, d, v, L, R, stream=sp) for d in range(3)])
+    for order in (3, 5, 7):
+        cf = [coefs(order, d) for d in range(3)]
+        timed(f"weno{order}_js_mp", lambda cf=cf, order=order: [
+            api.weno(g, d, order, v, cf[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
+    hc = [coefs(5, d, harness=True) for d in range(3)]
+    timed("weno5_js_mp_harness_coefficients", lambda: [
+        api.weno(g, d, 5, v, hc[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
+    timed("mp_standalone", lambda: [api.preserve_monotonicity(g, d, rs[d], L, R, stream=sp) for d in range(3)])
+    cf5 = [coefs(5, d) for d in range(3)]
+    timed("weno5_teno_mp", lambda: [
+        api.weno(gt, d, 5, v, cf5[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
+    res["note"] = ("value = face-states/s of the WENO5 face count (3 x 148,135,424) for every family, so "
+                   "the rows compare as times; WENO3 writes all ns faces")
     return res
 
 
