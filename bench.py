@@ -498,7 +498,7 @@ def measure_e2e(g, vf_host, coefs, K, dev, full_download=False):
         src = torch.from_numpy(vf_host.ravel(order="F")).pin_memory()
         nface = int(np.prod(g.face_shape(0)))
         dst = [torch.empty(nface, dtype=torch.float64).pin_memory() for _ in range(6)] if full_download else []
-        sums = (ctypes.c_double * 6)()
+        sums = [ctypes.c_double() for _ in range(6)]
         lib = L.lib()
 
         def step():
@@ -510,8 +510,8 @@ def measure_e2e(g, vf_host, coefs, K, dev, full_download=False):
                     L.check(lib.weno_sb_download(h.handle, L.A_VL(d), dst[2 * d].data_ptr()))
                     L.check(lib.weno_sb_download(h.handle, L.A_VR(d), dst[2 * d + 1].data_ptr()))
                 else:
-                    L.check(lib.weno_sb_checksum(h.handle, L.A_VL(d), ctypes.byref(sums, 16 * d)))
-                    L.check(lib.weno_sb_checksum(h.handle, L.A_VR(d), ctypes.byref(sums, 16 * d + 8)))
+                    L.check(lib.weno_sb_checksum(h.handle, L.A_VL(d), ctypes.byref(sums[2 * d])))
+                    L.check(lib.weno_sb_checksum(h.handle, L.A_VR(d), ctypes.byref(sums[2 * d + 1])))
 
         step()
         t0 = time.perf_counter()
