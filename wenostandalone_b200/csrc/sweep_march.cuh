@@ -55,7 +55,89 @@ struct MarchArgs {
     double kL[6], kR[6];
     // FP32-bulk engine: (polyL, polyR) float pairs, Coef<5>::pL index order
     float2 pf2[6];
+    // face-dependent coefficients (FP64 kernels): the per-face table built by
+    // march_face_table_kernel, and the arrays it was built from (for faces
+    // that are redone); ftab is null for face-independent coefficients
+    const double* ftab;
+    CoefPtrs cp;
 };
+
+// Row of the per-face table (doubles per face; 224 bytes, a multiple of 16).
+constexpr int kFaceRow = 28;
+
+// Coefficient sources of the FP64 marching engine.  ParamCoefs reads the
+// face-independent coefficients from the kernel-parameter bank; FaceRow and
+// BetaRow hold one face's row of the per-face table (FaceRow: the candidate
+// coefficients and ideal weights of face f; BetaRow: the beta coefficients
+// that the difference pair (d[f], d[f+1]) enters, b(f + r, r, s) at 3r + s).
+struct ParamCoefs {
+    const MarchArgs& a;
+    __device__ __forceinline__ double kL(int q) const { return a.kL[q]; }
+    __device__ __forceinline__ double kR(int q) const { return a.kR[q]; }
+    __device__ __forceinline__ double dL(int r) const { return a.ucf[12 + r]; }
+    __device__ __forceinline__ double dR(int r) const { return a.ucf[15 + r]; }
+    __device__ __forceinline__ double b(int q) const { return a.ucf[18 + q]; }
+};
+
+// (rows are read from the per-face table in global memory or from a copy
+// staged in shared memory)
+struct FaceRow {
+    double2 k[9];  // kL[0..5], kR[0..5], dL[0..2], dR[0..2]
+    __device__ __forceinline__ explicit FaceRow(const double* row) {
+        const double2* p = reinterpret_cast<const double2*>(row);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) k[q] = p[q];
+    }
+    __device__ __forceinline__ double g(int q) const { return (q & 1) ? k[q >> 1].y : k[q >> 1].x; }
+    __device__ __forceinline__ double kL(int q) const { return g(q); }
+    __device__ __forceinline__ double kR(int q) const { return g(6 + q); }
+    __device__ __forceinline__ double dL(int r) const { return g(12 + r); }
+    __device__ __forceinline__ double dR(int r) const { return g(15 + r); }
+};
+
+struct BetaRow {
+    double2 k[5];  // b[0..8] (row entries 18 .. 26) and the pad at 27
+    __device__ __forceinline__ explicit BetaRow(const double* row) {
+        const double2* p = reinterpret_cast<const double2*>(row) + 9;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) k[q] = p[q];
+    }
+    __device__ __forceinline__ double b(int q) const { return (q & 1) ? k[q >> 1].y : k[q >> 1].x; }
+};
+
+// Builds the per-face table: row f (f = 0 .. rows-1, face f of the sweep)
+// from core face c(f) = clamp(f - 3, 0, nc - 1) of the coefficient arrays
+// (f90:541-550, 552-555, 623-625 read polyL/R(j, r, s), d(r, j) and
+// beta_coef(j, r, s) at the core index of the face):
+//   [0..5]    kL[2r+s] = dL(r) polyL(c, r, s) (the ideal weight folded in)
+//   [6..11]   kR[2r+s] = dR(r) polyR(c, r, s)
+//   [12..14]  dL(r), [15..17] dR(r)
+//   [18+3r+s] beta_coef(c(f + r), r, s); [27] zero
+// A face with a negative ideal weight gets a NaN in dL(0): its normalisation
+// test fails and the kernels redo it from the arrays, as the one-sided MP
+// median needs sign(v_L - v_0) = sign(E_L), which non-negative weights give.
+__global__ void march_face_table_kernel(CoefPtrs cp, long long nc, int rows, double* __restrict__ tab) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= rows) return;
+    auto core = [&](long long x) { x -= 3; return x < 0 ? 0 : (x > nc - 1 ? nc - 1 : x); };
+    const long long c = core(f);
+    double* row = tab + (long long)f * kFaceRow;
+    bool neg = false;
+    for (int r = 0; r < 3; ++r) {
+        const double dl = cp.dL[r + 5 * c], dr = cp.dR[r + 5 * c];
+        neg |= !(dl >= 0.0) || !(dr >= 0.0);
+        for (int s = 0; s < 2; ++s) {
+            row[2 * r + s] = dl * cp.polyL[c + nc * (r + 5 * s)];
+            row[6 + 2 * r + s] = dr * cp.polyR[c + nc * (r + 5 * s)];
+        }
+        row[12 + r] = dl;
+        row[15 + r] = dr;
+        const long long cr = core(f + r);
+        for (int s = 0; s < 3; ++s) row[18 + 3 * r + s] = cp.beta[cr + nc * (r + 5 * s)];
+    }
+    if (neg) row[12] = __longlong_as_double(0x7ff8000000000000LL);
+    row[27] = 0.0;
+}
 
 // Second-order minmod of the MP limiter (same decisions as mp_minmod /
 // mp_minmod_f), for the storage type.
@@ -364,26 +446,35 @@ struct March64 {
     double e2;                  // curvature d[J+1] - d[J]
     double mA, mB;              // minmod(e2[J-1], e2[J]), minmod(e2[J], e2[J+1])
 
-    // beta of the three stencils that pair (x, y) = (d[k], d[k+1]) enters
+    // beta of the three stencils that pair (x, y) = (d[k], d[k+1]) enters:
+    // stencil 0 of face k, 1 of face k+1, 2 of face k+2 (coefficients of
+    // those faces from the source c)
+    template <class C>
+    __device__ __forceinline__ static void betas(const MarchArgs& a, const C& c, double sx, double cxy, double sy,
+                                                 double& g0, double& g1, double& g2) {
+        const double eps = a.wp.eps;
+        g0 = fma(c.b(0), sy, fma(c.b(1), cxy, fma(c.b(2), sx, eps)));
+        g1 = fma(c.b(3), sy, fma(c.b(4), cxy, fma(c.b(5), sx, eps)));
+        g2 = fma(c.b(6), sy, fma(c.b(7), cxy, fma(c.b(8), sx, eps)));
+    }
     __device__ __forceinline__ static void betas(const MarchArgs& a, double sx, double cxy, double sy, double& g0,
                                                  double& g1, double& g2) {
-        const double eps = a.wp.eps;
-        g0 = fma(a.ucf[18], sy, fma(a.ucf[19], cxy, fma(a.ucf[20], sx, eps)));
-        g1 = fma(a.ucf[21], sy, fma(a.ucf[22], cxy, fma(a.ucf[23], sx, eps)));
-        g2 = fma(a.ucf[24], sy, fma(a.ucf[25], cxy, fma(a.ucf[26], sx, eps)));
+        betas(a, ParamCoefs{a}, sx, cxy, sy, g0, g1, g2);
     }
 
-    // Window of face J from cells J-2 .. J+2.
-    __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3,
-                                         double c4) {
+    // Window of face J from cells J-2 .. J+2; cm2, cm1, cz are the beta
+    // sources of the pairs starting at d[J-2], d[J-1], d[J].
+    template <class C2, class C1, class C0>
+    __device__ __forceinline__ void init(const MarchArgs& a, const C2& cm2, const C1& cm1, const C0& cz, double c0,
+                                         double c1, double c2, double c3, double c4) {
         vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
         dm2 = c1 - c0; dm1 = c2 - c1; d0 = c3 - c2; dp1 = c4 - c3;
         const double sm2 = dm2 * dm2, sm1 = dm1 * dm1, s0 = d0 * d0;
         s1 = dp1 * dp1;
         double g0, g1, g2, u;
-        betas(a, sm2, dm2 * dm1, sm1, u, u, b2);      // pair (d[J-2], d[J-1])
-        betas(a, sm1, dm1 * d0, s0, u, b1, b2n);      // pair (d[J-1], d[J])
-        betas(a, s0, d0 * dp1, s1, g0, g1, g2);       // pair (d[J], d[J+1])
+        betas(a, cm2, sm2, dm2 * dm1, sm1, u, u, b2);      // pair (d[J-2], d[J-1])
+        betas(a, cm1, sm1, dm1 * d0, s0, u, b1, b2n);      // pair (d[J-1], d[J])
+        betas(a, cz, s0, d0 * dp1, s1, g0, g1, g2);        // pair (d[J], d[J+1])
         b0 = g0; b1n = g1; b2nn = g2;
         const double em = dm1 - dm2, ez = d0 - dm1;
         e2 = dp1 - d0;
@@ -391,12 +482,20 @@ struct March64 {
         mB = mm64(ez, e2);
     }
 
-    // Advance to face J+1; n is cell J+3.
-    __device__ __forceinline__ void push(const MarchArgs& a, double n) {
+    __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3,
+                                         double c4) {
+        const ParamCoefs u{a};
+        init(a, u, u, u, c0, c1, c2, c3, c4);
+    }
+
+    // Advance to face J+1; n is cell J+3; c is the beta source of the new
+    // pair (d[J+1], d[J+2]).
+    template <class C>
+    __device__ __forceinline__ void push(const MarchArgs& a, const C& c, double n) {
         const double dn = n - vp2;
         const double sn = dn * dn;
         double g0, g1, g2;
-        betas(a, s1, dp1 * dn, sn, g0, g1, g2);
+        betas(a, c, s1, dp1 * dn, sn, g0, g1, g2);
         const double ne2 = dn - dp1;
         const double nmB = mm64(e2, ne2);
         vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
@@ -406,19 +505,24 @@ struct March64 {
         b1n = g1; b2n = b2nn; b2nn = g2;
         e2 = ne2; mA = mB; mB = nmB;
     }
+    __device__ __forceinline__ void push(const MarchArgs& a, double n) { push(a, ParamCoefs{a}, n); }
 
     // WENO5-JS (+ MP) state of face J; false when the one-reciprocal form
     // is out of range (the caller redoes the face).
     template <bool MPF>
     __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+        return face<MPF, ParamCoefs>(a, ParamCoefs{a}, L, R);
+    }
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool face(const MarchArgs& a, const C& c, double& L, double& R) const {
         const double q0 = b0 * b0, q1 = b1 * b1, q2 = b2 * b2;
         const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
-        const double SL = fma(a.ucf[12], P0, fma(a.ucf[13], P1, a.ucf[14] * P2));
-        const double SR = fma(a.ucf[15], P0, fma(a.ucf[16], P1, a.ucf[17] * P2));
-        const double eL0 = fma(a.kL[1], d0, a.kL[0] * dp1), eL1 = fma(a.kL[3], dm1, a.kL[2] * d0),
-                     eL2 = fma(a.kL[5], dm2, a.kL[4] * dm1);
-        const double eR0 = fma(a.kR[1], d0, a.kR[0] * dp1), eR1 = fma(a.kR[3], dm1, a.kR[2] * d0),
-                     eR2 = fma(a.kR[5], dm2, a.kR[4] * dm1);
+        const double SL = fma(c.dL(0), P0, fma(c.dL(1), P1, c.dL(2) * P2));
+        const double SR = fma(c.dR(0), P0, fma(c.dR(1), P1, c.dR(2) * P2));
+        const double eL0 = fma(c.kL(1), d0, c.kL(0) * dp1), eL1 = fma(c.kL(3), dm1, c.kL(2) * d0),
+                     eL2 = fma(c.kL(5), dm2, c.kL(4) * dm1);
+        const double eR0 = fma(c.kR(1), d0, c.kR(0) * dp1), eR1 = fma(c.kR(3), dm1, c.kR(2) * d0),
+                     eR2 = fma(c.kR(5), dm2, c.kR(4) * dm1);
         const double EL = fma(P0, eL0, fma(P1, eL1, P2 * eL2));
         const double ER = fma(P0, eR0, fma(P1, eR1, P2 * eR2));
         // one range test on S_L S_R: the two sums share the P_k, so they are
@@ -476,6 +580,21 @@ __device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __re
     }
 #pragma unroll
     for (int q = 0; q < 9; ++q) c.b[q] = a.ucf[18 + q];
+    const double* p = col + (o + 1) * a.sJ;
+    const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
+                 vp2 = __ldg(p + 4 * a.sJ);
+    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, JS, a.wp.eps, 0.0, L, R);
+    if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
+}
+
+// The same for face-dependent coefficients: core face o - 3 of the arrays.
+template <bool MPF>
+__device__ __noinline__ void march64_redo_faces(const MarchArgs& a, const double* __restrict__ col, long long o,
+                                                double& L, double& R) {
+    Coef<5> c;
+    long long ci = o - 3;
+    ci = ci < 0 ? 0 : (ci > a.nc - 1 ? a.nc - 1 : ci);
+    c.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, ci);
     const double* p = col + (o + 1) * a.sJ;
     const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
                  vp2 = __ldg(p + 4 * a.sJ);
@@ -751,6 +870,7 @@ inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, v
     a.oV = g.ns * g.c1 * g.c2;
     a.NV = (int)g.nv;
     a.n_ut = (a.Nu + 31) / 32;
+    if (!ucf) return a;  // face-dependent coefficients: the caller sets ftab and cp
     for (int q = 0; q < 56; ++q) a.ucf[q] = ucf[q];
     for (int q = 0; q < 6; ++q) {
         a.ucf32[q] = (float)ucf[q];          // polyL (Coef<5>::pL)

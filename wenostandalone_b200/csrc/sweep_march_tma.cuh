@@ -55,6 +55,21 @@ namespace wsb {
 constexpr int kTmaF = 8;        // faces per chunk = cells per input tile
 constexpr int kTmaStages = WSB_MTMA_STAGES;
 constexpr int kTmaOut = WSB_MTMA_OUTBUF;
+// Face-dependent coefficients: each input stage also holds the chunk's
+// kTmaF + 1 rows of the per-face table (one bulk copy on the tile's
+// mbarrier), so the kernels run fewer stages and output buffers to keep
+// three CTAs per SM.
+#ifndef WSB_MTMA_PF_STAGES
+#define WSB_MTMA_PF_STAGES 3
+#endif
+#ifndef WSB_MTMA_PF_OUTBUF
+#define WSB_MTMA_PF_OUTBUF 1
+#endif
+constexpr int kPfStages = WSB_MTMA_PF_STAGES;
+constexpr int kPfOut = WSB_MTMA_PF_OUTBUF;
+constexpr int kPfRowBytes = (kTmaF + 1) * kFaceRow * 8;  // rows f0 .. f0 + 8 of a chunk
+static_assert(kPfRowBytes % 16 == 0, "bulk copies move 16-byte multiples");
+static_assert(WSB_MTMA_PF_STAGES <= 4 && WSB_MTMA_PF_STAGES >= 2, "stages of the per-face kernels");
 #ifndef WSB_MTMA_WARPS
 #define WSB_MTMA_WARPS 4        // warps per CTA (each with its own pipeline)
 #endif
@@ -69,6 +84,7 @@ struct MarchTmaArgs {
     int stage_bytes;   // one input tile (KIND 0: 2048, KIND 1: 8 rows x 34 cells)
     int warp_bytes;    // shared memory per warp, a multiple of 1024
     int ring_off;      // byte offset of the input ring within a warp's area
+    int rows_off;      // face-dependent coefficients: byte offset of the table-row ring
     unsigned box_bytes;
 };
 
@@ -77,6 +93,14 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void*
         "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];\n" ::"l"(map),
         "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
+}
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple
+// of 16), completed on the mbarrier like a tensor tile.
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
@@ -102,24 +126,28 @@ template <typename T> struct MarchEngine;
 template <> struct MarchEngine<double> { using type = March64; };
 template <> struct MarchEngine<float> { using type = March32; };
 
-template <bool MPF>
+template <bool MPF, bool PF>
 __device__ __forceinline__ void march_redo(const MarchArgs& a, const double* col, long long o, double& L, double& R) {
-    march64_redo<MPF>(a, col, o, L, R);
+    if constexpr (PF) march64_redo_faces<MPF>(a, col, o, L, R);
+    else march64_redo<MPF>(a, col, o, L, R);
 }
-template <bool MPF>
+template <bool MPF, bool PF>
 __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col, long long o, float& L, float& R) {
+    static_assert(!PF, "face-dependent coefficients: FP64 kernels only");
     march32_redo<MPF>(a, col, o, L, R);
 }
 
 #ifndef WSB_MTMA_MIN_BLOCKS_F32
 #define WSB_MTMA_MIN_BLOCKS_F32 3
 #endif
-template <bool MPF, int KIND, typename T, int LDR>
+// PF: face-dependent coefficients from the per-face table a.ftab (FP64).
+template <bool MPF, int KIND, typename T, int LDR, bool PF>
 __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32)
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
                            const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
                            const MarchTmaArgs t) {
-    constexpr int F = kTmaF, S = kTmaStages;
+    constexpr int F = kTmaF, S = PF ? kPfStages : kTmaStages;
+    constexpr int NOUT = PF ? kPfOut : kTmaOut;             // output tiles per warp
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
@@ -127,7 +155,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
     extern __shared__ __align__(1024) unsigned char smem_mt[];
     unsigned char* base = smem_mt + ((1024u - (smem_u32(smem_mt) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // per warp: kTmaOut output buffers x (vL, vR), then S input tiles
+    // per warp: NOUT output buffers x (vL, vR), then S input tiles (and, PF,
+    // S chunks of table rows)
     const int warp_bytes = t.warp_bytes;
     unsigned char* wbase = base + (size_t)warp * warp_bytes;
     unsigned char* obuf = wbase;
@@ -148,6 +177,12 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
     bool failed = false;
 
     auto tile_ptr = [&](unsigned k) { return ring + (size_t)(k % S) * t.stage_bytes; };
+    // per-face table rows (PF): in global memory, and the chunk's rows
+    // staged with input tile k
+    auto row = [&](int f) { return a.ftab + (long long)f * kFaceRow; };
+    auto srow = [&](unsigned k, int i) {
+        return (const double*)(wbase + t.rows_off + (size_t)(k % S) * kPfRowBytes) + i * kFaceRow;
+    };
     // byte offset in a tile of position p (0..7) of this lane's column
     auto cell_off = [&](int p) -> unsigned {
         if constexpr (KIND == 0) return swz<T>((unsigned)lane, (unsigned)p);
@@ -166,8 +201,10 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
                 const int c0 = t.dimJ == 0 ? J0 : (t.dimU == 0 ? cU : cW);
                 const int c1 = t.dimJ == 1 ? J0 : (t.dimU == 1 ? cU : cW);
                 const int c2 = t.dimJ == 2 ? J0 : (t.dimU == 2 ? cU : cW);
-                mbar_arrive_expect_tx(bar, t.box_bytes);
+                mbar_arrive_expect_tx(bar, t.box_bytes + (PF ? (unsigned)kPfRowBytes : 0u));
                 tma_load_4d(tile_ptr(k), &tin, bar, c0, c1, c2, v);
+                // rows J0 .. J0 + 8: the faces of the chunk starting at face J0
+                if constexpr (PF) bulk_load_1d((void*)srow(k, 0), row(J0), kPfRowBytes, bar);
             }
         } else {
             // each lane copies its own column's cells; cells past the end of
@@ -226,17 +263,30 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
         Engine w;
         if (sg == 0) {
             // face 3 (cells 4..8 = tile positions 0..4), plain stores
-            w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
             T L, R;
-            if (!w.template face<MPF>(a, L, R)) march_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
+            bool ok;
+            if constexpr (PF) {
+                w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
+                       cell(k0, 3), cell(k0, 4));
+                ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
+            } else {
+                w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
+                ok = w.template face<MPF>(a, L, R);
+            }
+            if (!ok) march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
             if (u0 + lane < a.Nu) {
                 const long long oi = 3 + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
                 outL[oi] = L;
                 outR[oi] = R;
             }
-            w.push(a, cell(k0, 5));
+            if constexpr (PF) w.push(a, BetaRow(row(4)), cell(k0, 5));
+            else w.push(a, cell(k0, 5));
         } else {
-            w.init(a, cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
+            if constexpr (PF)
+                w.init(a, BetaRow(row(f_start - 2)), BetaRow(row(f_start - 1)), BetaRow(row(f_start)), cell(k0, 1),
+                       cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
+            else
+                w.init(a, cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
         }
         // chunk c: faces f0 .. f0+7 (f0 = f_start + 8c), pushes cells
         // f0+6 .. f0+13 = positions 6, 7 of tile c and 0 .. 5 of tile c+1
@@ -244,13 +294,14 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
             const unsigned kc = k0 + c;
             if (!wait_tile(kc + 1)) { failed = true; break; }
             const int f0 = f_start + F * c;
-            unsigned char* ob = obuf + (size_t)(n_chunks % kTmaOut) * (2 * OB);
-            if (n_chunks >= (unsigned)kTmaOut) {
-                // the store issued from this buffer kTmaOut chunks ago has read it
-                if (lane == 0) {
-                    if constexpr (kTmaOut == 1) bulk_wait_read0();
-                    else bulk_wait_read1();
-                }
+            unsigned char* ob = obuf + (size_t)(n_chunks % NOUT) * (2 * OB);
+            // the store issued from this buffer NOUT chunks ago must have read
+            // it before the chunk's face states are written: waited here, or
+            // (one output buffer) just before the first write, so the first
+            // faces' arithmetic overlaps the store
+            const bool wait_out = n_chunks >= (unsigned)NOUT;
+            if (NOUT > 1 && wait_out) {
+                if (lane == 0) bulk_wait_read1();
                 __syncwarp();
             }
             unsigned bad = 0;
@@ -278,9 +329,16 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
                     }
                 }
                 T L, R;
-                if (!w.template face<MPF>(a, L, R)) bad |= 1u << i;
+                bool ok;
+                if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
+                else ok = w.template face<MPF>(a, L, R);
+                if (!ok) bad |= 1u << i;
                 Lg[i % G] = L;
                 Rg[i % G] = R;
+                if (NOUT == 1 && i == G - 1 && wait_out) {
+                    if (lane == 0) bulk_wait_read0();
+                    __syncwarp();
+                }
                 if (i % G == G - 1) {
                     unsigned char* dL = ob + swz<T>((unsigned)lane, (unsigned)(i - G + 1));
                     if constexpr (sizeof(T) == 8) {
@@ -291,8 +349,11 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
                         *(float4*)(dL + OB) = make_float4(Rg[0], Rg[1], Rg[2], Rg[3]);
                     }
                 }
-                if constexpr (KIND == 0) w.push(a, cg[pq % G]);
-                else w.push(a, cell(kq, pq));
+                T n;
+                if constexpr (KIND == 0) n = cg[pq % G];
+                else n = cell(kq, pq);
+                if constexpr (PF) w.push(a, BetaRow(srow(kc, i + 1)), n);
+                else w.push(a, n);
             }
             const int nF = f_end - f0 < F ? f_end - f0 : F;
             bad &= (1u << nF) - 1u;
@@ -302,7 +363,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    march_redo<MPF>(a, col, f0 + i, L, R);
+                    march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
@@ -438,17 +499,32 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     a.seg = (int)seg;
     a.n_seg = (int)((nf4 + seg - 1) / seg);
     a.n_items = cols * a.n_seg;
-    const int out_bytes = kTmaOut * 2 * 32 * kTmaF * ES;
+    const bool pf = a.ftab != nullptr;
+    const int nst = pf ? kPfStages : kTmaStages;
+    const int out_bytes = (pf ? kPfOut : kTmaOut) * 2 * 32 * kTmaF * ES;
     t.ring_off = out_bytes;
-    t.warp_bytes = ((out_bytes + kTmaStages * t.stage_bytes + 1023) / 1024) * 1024;
-    const size_t smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * kTmaStages * 8;
+    t.rows_off = out_bytes + nst * t.stage_bytes;
+    t.warp_bytes = ((t.rows_off + (pf ? nst * kPfRowBytes : 0) + 1023) / 1024) * 1024;
+    const size_t smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * nst * 8;
     using KFn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, MarchArgs, MarchTmaArgs);
     static const KFn table[2][2][2] = {
-        {{sweep_march_tma_kernel<false, 0, T, 0>, sweep_march_tma_kernel<false, 0, T, 1>},
-         {sweep_march_tma_kernel<false, 1, T, 0>, sweep_march_tma_kernel<false, 1, T, 1>}},
-        {{sweep_march_tma_kernel<true, 0, T, 0>, sweep_march_tma_kernel<true, 0, T, 1>},
-         {sweep_march_tma_kernel<true, 1, T, 0>, sweep_march_tma_kernel<true, 1, T, 1>}}};
-    const KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+        {{sweep_march_tma_kernel<false, 0, T, 0, false>, sweep_march_tma_kernel<false, 0, T, 1, false>},
+         {sweep_march_tma_kernel<false, 1, T, 0, false>, sweep_march_tma_kernel<false, 1, T, 1, false>}},
+        {{sweep_march_tma_kernel<true, 0, T, 0, false>, sweep_march_tma_kernel<true, 0, T, 1, false>},
+         {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
+    KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+    if (a.ftab) {
+        // face-dependent coefficients: FP64 with TMA input tiles
+        if constexpr (sizeof(T) == 8) {
+            if (ldr) return 1003;
+            static const KFn ptable[2][2] = {
+                {sweep_march_tma_kernel<false, 0, T, 0, true>, sweep_march_tma_kernel<false, 1, T, 0, true>},
+                {sweep_march_tma_kernel<true, 0, T, 0, true>, sweep_march_tma_kernel<true, 1, T, 0, true>}};
+            kfn = ptable[mp ? 1 : 0][kind1 ? 1 : 0];
+        } else {
+            return 1003;
+        }
+    }
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kTmaWarps * 32, smem);

@@ -284,6 +284,39 @@ int kernel_choice() {
     return 0;
 }
 
+// The marching kernels' one-sided MP median takes sign(v_L - v_0) from the
+// sign of the weighted candidate sum, which holds for non-negative ideal
+// weights (Coef<5> layout: dL at 12..14, dR at 15..17).
+bool march_weights_ok(const double* ucf) {
+    for (int q = 12; q < 18; ++q)
+        if (!(ucf[q] >= 0.0)) return false;
+    return true;
+}
+
+// FP64 WENO5-JS marching sweep with face-dependent coefficient arrays: the
+// per-face table (one 224-byte row per face; ns + 16 rows: the kernel stages
+// rows f0 .. f0 + 8 with every input tile, and its last tile starts below
+// ns + 5) is built on the stream, used by the TMA marching kernel and freed
+// stream-ordered.  Returns WENO_SB_ERR_UNSUPPORTED when the layout does not
+// suit the kernel.
+int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const double* in,
+                       double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st) {
+    if (!cp.polyL || !cp.polyR || !cp.dL || !cp.dR || !cp.beta) return WENO_SB_ERR_UNSUPPORTED;
+    if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
+    const int rows = (int)g.ns + 16;
+    double* tab = nullptr;
+    WSB_CUDA(cudaMallocAsync((void**)&tab, sizeof(double) * kFaceRow * (size_t)rows, st));
+    march_face_table_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
+    MarchArgs a0 = make_march_args(g, in, vL, vR, wp, nullptr);
+    a0.ftab = tab;
+    a0.cp = cp;
+    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
+    const cudaError_t le = cudaGetLastError();
+    WSB_CUDA(cudaFreeAsync(tab, st));
+    if (rc) return rc;
+    return cuda_err(le, "march sweep launch (per-face coefficients)");
+}
+
 // Coefficients come either per face (cf, device arrays) or, when ucf is
 // non-null, as one face-independent set laid out like Coef<order>.
 template <typename T>
@@ -298,7 +331,8 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
-    if ((choice == 0 || choice == 3 || choice == 5) && ucf && order == 5 && gr->scheme == WENO_SB_JS) {
+    if ((choice == 0 || choice == 3 || choice == 5) && ucf && order == 5 && gr->scheme == WENO_SB_JS &&
+        march_weights_ok(ucf)) {
         if (choice != 5 && g.nc >= 1) {
             const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
             int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
@@ -307,6 +341,12 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
         }
         int rc = launch_march_sweep<T>(g, mp, in, vL, vR, wp, ucf, st, num_sms());
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
+    }
+    if constexpr (sizeof(T) == 8) {
+        if ((choice == 0 || choice == 3) && !ucf && order == 5 && gr->scheme == WENO_SB_JS) {
+            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st);
+            if (rc != WENO_SB_ERR_UNSUPPORTED) return rc;
+        }
     }
     if constexpr (sizeof(T) == 8) {
         if (choice == 0 || choice == 3 || choice == 4) {
@@ -362,7 +402,7 @@ int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsign
     if (folded && !acc_flag)
         WSB_CUDA(cudaMemsetAsync(gv, 0, sizeof(double) * d.E[0] * d.E[1] * d.E[2] * d.nv, st));
     const bool uni = ucf != nullptr;
-    if (uni && order == 5 && gr->scheme == WENO_SB_JS && kernel_choice() != 1) {
+    if (uni && order == 5 && gr->scheme == WENO_SB_JS && kernel_choice() != 1 && march_weights_ok(ucf)) {
         int rc = launch_vjp_march(d.E, a.g, dir, folded, a.mp != 0, a.accumulate != 0, v, ucf, a.wp, gL, gR, gv, st,
                                   num_sms());
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "vjp march launch") : rc;
