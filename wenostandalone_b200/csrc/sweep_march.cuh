@@ -620,20 +620,6 @@ __device__ __forceinline__ float mm32(float dl, float dr) {
     return __int_as_float((hu & ~kill) | (hl & (int)0x80000000));
 }
 
-// A weight w in [0, 2) to float through 2 + w, whose exponent is fixed:
-// the float mantissa is read off the double's bits and 2 is taken back off
-// exactly.  Truncation, absolute error below 2^-22; the weights only scale
-// differences of candidate offsets, so an absolute bound is what matters.
-__device__ __forceinline__ float w2f(double w) {
-    const double s = 2.0 + w;
-    const unsigned t = __funnelshift_l((unsigned)__double2loint(s), (unsigned)__double2hiint(s), 3);
-    return __uint_as_float((t & 0x007FFFFFu) | 0x40000000u) - 2.0f;
-}
-
-// +-1 with the sign of x.
-__device__ __forceinline__ float sign1(float x) {
-    return __int_as_float((__float_as_int(x) & (int)0x80000000) | 0x3F800000);
-}
 
 struct March32 {
     float vm1, v0, vp1, vp2;    // cells J-1 .. J+2
@@ -649,8 +635,8 @@ struct March32 {
     __device__ __forceinline__ void init(const MarchArgs& a, float c0, float c1, float c2, float c3, float c4) {
         vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
         fm2 = c1 - c0; fm1 = c2 - c1; f0 = c3 - c2; fp1 = c4 - c3;
-        const double D0 = f2d_bits(c0), D1 = f2d_bits(c1), D2 = f2d_bits(c2), D3 = f2d_bits(c3);
-        Dp2 = f2d_bits(c4);
+        const double D0 = c0, D1 = c1, D2 = c2, D3 = c3;
+        Dp2 = c4;
         const double dm2 = D1 - D0, dm1 = D2 - D1, d0 = D3 - D2;
         dp1 = Dp2 - D3;
         const double sm2 = dm2 * dm2, sm1 = dm1 * dm1, s0 = d0 * d0;
@@ -667,7 +653,7 @@ struct March32 {
     }
 
     __device__ __forceinline__ void push(const MarchArgs& a, float n) {
-        const double Dn = f2d_bits(n);
+        const double Dn = n;
         const double dn = Dn - Dp2;
         const double sn = dn * dn;
         double g0, g1, g2;
@@ -689,9 +675,11 @@ struct March32 {
         const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
         const double aL0 = a.ucf[12] * P0, aL2 = a.ucf[14] * P2, aR0 = a.ucf[15] * P0, aR2 = a.ucf[17] * P2;
         const double SL = fma(a.ucf[13], P1, aL0 + aL2), SR = fma(a.ucf[16], P1, aR0 + aR2);
-        const bool ok = mid_range(SL) && mid_range(SR);
-        const double r = rcp1(SL * SR), gL = SR * r, gR = SL * r;
-        const float wL0 = w2f(aL0 * gL), wL2 = w2f(aL2 * gL), wR0 = w2f(aR0 * gR), wR2 = w2f(aR2 * gR);
+        const double p = SL * SR;
+        const bool ok = mid_range_prod(p);
+        const double r = rcp1(p), gL = SR * r, gR = SL * r;
+        const float wL0 = __double2float_rn(aL0 * gL), wL2 = __double2float_rn(aL2 * gL),
+                    wR0 = __double2float_rn(aR0 * gR), wR2 = __double2float_rn(aR2 * gR);
         // candidate offsets e_k = p_k - v0; pf2[q] = (polyL, polyR) of Coef<5> index q
         const float eL0 = fmaf(a.pf2[0].x, fp1, a.pf2[1].x * f0), eR0 = fmaf(a.pf2[0].y, fp1, a.pf2[1].y * f0);
         const float eL1 = fmaf(a.pf2[2].x, f0, a.pf2[3].x * fm1), eR1 = fmaf(a.pf2[2].y, f0, a.pf2[3].y * fm1);
@@ -700,28 +688,27 @@ struct March32 {
         float xL = fmaf(wL0, eL0 - eL1, fmaf(wL2, eL2 - eL1, eL1));
         float xR = fmaf(wR0, eR0 - eR1, fmaf(wR2, eR2 - eR1, eR1));
         if constexpr (MPF) {
-            // one-sided median in offset space (see March64::face): with
-            // s = sign(x), s * result = min(s x, max(max(0, -s b), s MD),
-            // max(max(0, s UL), s LC)), b = v0 - vm1, c = vp1 - v0; the
-            // right state is the same formula with (b, c, mA, mB) -> (-c, -b, mB, mA)
+            // one-sided median in offset space (see March64::face): the
+            // bounds relative to v0 are lo = max(min(0, -b, md), min(0, ul, lc))
+            // and hi = min(max(0, -b, md), max(0, ul, lc)) with b = v0 - vm1,
+            // c = vp1 - v0, md = -(b + mA)/2, ul = -2c, lc = 4/3 mB - c/2;
+            // for x >= 0 the result is min(x, hi), else max(x, lo), so each
+            // min/max below is chosen by the sign of x.  The right state is the
+            // same formula with (b, c, mA, mB) -> (-c, -b, mB, mA).
             const float kB = 4.0f / 3.0f;
             {
-                const float sg = sign1(xL);
-                const float sMD = (-0.5f * sg) * (fm1 + mA);
-                const float sLC = sg * fmaf(kB, mB, -0.5f * f0);
-                const float sUL = (-2.0f * sg) * f0;
-                const float sNB = -sg * fm1;
-                const float T = fminf(fminf(sg * xL, fmaxf(fmaxf(0.0f, sNB), sMD)), fmaxf(fmaxf(0.0f, sUL), sLC));
-                xL = sg * T;
+                const bool pos = xL >= 0.0f;
+                const float md = -0.5f * (fm1 + mA), ul = -2.0f * f0, lc = fmaf(kB, mB, -0.5f * f0), nb = -fm1;
+                const float A = pos ? fmaxf(fmaxf(0.0f, nb), md) : fminf(fminf(0.0f, nb), md);
+                const float B = pos ? fmaxf(fmaxf(0.0f, ul), lc) : fminf(fminf(0.0f, ul), lc);
+                xL = pos ? fminf(fminf(xL, A), B) : fmaxf(fmaxf(xL, A), B);
             }
             {
-                const float sg = sign1(xR);
-                const float sMD = (-0.5f * sg) * (mB - f0);
-                const float sLC = sg * fmaf(kB, mA, 0.5f * fm1);
-                const float sUL = (2.0f * sg) * fm1;
-                const float sNB = sg * f0;
-                const float T = fminf(fminf(sg * xR, fmaxf(fmaxf(0.0f, sNB), sMD)), fmaxf(fmaxf(0.0f, sUL), sLC));
-                xR = sg * T;
+                const bool pos = xR >= 0.0f;
+                const float md = -0.5f * (mB - f0), ul = 2.0f * fm1, lc = fmaf(kB, mA, 0.5f * fm1), nb = f0;
+                const float A = pos ? fmaxf(fmaxf(0.0f, nb), md) : fminf(fminf(0.0f, nb), md);
+                const float B = pos ? fmaxf(fmaxf(0.0f, ul), lc) : fminf(fminf(0.0f, ul), lc);
+                xR = pos ? fminf(fminf(xR, A), B) : fmaxf(fmaxf(xR, A), B);
             }
         }
         L = v0 + xL;

@@ -85,6 +85,7 @@ struct MarchTmaArgs {
     int warp_bytes;    // shared memory per warp, a multiple of 1024
     int ring_off;      // byte offset of the input ring within a warp's area
     int rows_off;      // face-dependent coefficients: byte offset of the table-row ring
+    int ldr8;          // per-lane loader, row tiles of floats: cells copied in 8-byte pairs
     unsigned box_bytes;
 };
 
@@ -212,15 +213,31 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
             unsigned char* tp = tile_ptr(k);
             const T* col = column(u0, w, v);
             const long long ncell = a.ns + 6;
+            if (KIND == 0 && sizeof(T) == 4 && t.ldr8) {
+                // contiguous, 8-byte aligned cell pairs (even J0, even column
+                // offsets, even ncell: a pair is wholly inside or outside the
+                // column); the 32-byte swizzle keeps pairs adjacent
 #pragma unroll
-            for (int p = 0; p < F; ++p) {
-                const long long J = (long long)J0 + p;
-                const bool inb = J < ncell;
-                const T* src = col + (inb ? J : 0) * a.sJ;
-                const unsigned dst = smem_u32(tp + cell_off(p));
-                asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src), "n"(sizeof(T)),
-                             "r"(inb ? (unsigned)sizeof(T) : 0u)
-                             : "memory");
+                for (int p = 0; p < F; p += 2) {
+                    const long long J = (long long)J0 + p;
+                    const bool inb = J < ncell;
+                    const T* src = col + (inb ? J : 0);
+                    const unsigned dst = smem_u32(tp + cell_off(p));
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
+                                 "r"(inb ? 8u : 0u)
+                                 : "memory");
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < F; ++p) {
+                    const long long J = (long long)J0 + p;
+                    const bool inb = J < ncell;
+                    const T* src = col + (inb ? J : 0) * a.sJ;
+                    const unsigned dst = smem_u32(tp + cell_off(p));
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src),
+                                 "n"(sizeof(T)), "r"(inb ? (unsigned)sizeof(T) : 0u)
+                                 : "memory");
+                }
             }
             asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
@@ -464,6 +481,13 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
         enc(&mi, dt, 4, (void*)in, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
         ldr = 0;
+    // per-lane loader in 8-byte pairs: float row tiles whose column starts
+    // are all even cells from an 8-byte aligned base (chunks start at even
+    // cells, and an even column length keeps every pair inside or outside)
+    t.ldr8 = (ES == 4 && !kind1 && a.sJ == 1 && ((uintptr_t)in & 7) == 0 && (a.in_off & 1) == 0 &&
+              (a.sU & 1) == 0 && (a.sW & 1) == 0 && (a.sV & 1) == 0 && ((g.ns + 6) & 1) == 0)
+                 ? 1
+                 : 0;
     // outputs (ns, c1, c2, V).  The store unit clips the innermost axis in
     // 16-byte steps, so the face extent is ns - 4 (a 16-byte multiple):
     // faces up to ns-5 are stored by the TMA unit, the last core face ns-4
