@@ -218,6 +218,7 @@ def run_ours(args):
     sp = int(stream.cuda_stream)
     flags = wsb.F_MP | wsb.F_FOLDED
     fp32_main = args.precision == "fp32"
+    pf_main = args.coefficients == "arrays" and not fp32_main
     if fp32_main:
         # FP32-bulk as the timed step: FP32 v_rs_ws per direction (reshaped
         # once, before timing) and FP32 face states
@@ -233,7 +234,7 @@ def run_ours(args):
                 evs[d][0].record(stream)
             if fp32_main:
                 api.weno_uniform(g, d, ORDER, rs32[d], faces[d], o32[d][0], o32[d][1], flags=wsb.F_MP, stream=sp)
-            elif per_face:
+            elif per_face or pf_main:
                 api.weno(g, d, ORDER, v, cstructs[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
             else:
                 api.weno_uniform(g, d, ORDER, v, faces[d], outs[d][0], outs[d][1], flags=flags, stream=sp)
@@ -281,7 +282,7 @@ def run_ours(args):
 
     # the same step with per-face coefficient arrays (stretched-grid form)
     per_face = None
-    if not args.no_extras and not fp32_main:
+    if not args.no_extras and not fp32_main and not pf_main:
         for _ in range(3):
             step(per_face=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -336,21 +337,25 @@ def run_ours(args):
                                     "v_rs_ws" if fp32_main else
                                     "FP64 WENO5-JS + MP fused, x/y/z sweeps reading v_vf directly "
                                     "(reshape folded)") + f", {M + 1}^3 cells x 8 vars, buff_size 6",
-                       "m=n=p": M, "v_size": NV, "buff_size": BUFF, "coefficients": "uniform-grid WENO5-JS",
+                       "m=n=p": M, "v_size": NV, "buff_size": BUFF,
+                       "coefficients": ("uniform-grid WENO5-JS values as per-face device arrays (weno_sb_weno_dev)"
+                                        if pf_main else "uniform-grid WENO5-JS"),
                        "field": "seeded smooth-plus-jump", "l2": "inputs (663 MB) and outputs (3.7 GB) exceed "
                                                                   "the 126 MB L2; no flush",
                        "parallelism": f"{ws} independent blocks (weak scaling, no collective)"},
             "roofline": {"bound": "hbm", "kernel": (f"sweep_march_tma_kernel<MP,row tiles,float,cp.async loader> "
                                                     f"{'xyz'[dk]} sweep" if fp32_main else
                                                     f"sweep_march_tma_kernel<MP,{'row' if dk == 0 else 'column'} "
-                                                    f"tiles,double,TMA loader> {'xyz'[dk]} sweep"),
+                                                    f"tiles,double,TMA loader{',per-face table' if pf_main else ''}> "
+                                                    f"{'xyz'[dk]} sweep"),
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "alg_bytes_per_launch": ab, "launch_ms": dk_ms,
-                         "traffic": None if (fp32_main or M != 199) else read_traffic()},
+                         "traffic": None if (fp32_main or pf_main or M != 199) else read_traffic()},
             "per_sweep_ms": [s / K for s in sums],
-            "gpu_launches": 3 * K,
+            # the per-face form launches the table build and the sweep
+            "gpu_launches": (6 if pf_main else 3) * K,
             "clocks": clk.summary(),
         }
         if per_face:
@@ -776,6 +781,9 @@ def main():
     ap.add_argument("--m", type=int, default=199, help="cells per axis minus one (m=n=p); 199 = 200^3")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="fp32: time the FP32-bulk form as the main step (no extras)")
+    ap.add_argument("--coefficients", choices=["uniform", "arrays"], default="uniform",
+                    help="arrays: the main step passes the coefficients as per-face device arrays "
+                         "(weno_sb_weno_dev, the drop-in form) instead of one face-independent set")
     args = ap.parse_args()
     global M
     M = args.m
