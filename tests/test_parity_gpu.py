@@ -385,6 +385,36 @@ def test_full_size_weno5_mp(wsb, oracle_mod, entry):
         torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("order", [5, 7])
+def test_mid_size_uniform_entry(wsb, oracle_mod, order):
+    """96^3 x 4 (several segments per column, every tile shape), WENO5 / WENO7
+    JS + MP through the face-independent entry, drop-in and folded, against
+    the oracle at 1e-12 per array."""
+    import torch
+    from wenostandalone_b200 import api, fields
+    m, nv = 95, 4
+    g = wsb.Grid(m, m, m, nv, 6)
+    vf = fields.smooth_jump_field(m, m, m, nv, 6, seed=2)
+    v = to_dev(vf)
+    for d in range(3):
+        coefs = fields.uniform_weno_coefficients(order, g.nc(d))
+        rs = oracle_mod.reshape(vf, m, m, m, 6, d)
+        Lr, Rr = oracle_mod.order1_copy(vf, m, m, m, 6, d)
+        oracle_mod.reconstruct(rs, coefs, order, vL=Lr, vR=Rr)
+        oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+        for folded in (False, True):
+            L, R = nan_dev(g.face_shape(d)), nan_dev(g.face_shape(d))
+            api.order1_copy(g, d, v, L, R)
+            src = v
+            if not folded:
+                src = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float64, device="cuda")
+                api.reshape(g, d, v, src)
+            api.weno_uniform(g, d, order, src, coefs, L, R, flags=wsb.F_MP | (wsb.F_FOLDED if folded else 0))
+            eL = rel_err(from_dev(L, g.face_shape(d)), Lr)
+            eR = rel_err(from_dev(R, g.face_shape(d)), Rr)
+            assert eL <= TOL64 and eR <= TOL64, (d, folded, eL, eR)
+
+
 def test_argument_errors(wsb):
     import ctypes
     import torch

@@ -55,6 +55,9 @@ struct MarchArgs {
     double kL[6], kR[6];
     // FP32-bulk engine: (polyL, polyR) float pairs, Coef<5>::pL index order
     float2 pf2[6];
+    // WENO7 engine (ucf in the Coef<7> layout): kL7[3s+t] = dL[s] polyL[3(3-s)+t]
+    // for stencil s, term t (and kR7 likewise)
+    double kL7[12], kR7[12];
     // face-dependent coefficients (FP64 kernels): the per-face table built by
     // march_face_table_kernel, and the arrays it was built from (for faces
     // that are redone); ftab is null for face-independent coefficients
@@ -587,6 +590,148 @@ __device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __re
     if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
 }
 
+// ---------------------------------------------------------------------
+// WENO7-JS (+ MP) marching engine, FP64, face-independent coefficients
+// (Coef<7> layout in MarchArgs::ucf: polyL 0..11, polyR 12..23, dL 24..27,
+// dR 28..31, beta 32..55).  Stencil s (0..3) of face J reads the triple
+// (a, b, e) = (d[J+s-1], d[J+s-2], d[J+s-3]) with coefficient row r = 3 - s
+// (f90:1462-1473 and 1480-1488: beta(3-r) and poly(3-r) from dvd(2-r),
+// dvd(1-r), dvd(-r)).  The newest triple T_m = (d[m], d[m+1], d[m+2]) is
+// stencil 3 of face m, 2 of m+1, 1 of m+2 and 0 of m+3: each pushed cell
+// gives one beta to each of four faces (its six products: three new, three
+// carried from the previous triple), kept in registers until its face.
+// Weights as March64: ideal weights folded into the candidate coefficients
+// (MarchArgs::kL7 / kR7), one reciprocal of S_L S_R, the one-sided MP median.
+// ---------------------------------------------------------------------
+struct March64_7 {
+    double vm1, v0, vp1, vp2, vp3;        // cells J-1 .. J+3
+    double dm3, dm2, dm1, d0, dp1, dp2;    // d[k] = v[k+1] - v[k], k = J-3 .. J+2
+    double s1, s2, c12;                    // d[J+1]^2, d[J+2]^2, d[J+1] d[J+2]
+    double q0, q1, q2, q3;                 // beta_s(J)^2
+    double n0a, n0b, n0c, n1a, n1b, n2a;   // beta_0(J+1 .. J+3), beta_1(J+1 .. J+2), beta_2(J+1)
+    double e2, mA, mB;                     // d[J+1] - d[J]; minmods of the MP limiter
+
+    // beta of coefficient row r from the products of a triple (a newest, e oldest)
+    __device__ __forceinline__ static double beta_row(const MarchArgs& a, int r, double aa, double ab, double ae,
+                                                      double bb, double be, double ee) {
+        const int o = 32 + 6 * r;
+        return fma(a.ucf[o], aa, fma(a.ucf[o + 1], ab, fma(a.ucf[o + 2], ae,
+                   fma(a.ucf[o + 3], bb, fma(a.ucf[o + 4], be, fma(a.ucf[o + 5], ee, a.wp.eps))))));
+    }
+    __device__ __forceinline__ static double beta_row(const MarchArgs& a, int r, double x, double y, double z) {
+        // triple (e, b, a) = (x, y, z)
+        return beta_row(a, r, z * z, z * y, z * x, y * y, y * x, x * x);
+    }
+
+    // Window of face J from cells J-3 .. J+3.
+    __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3, double c4,
+                                         double c5, double c6) {
+        vm1 = c2; v0 = c3; vp1 = c4; vp2 = c5; vp3 = c6;
+        dm3 = c1 - c0; dm2 = c2 - c1; dm1 = c3 - c2; d0 = c4 - c3; dp1 = c5 - c4; dp2 = c6 - c5;
+        s1 = dp1 * dp1; s2 = dp2 * dp2; c12 = dp1 * dp2;
+        const double b0 = beta_row(a, 3, dm3, dm2, dm1);               // T_{J-3}
+        const double b1 = beta_row(a, 2, dm2, dm1, d0);                // T_{J-2}
+        n0a = beta_row(a, 3, dm2, dm1, d0);
+        const double b2 = beta_row(a, 1, dm1, d0, dp1);                // T_{J-1}
+        n1a = beta_row(a, 2, dm1, d0, dp1);
+        n0b = beta_row(a, 3, dm1, d0, dp1);
+        const double b3 = beta_row(a, 0, d0, dp1, dp2);                // T_J
+        n2a = beta_row(a, 1, d0, dp1, dp2);
+        n1b = beta_row(a, 2, d0, dp1, dp2);
+        n0c = beta_row(a, 3, d0, dp1, dp2);
+        q0 = b0 * b0; q1 = b1 * b1; q2 = b2 * b2; q3 = b3 * b3;
+        const double em = dm1 - dm2, ez = d0 - dm1;
+        e2 = dp1 - d0;
+        mA = mm64(em, ez);
+        mB = mm64(ez, e2);
+    }
+
+    // Advance to face J+1; n is cell J+4.
+    __device__ __forceinline__ void push(const MarchArgs& a, double n) {
+        const double dn = n - vp3;
+        const double aa = dn * dn, ab = dn * dp2, ae = dn * dp1;       // T_{J+1}: a = dn, b = dp2, e = dp1
+        const double g0 = beta_row(a, 0, aa, ab, ae, s2, c12, s1);
+        const double g1 = beta_row(a, 1, aa, ab, ae, s2, c12, s1);
+        const double g2 = beta_row(a, 2, aa, ab, ae, s2, c12, s1);
+        const double g3 = beta_row(a, 3, aa, ab, ae, s2, c12, s1);
+        q0 = n0a * n0a; q1 = n1a * n1a; q2 = n2a * n2a; q3 = g0 * g0;
+        n0a = n0b; n0b = n0c; n0c = g3;
+        n1a = n1b; n1b = g2;
+        n2a = g1;
+        const double ne2 = dp2 - dp1;
+        const double nmB = mm64(e2, ne2);
+        vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = vp3; vp3 = n;
+        dm3 = dm2; dm2 = dm1; dm1 = d0; d0 = dp1; dp1 = dp2; dp2 = dn;
+        s1 = s2; s2 = aa; c12 = ab;
+        e2 = ne2; mA = mB; mB = nmB;
+    }
+
+    // WENO7-JS (+ MP) state of face J; false when the one-reciprocal form is
+    // out of range (the caller redoes the face).
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+        const double q01 = q0 * q1, q23 = q2 * q3;
+        const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
+        const double SL = fma(a.ucf[24], P0, fma(a.ucf[25], P1, fma(a.ucf[26], P2, a.ucf[27] * P3)));
+        const double SR = fma(a.ucf[28], P0, fma(a.ucf[29], P1, fma(a.ucf[30], P2, a.ucf[31] * P3)));
+        // stencil s: (a, b, e) = (d[J+s-1], d[J+s-2], d[J+s-3])
+        const double eL0 = fma(a.kL7[0], dm1, fma(a.kL7[1], dm2, a.kL7[2] * dm3));
+        const double eL1 = fma(a.kL7[3], d0, fma(a.kL7[4], dm1, a.kL7[5] * dm2));
+        const double eL2 = fma(a.kL7[6], dp1, fma(a.kL7[7], d0, a.kL7[8] * dm1));
+        const double eL3 = fma(a.kL7[9], dp2, fma(a.kL7[10], dp1, a.kL7[11] * d0));
+        const double eR0 = fma(a.kR7[0], dm1, fma(a.kR7[1], dm2, a.kR7[2] * dm3));
+        const double eR1 = fma(a.kR7[3], d0, fma(a.kR7[4], dm1, a.kR7[5] * dm2));
+        const double eR2 = fma(a.kR7[6], dp1, fma(a.kR7[7], d0, a.kR7[8] * dm1));
+        const double eR3 = fma(a.kR7[9], dp2, fma(a.kR7[10], dp1, a.kR7[11] * d0));
+        const double EL = fma(P0, eL0, fma(P1, eL1, fma(P2, eL2, P3 * eL3)));
+        const double ER = fma(P0, eR0, fma(P1, eR1, fma(P2, eR2, P3 * eR3)));
+        const double p = SL * SR;
+        const bool ok = mid_range_prod(p);
+        const double r = rcp1(p);
+        L = fma(EL * SR, r, v0);
+        R = fma(ER * SL, r, v0);
+        if constexpr (MPF) {
+            // the one-sided MP median of March64::face (the limiter reads
+            // cells J-2 .. J+2 for every order)
+            const double kBetaMP = 4.0 / 3.0;
+            const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
+            {
+                const bool pos = sign_clear(EL);
+                const double UL = fma(-2.0, d0, v0);
+                const double MD = fma(-0.5, dm1 + mA, v0);
+                const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
+                const double Q1 = (pos == up_l) ? v0 : vm1;
+                const double Q2 = (pos == up_r) ? v0 : UL;
+                const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
+                L = mm_sel(mm_sel(L, A, !pos), B, !pos);
+            }
+            {
+                const bool pos = sign_clear(ER);
+                const double UL = fma(2.0, dm1, v0);
+                const double MD = fma(0.5, d0 - mB, v0);
+                const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
+                const double Q1 = (pos == up_r) ? vp1 : v0;
+                const double Q2 = (pos == up_l) ? UL : v0;
+                const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
+                R = mm_sel(mm_sel(R, A, !pos), B, !pos);
+            }
+        }
+        return ok;
+    }
+};
+
+// The reference sequence for one WENO7 face (cells o .. o+6 of the column).
+template <bool MPF>
+__device__ __noinline__ void march64_7_redo(const MarchArgs& a, const double* __restrict__ col, long long o,
+                                            double& L, double& R) {
+    const Coef<7>& c = *reinterpret_cast<const Coef<7>*>(a.ucf);
+    double v[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) v[q] = __ldg(col + (o + q) * a.sJ);
+    weno7_face<double>(v + 3, c, JS, a.wp.eps, 0.0, L, R);
+    if (MPF) mp_limit(v[1], v[2], v[3], v[4], v[5], L, R);
+}
+
 // The same for face-dependent coefficients: core face o - 3 of the arrays.
 template <bool MPF>
 __device__ __noinline__ void march64_redo_faces(const MarchArgs& a, const double* __restrict__ col, long long o,
@@ -841,7 +986,7 @@ __global__ void __launch_bounds__(128, WSB_MARCH64_MIN_BLOCKS)
 // Arguments of a marching sweep for face-independent WENO5-JS coefficients
 // (everything but the segmentation).
 inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, void* vR, const WenoParams& wp,
-                                 const double* ucf) {
+                                 const double* ucf, int order = 5) {
     MarchArgs a{};
     a.in = in; a.vL = vL; a.vR = vR; a.wp = wp;
     a.ns = g.ns; a.nc = g.nc;
@@ -859,6 +1004,14 @@ inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, v
     a.n_ut = (a.Nu + 31) / 32;
     if (!ucf) return a;  // face-dependent coefficients: the caller sets ftab and cp
     for (int q = 0; q < 56; ++q) a.ucf[q] = ucf[q];
+    if (order == 7) {
+        for (int s = 0; s < 4; ++s)
+            for (int t = 0; t < 3; ++t) {
+                a.kL7[3 * s + t] = ucf[24 + s] * ucf[3 * (3 - s) + t];
+                a.kR7[3 * s + t] = ucf[28 + s] * ucf[12 + 3 * (3 - s) + t];
+            }
+        return a;
+    }
     for (int q = 0; q < 6; ++q) {
         a.ucf32[q] = (float)ucf[q];          // polyL (Coef<5>::pL)
         a.ucf32[6 + q] = (float)ucf[6 + q];  // polyR

@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <type_traits>
 
 #include "sweep_march.cuh"
 #include "sweep_pipe.cuh"
@@ -141,9 +142,15 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col,
 #ifndef WSB_MTMA_MIN_BLOCKS_F32
 #define WSB_MTMA_MIN_BLOCKS_F32 3
 #endif
+#ifndef WSB_MTMA_MIN_BLOCKS_W7
+#define WSB_MTMA_MIN_BLOCKS_W7 2  // WENO7 carries ~27 doubles of state: 3 CTAs per SM would spill
+#endif
 // PF: face-dependent coefficients from the per-face table a.ftab (FP64).
-template <bool MPF, int KIND, typename T, int LDR, bool PF>
-__global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32)
+// ORDER 7: the WENO7 engine (FP64, face-independent coefficients); face f
+// reads cells f .. f+6 and pushes cell f+7.
+template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5>
+__global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
+                                                  : (sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32))
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
                            const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
                            const MarchTmaArgs t) {
@@ -152,7 +159,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
-    using Engine = typename MarchEngine<T>::type;
+    static_assert(ORDER == 5 || (ORDER == 7 && sizeof(T) == 8 && !PF), "WENO7: FP64, face-independent");
+    using Engine = std::conditional_t<ORDER == 7, March64_7, typename MarchEngine<T>::type>;
+    constexpr int PUSH0 = ORDER == 7 ? 7 : 6;             // tile position of the cell pushed after face f0
     extern __shared__ __align__(1024) unsigned char smem_mt[];
     unsigned char* base = smem_mt + ((1024u - (smem_u32(smem_mt) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -282,7 +291,12 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
             // face 3 (cells 4..8 = tile positions 0..4), plain stores
             T L, R;
             bool ok;
-            if constexpr (PF) {
+            if constexpr (ORDER == 7) {
+                // face 3 reads cells 3 .. 9: cell 3 lies before tile 0 (cells 4 .. 11)
+                const T c3 = __ldg(column(u0, wv, vv) + 3 * a.sJ);
+                w.init(a, c3, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
+                ok = w.template face<MPF>(a, L, R);
+            } else if constexpr (PF) {
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
                 ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
@@ -290,16 +304,22 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
                 ok = w.template face<MPF>(a, L, R);
             }
-            if (!ok) march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
+            if (!ok) {
+                if constexpr (ORDER == 7) march64_7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
+                else march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
+            }
             if (u0 + lane < a.Nu) {
                 const long long oi = 3 + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
                 outL[oi] = L;
                 outR[oi] = R;
             }
-            if constexpr (PF) w.push(a, BetaRow(row(4)), cell(k0, 5));
+            if constexpr (ORDER == 7) w.push(a, cell(k0, 6));
+            else if constexpr (PF) w.push(a, BetaRow(row(4)), cell(k0, 5));
             else w.push(a, cell(k0, 5));
         } else {
-            if constexpr (PF)
+            if constexpr (ORDER == 7)
+                w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5), cell(k0, 6));
+            else if constexpr (PF)
                 w.init(a, BetaRow(row(f_start - 2)), BetaRow(row(f_start - 1)), BetaRow(row(f_start)), cell(k0, 1),
                        cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
             else
@@ -329,7 +349,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
             T Lg[G], Rg[G], cg[G];
 #pragma unroll
             for (int i = 0; i < F; ++i) {
-                const int q = 6 + i;                      // position of the pushed cell, tiles c / c+1
+                const int q = PUSH0 + i;                  // position of the pushed cell, tiles c / c+1
                 const unsigned kq = q < 8 ? kc : kc + 1;
                 const int pq = q & 7;
                 if constexpr (KIND == 0) {
@@ -380,7 +400,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    march_redo<MPF, PF>(a, col, f0 + i, L, R);
+                    if constexpr (ORDER == 7) march64_7_redo<MPF>(a, col, f0 + i, L, R);
+                    else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
@@ -427,7 +448,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, sizeof(T) == 8 ? WSB_MTMA_MIN_
 // kernel with per-lane loads.
 template <typename T>
 int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const T* in, T* vL,
-                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms) {
+                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms, int order = 5) {
     constexpr int ES = (int)sizeof(T);
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return 1003;
@@ -537,7 +558,20 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
         {{sweep_march_tma_kernel<true, 0, T, 0, false>, sweep_march_tma_kernel<true, 0, T, 1, false>},
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
-    if (a.ftab) {
+    if (order == 7) {
+        // WENO7: FP64, face-independent coefficients
+        if constexpr (sizeof(T) == 8) {
+            if (a.ftab) return 1003;
+            static const KFn table7[2][2][2] = {
+                {{sweep_march_tma_kernel<false, 0, T, 0, false, 7>, sweep_march_tma_kernel<false, 0, T, 1, false, 7>},
+                 {sweep_march_tma_kernel<false, 1, T, 0, false, 7>, sweep_march_tma_kernel<false, 1, T, 1, false, 7>}},
+                {{sweep_march_tma_kernel<true, 0, T, 0, false, 7>, sweep_march_tma_kernel<true, 0, T, 1, false, 7>},
+                 {sweep_march_tma_kernel<true, 1, T, 0, false, 7>, sweep_march_tma_kernel<true, 1, T, 1, false, 7>}}};
+            kfn = table7[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+        } else {
+            return 1003;
+        }
+    } else if (a.ftab) {
         // face-dependent coefficients: FP64 with TMA input tiles
         if constexpr (sizeof(T) == 8) {
             if (ldr) return 1003;

@@ -286,9 +286,10 @@ int kernel_choice() {
 
 // The marching kernels' one-sided MP median takes sign(v_L - v_0) from the
 // sign of the weighted candidate sum, which holds for non-negative ideal
-// weights (Coef<5> layout: dL at 12..14, dR at 15..17).
-bool march_weights_ok(const double* ucf) {
-    for (int q = 12; q < 18; ++q)
+// weights (Coef<5> layout: dL, dR at 12..17; Coef<7>: at 24..31).
+bool march_weights_ok(const double* ucf, int order = 5) {
+    const int q0 = order == 7 ? 24 : 12, q1 = order == 7 ? 32 : 18;
+    for (int q = q0; q < q1; ++q)
         if (!(ucf[q] >= 0.0)) return false;
     return true;
 }
@@ -331,6 +332,15 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
+    if constexpr (sizeof(T) == 8) {
+        if ((choice == 0 || choice == 3) && ucf && order == 7 && gr->scheme == WENO_SB_JS &&
+            march_weights_ok(ucf, 7)) {
+            const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 7);
+            int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 7);
+            if (rc != WENO_SB_ERR_UNSUPPORTED)
+                return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (WENO7)") : rc;
+        }
+    }
     if ((choice == 0 || choice == 3 || choice == 5) && ucf && order == 5 && gr->scheme == WENO_SB_JS &&
         march_weights_ok(ucf)) {
         if (choice != 5 && g.nc >= 1) {
