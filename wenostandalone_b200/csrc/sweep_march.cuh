@@ -58,6 +58,8 @@ struct MarchArgs {
     // WENO7 engine (ucf in the Coef<7> layout): kL7[3s+t] = dL[s] polyL[3(3-s)+t]
     // for stencil s, term t (and kR7 likewise)
     double kL7[12], kR7[12];
+    // FP32-bulk WENO7 engine: float polyL[0..11], polyR[0..11] (Coef<7> order)
+    float pf7[24];
     // face-dependent coefficients (FP64 kernels): the per-face table built by
     // march_face_table_kernel, and the arrays it was built from (for faces
     // that are redone); ftab is null for face-independent coefficients
@@ -890,6 +892,137 @@ __device__ __noinline__ void march32_redo(const MarchArgs& a, const float* __res
     if (MPF) MP<float>::apply(vm2, vm1, v0, vp1, vp2, L, R);
 }
 
+// ---------------------------------------------------------------------
+// FP32-bulk WENO7-JS (+ MP) marching engine: FP32 cells, candidates, MP and
+// face states; FP64 differences, beta and weight normalisation (the split of
+// weno7_js_mixed), with March64_7's carrying of betas from difference
+// triples.  Weights pivot on stencil 1: x = e1 + sum_{s != 1} w_s (e_s - e1).
+// ---------------------------------------------------------------------
+struct March32_7 {
+    float vm1, v0, vp1, vp2, vp3;          // cells J-1 .. J+3
+    float fm3, fm2, fm1, f0, fp1, fp2;      // FP32 differences, k = J-3 .. J+2
+    double Dp3;                             // vp3, widened
+    double dp1, dp2, s1, s2, c12;           // FP64 d[J+1], d[J+2], their squares and product
+    double q0, q1, q2, q3;                  // beta_s(J)^2
+    double n0a, n0b, n0c, n1a, n1b, n2a;    // as March64_7
+    float e2, mA, mB;
+
+    __device__ __forceinline__ void init(const MarchArgs& a, float c0, float c1, float c2, float c3, float c4,
+                                         float c5, float c6) {
+        vm1 = c2; v0 = c3; vp1 = c4; vp2 = c5; vp3 = c6;
+        fm3 = c1 - c0; fm2 = c2 - c1; fm1 = c3 - c2; f0 = c4 - c3; fp1 = c5 - c4; fp2 = c6 - c5;
+        const double D0 = c0, D1 = c1, D2 = c2, D3 = c3, D4 = c4, D5 = c5;
+        Dp3 = c6;
+        const double dm3 = D1 - D0, dm2 = D2 - D1, dm1 = D3 - D2, d0 = D4 - D3;
+        dp1 = D5 - D4; dp2 = Dp3 - D5;
+        s1 = dp1 * dp1; s2 = dp2 * dp2; c12 = dp1 * dp2;
+        const double b0 = March64_7::beta_row(a, 3, dm3, dm2, dm1);
+        const double b1 = March64_7::beta_row(a, 2, dm2, dm1, d0);
+        n0a = March64_7::beta_row(a, 3, dm2, dm1, d0);
+        const double b2 = March64_7::beta_row(a, 1, dm1, d0, dp1);
+        n1a = March64_7::beta_row(a, 2, dm1, d0, dp1);
+        n0b = March64_7::beta_row(a, 3, dm1, d0, dp1);
+        const double b3 = March64_7::beta_row(a, 0, d0, dp1, dp2);
+        n2a = March64_7::beta_row(a, 1, d0, dp1, dp2);
+        n1b = March64_7::beta_row(a, 2, d0, dp1, dp2);
+        n0c = March64_7::beta_row(a, 3, d0, dp1, dp2);
+        q0 = b0 * b0; q1 = b1 * b1; q2 = b2 * b2; q3 = b3 * b3;
+        const float em = fm1 - fm2, ez = f0 - fm1;
+        e2 = fp1 - f0;
+        mA = mm32(em, ez);
+        mB = mm32(ez, e2);
+    }
+
+    __device__ __forceinline__ void push(const MarchArgs& a, float n) {
+        const double Dn = n;
+        const double dn = Dn - Dp3;
+        const double aa = dn * dn, ab = dn * dp2, ae = dn * dp1;
+        const double g0 = March64_7::beta_row(a, 0, aa, ab, ae, s2, c12, s1);
+        const double g1 = March64_7::beta_row(a, 1, aa, ab, ae, s2, c12, s1);
+        const double g2 = March64_7::beta_row(a, 2, aa, ab, ae, s2, c12, s1);
+        const double g3 = March64_7::beta_row(a, 3, aa, ab, ae, s2, c12, s1);
+        q0 = n0a * n0a; q1 = n1a * n1a; q2 = n2a * n2a; q3 = g0 * g0;
+        n0a = n0b; n0b = n0c; n0c = g3;
+        n1a = n1b; n1b = g2;
+        n2a = g1;
+        const float fn = n - vp3;
+        const float ne2 = fp2 - fp1;
+        const float nmB = mm32(e2, ne2);
+        vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = vp3; vp3 = n;
+        fm3 = fm2; fm2 = fm1; fm1 = f0; f0 = fp1; fp1 = fp2; fp2 = fn;
+        Dp3 = Dn; dp1 = dp2; dp2 = dn;
+        s1 = s2; s2 = aa; c12 = ab;
+        e2 = ne2; mA = mB; mB = nmB;
+    }
+
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, float& L, float& R) const {
+        const double q01 = q0 * q1, q23 = q2 * q3;
+        const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
+        const double aL0 = a.ucf[24] * P0, aL2 = a.ucf[26] * P2, aL3 = a.ucf[27] * P3;
+        const double aR0 = a.ucf[28] * P0, aR2 = a.ucf[30] * P2, aR3 = a.ucf[31] * P3;
+        const double SL = fma(a.ucf[25], P1, (aL0 + aL2) + aL3), SR = fma(a.ucf[29], P1, (aR0 + aR2) + aR3);
+        const double p = SL * SR;
+        const bool ok = mid_range_prod(p);
+        const double r = rcp1(p), gL = SR * r, gR = SL * r;
+        const float wL0 = __double2float_rn(aL0 * gL), wL2 = __double2float_rn(aL2 * gL),
+                    wL3 = __double2float_rn(aL3 * gL);
+        const float wR0 = __double2float_rn(aR0 * gR), wR2 = __double2float_rn(aR2 * gR),
+                    wR3 = __double2float_rn(aR3 * gR);
+        // candidate offsets of stencil s (row 3 - s), (a, b, e) = (f[J+s-1], f[J+s-2], f[J+s-3])
+        const float eL0 = fmaf(a.pf7[9], fm1, fmaf(a.pf7[10], fm2, a.pf7[11] * fm3));
+        const float eL1 = fmaf(a.pf7[6], f0, fmaf(a.pf7[7], fm1, a.pf7[8] * fm2));
+        const float eL2 = fmaf(a.pf7[3], fp1, fmaf(a.pf7[4], f0, a.pf7[5] * fm1));
+        const float eL3 = fmaf(a.pf7[0], fp2, fmaf(a.pf7[1], fp1, a.pf7[2] * f0));
+        const float eR0 = fmaf(a.pf7[21], fm1, fmaf(a.pf7[22], fm2, a.pf7[23] * fm3));
+        const float eR1 = fmaf(a.pf7[18], f0, fmaf(a.pf7[19], fm1, a.pf7[20] * fm2));
+        const float eR2 = fmaf(a.pf7[15], fp1, fmaf(a.pf7[16], f0, a.pf7[17] * fm1));
+        const float eR3 = fmaf(a.pf7[12], fp2, fmaf(a.pf7[13], fp1, a.pf7[14] * f0));
+        float xL = fmaf(wL0, eL0 - eL1, fmaf(wL2, eL2 - eL1, fmaf(wL3, eL3 - eL1, eL1)));
+        float xR = fmaf(wR0, eR0 - eR1, fmaf(wR2, eR2 - eR1, fmaf(wR3, eR3 - eR1, eR1)));
+        if constexpr (MPF) {
+            // the one-sided median of March32::face
+            const float kB = 4.0f / 3.0f;
+            {
+                const bool pos = xL >= 0.0f;
+                const float md = -0.5f * (fm1 + mA), ul = -2.0f * f0, lc = fmaf(kB, mB, -0.5f * f0), nb = -fm1;
+                const float A = pos ? fmaxf(fmaxf(0.0f, nb), md) : fminf(fminf(0.0f, nb), md);
+                const float B = pos ? fmaxf(fmaxf(0.0f, ul), lc) : fminf(fminf(0.0f, ul), lc);
+                xL = pos ? fminf(fminf(xL, A), B) : fmaxf(fmaxf(xL, A), B);
+            }
+            {
+                const bool pos = xR >= 0.0f;
+                const float md = -0.5f * (mB - f0), ul = 2.0f * fm1, lc = fmaf(kB, mA, 0.5f * fm1), nb = f0;
+                const float A = pos ? fmaxf(fmaxf(0.0f, nb), md) : fminf(fminf(0.0f, nb), md);
+                const float B = pos ? fmaxf(fmaxf(0.0f, ul), lc) : fminf(fminf(0.0f, ul), lc);
+                xR = pos ? fminf(fminf(xR, A), B) : fmaxf(fmaxf(xR, A), B);
+            }
+        }
+        L = v0 + xL;
+        R = v0 + xR;
+        return ok;
+    }
+};
+
+// The reference sequence for one WENO7 face, FP32 storage (FP64 arithmetic).
+template <bool MPF>
+__device__ __noinline__ void march32_7_redo(const MarchArgs& a, const float* __restrict__ col, long long o, float& L,
+                                            float& R) {
+    const Coef<7>& c = *reinterpret_cast<const Coef<7>*>(a.ucf);
+    float f[7];
+    double v[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        f[q] = __ldg(col + (o + q) * a.sJ);
+        v[q] = f[q];
+    }
+    double Ld, Rd;
+    weno7_face<double>(v + 3, c, JS, a.wp.eps, 0.0, Ld, Rd);
+    L = (float)Ld;
+    R = (float)Rd;
+    if (MPF) MP<float>::apply(f[1], f[2], f[3], f[4], f[5], L, R);
+}
+
 #ifndef WSB_MARCH64_MIN_BLOCKS
 #define WSB_MARCH64_MIN_BLOCKS 3
 #endif
@@ -1010,6 +1143,7 @@ inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, v
                 a.kL7[3 * s + t] = ucf[24 + s] * ucf[3 * (3 - s) + t];
                 a.kR7[3 * s + t] = ucf[28 + s] * ucf[12 + 3 * (3 - s) + t];
             }
+        for (int q = 0; q < 24; ++q) a.pf7[q] = (float)ucf[q];
         return a;
     }
     for (int q = 0; q < 6; ++q) {

@@ -133,6 +133,14 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const double* col
     if constexpr (PF) march64_redo_faces<MPF>(a, col, o, L, R);
     else march64_redo<MPF>(a, col, o, L, R);
 }
+template <bool MPF>
+__device__ __forceinline__ void march7_redo(const MarchArgs& a, const double* col, long long o, double& L, double& R) {
+    march64_7_redo<MPF>(a, col, o, L, R);
+}
+template <bool MPF>
+__device__ __forceinline__ void march7_redo(const MarchArgs& a, const float* col, long long o, float& L, float& R) {
+    march32_7_redo<MPF>(a, col, o, L, R);
+}
 template <bool MPF, bool PF>
 __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col, long long o, float& L, float& R) {
     static_assert(!PF, "face-dependent coefficients: FP64 kernels only");
@@ -159,8 +167,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
-    static_assert(ORDER == 5 || (ORDER == 7 && sizeof(T) == 8 && !PF), "WENO7: FP64, face-independent");
-    using Engine = std::conditional_t<ORDER == 7, March64_7, typename MarchEngine<T>::type>;
+    static_assert(ORDER == 5 || (ORDER == 7 && !PF), "WENO7: face-independent coefficients");
+    using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
+                                      typename MarchEngine<T>::type>;
     constexpr int PUSH0 = ORDER == 7 ? 7 : 6;             // tile position of the cell pushed after face f0
     extern __shared__ __align__(1024) unsigned char smem_mt[];
     unsigned char* base = smem_mt + ((1024u - (smem_u32(smem_mt) & 1023u)) & 1023u);
@@ -305,7 +314,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 ok = w.template face<MPF>(a, L, R);
             }
             if (!ok) {
-                if constexpr (ORDER == 7) march64_7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
+                if constexpr (ORDER == 7) march7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
                 else march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
             }
             if (u0 + lane < a.Nu) {
@@ -400,7 +409,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    if constexpr (ORDER == 7) march64_7_redo<MPF>(a, col, f0 + i, L, R);
+                    if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
                     else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
@@ -559,18 +568,14 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     if (order == 7) {
-        // WENO7: FP64, face-independent coefficients
-        if constexpr (sizeof(T) == 8) {
-            if (a.ftab) return 1003;
-            static const KFn table7[2][2][2] = {
-                {{sweep_march_tma_kernel<false, 0, T, 0, false, 7>, sweep_march_tma_kernel<false, 0, T, 1, false, 7>},
-                 {sweep_march_tma_kernel<false, 1, T, 0, false, 7>, sweep_march_tma_kernel<false, 1, T, 1, false, 7>}},
-                {{sweep_march_tma_kernel<true, 0, T, 0, false, 7>, sweep_march_tma_kernel<true, 0, T, 1, false, 7>},
-                 {sweep_march_tma_kernel<true, 1, T, 0, false, 7>, sweep_march_tma_kernel<true, 1, T, 1, false, 7>}}};
-            kfn = table7[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
-        } else {
-            return 1003;
-        }
+        // WENO7: face-independent coefficients
+        if (a.ftab) return 1003;
+        static const KFn table7[2][2][2] = {
+            {{sweep_march_tma_kernel<false, 0, T, 0, false, 7>, sweep_march_tma_kernel<false, 0, T, 1, false, 7>},
+             {sweep_march_tma_kernel<false, 1, T, 0, false, 7>, sweep_march_tma_kernel<false, 1, T, 1, false, 7>}},
+            {{sweep_march_tma_kernel<true, 0, T, 0, false, 7>, sweep_march_tma_kernel<true, 0, T, 1, false, 7>},
+             {sweep_march_tma_kernel<true, 1, T, 0, false, 7>, sweep_march_tma_kernel<true, 1, T, 1, false, 7>}}};
+        kfn = table7[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     } else if (a.ftab) {
         // face-dependent coefficients: FP64 with TMA input tiles
         if constexpr (sizeof(T) == 8) {
