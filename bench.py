@@ -661,9 +661,11 @@ def measure_families(g, v, stream, K, dev):
     """Every kernel family of the path at 200^3 x 8 (FP64, x/y/z each):
     reshape (s_initialize_weno), order-1 copy, WENO3 / WENO5 / WENO7 with
     JS weights and MP fused, the standalone MP limiter, and WENO5 with TENO
-    weights (teno_CT 1e-5); the harness's per-face coefficient arrays
-    (face-dependent, as s_fill_coefficients makes them) for WENO5, true
-    uniform-grid coefficients for the rest.  ms per three sweeps."""
+    weights (teno_CT 1e-5).  True uniform-grid coefficients go through the
+    face-independent entry (weno_sb_weno_uniform_dev, which the handle API
+    also takes when its coefficient banks are uniform); the harness's
+    coefficient arrays (s_fill_coefficients) through the per-face entry
+    (weno_sb_weno_dev), for WENO5 and WENO7.  ms per three sweeps."""
     import torch
 
     import wenostandalone_b200 as wsb
@@ -689,17 +691,22 @@ def measure_families(g, v, stream, K, dev):
 
     timed("reshape", lambda: [api.reshape(g, d, v, rs[d], stream=sp) for d in range(3)])
     timed("order1_copy", lambda: [api.order1_copy(g, d, v, L, R, stream=sp) for d in range(3)])
+    def face(order, d):
+        return api.face_coefs(fields.uniform_weno_coefficients(order, g.nc(d)))
+
     for order in (3, 5, 7):
-        cf = [coefs(order, d) for d in range(3)]
-        timed(f"weno{order}_js_mp", lambda cf=cf, order=order: [
-            api.weno(g, d, order, v, cf[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
-    hc = [coefs(5, d, harness=True) for d in range(3)]
-    timed("weno5_js_mp_harness_coefficients", lambda: [
-        api.weno(g, d, 5, v, hc[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
+        fc = [face(order, d) for d in range(3)]
+        timed(f"weno{order}_js_mp", lambda fc=fc, order=order: [
+            api.weno_uniform(g, d, order, v, fc[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp)
+            for d in range(3)])
+    for order in (5, 7):
+        hc = [coefs(order, d, harness=True) for d in range(3)]
+        timed(f"weno{order}_js_mp_harness_coefficient_arrays", lambda hc=hc, order=order: [
+            api.weno(g, d, order, v, hc[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
     timed("mp_standalone", lambda: [api.preserve_monotonicity(g, d, rs[d], L, R, stream=sp) for d in range(3)])
-    cf5 = [coefs(5, d) for d in range(3)]
+    fc5 = [face(5, d) for d in range(3)]
     timed("weno5_teno_mp", lambda: [
-        api.weno(gt, d, 5, v, cf5[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
+        api.weno_uniform(gt, d, 5, v, fc5[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
     res["note"] = ("value = face-states/s of the WENO5 face count (3 x 148,135,424) for every family, so "
                    "the rows compare as times; WENO3 writes all ns faces")
     return res

@@ -566,6 +566,63 @@ struct March64 {
         }
         return ok;
     }
+    // WENO5-TENO (+ MP) state of face J (f90:578-606): tau = |beta_2 - beta_0|,
+    // alpha_k = (1 + tau / beta_k)^6, delta_k = [alpha_k / sum alpha >= CT],
+    // weights d_k delta_k / sum d delta; the offsets v - v0 in the folded form
+    // E = sum delta_k (kL_k . differences), S = sum delta_k d_k.  False when a
+    // sum leaves the range of the reciprocal form (the caller redoes the face).
+    template <bool MPF>
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, double& L, double& R) const {
+        const double tau = fabs(b2 - b0);
+        const double t0 = fma(tau, rcp1(b0), 1.0), t1 = fma(tau, rcp1(b1), 1.0), t2 = fma(tau, rcp1(b2), 1.0);
+        const double x0 = t0 * t0, x1 = t1 * t1, x2 = t2 * t2;
+        const double al0 = x0 * x0 * x0, al1 = x1 * x1 * x1, al2 = x2 * x2 * x2;
+        const double s = (al0 + al1) + al2;
+        // s >= 1 (every alpha is); below 2^996 its reciprocal and the
+        // products with it stay normal (NaN and inf fail the test too)
+        const bool s_ok = mid_range_prod(s);
+        const double rs = rcp1(s), ct = a.wp.teno_ct;
+        const bool k0 = !(al0 * rs < ct), k1 = !(al1 * rs < ct), k2 = !(al2 * rs < ct);
+        const double eL0 = fma(a.kL[1], d0, a.kL[0] * dp1), eL1 = fma(a.kL[3], dm1, a.kL[2] * d0),
+                     eL2 = fma(a.kL[5], dm2, a.kL[4] * dm1);
+        const double eR0 = fma(a.kR[1], d0, a.kR[0] * dp1), eR1 = fma(a.kR[3], dm1, a.kR[2] * d0),
+                     eR2 = fma(a.kR[5], dm2, a.kR[4] * dm1);
+        const double EL = ((k0 ? eL0 : 0.0) + (k1 ? eL1 : 0.0)) + (k2 ? eL2 : 0.0);
+        const double ER = ((k0 ? eR0 : 0.0) + (k1 ? eR1 : 0.0)) + (k2 ? eR2 : 0.0);
+        const double SL = ((k0 ? a.ucf[12] : 0.0) + (k1 ? a.ucf[13] : 0.0)) + (k2 ? a.ucf[14] : 0.0);
+        const double SR = ((k0 ? a.ucf[15] : 0.0) + (k1 ? a.ucf[16] : 0.0)) + (k2 ? a.ucf[17] : 0.0);
+        const double p = SL * SR;
+        const bool ok = s_ok && mid_range_prod(p);
+        const double r = rcp1(p);
+        L = fma(EL * SR, r, v0);
+        R = fma(ER * SL, r, v0);
+        if constexpr (MPF) {
+            // the one-sided MP median of face()
+            const double kBetaMP = 4.0 / 3.0;
+            const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
+            {
+                const bool pos = sign_clear(EL);
+                const double UL = fma(-2.0, d0, v0);
+                const double MD = fma(-0.5, dm1 + mA, v0);
+                const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
+                const double Q1 = (pos == up_l) ? v0 : vm1;
+                const double Q2 = (pos == up_r) ? v0 : UL;
+                const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
+                L = mm_sel(mm_sel(L, A, !pos), B, !pos);
+            }
+            {
+                const bool pos = sign_clear(ER);
+                const double UL = fma(2.0, dm1, v0);
+                const double MD = fma(0.5, d0 - mB, v0);
+                const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
+                const double Q1 = (pos == up_r) ? vp1 : v0;
+                const double Q2 = (pos == up_l) ? UL : v0;
+                const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
+                R = mm_sel(mm_sel(R, A, !pos), B, !pos);
+            }
+        }
+        return ok;
+    }
 };
 
 // The reference sequence for one face (cells o+1 .. o+5 of the column).
@@ -732,6 +789,18 @@ __device__ __noinline__ void march64_7_redo(const MarchArgs& a, const double* __
     for (int q = 0; q < 7; ++q) v[q] = __ldg(col + (o + q) * a.sJ);
     weno7_face<double>(v + 3, c, JS, a.wp.eps, 0.0, L, R);
     if (MPF) mp_limit(v[1], v[2], v[3], v[4], v[5], L, R);
+}
+
+// The reference sequence for a TENO face (cells o+1 .. o+5).
+template <bool MPF>
+__device__ __noinline__ void march64_teno_redo(const MarchArgs& a, const double* __restrict__ col, long long o,
+                                               double& L, double& R) {
+    const Coef<5>& c = *reinterpret_cast<const Coef<5>*>(a.ucf);
+    const double* p = col + (o + 1) * a.sJ;
+    const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
+                 vp2 = __ldg(p + 4 * a.sJ);
+    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, TENO, a.wp.eps, a.wp.teno_ct, L, R);
+    if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
 }
 
 // The same for face-dependent coefficients: core face o - 3 of the arrays.

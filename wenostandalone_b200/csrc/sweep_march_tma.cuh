@@ -154,9 +154,10 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col,
 #define WSB_MTMA_MIN_BLOCKS_W7 2  // WENO7 carries ~27 doubles of state: 3 CTAs per SM would spill
 #endif
 // PF: face-dependent coefficients from the per-face table a.ftab (FP64).
-// ORDER 7: the WENO7 engine (FP64, face-independent coefficients); face f
-// reads cells f .. f+6 and pushes cell f+7.
-template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5>
+// ORDER 7: the WENO7 engine (face-independent coefficients); face f reads
+// cells f .. f+6 and pushes cell f+7.  TENO: WENO5 TENO weights (FP64,
+// face-independent coefficients).
+template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5, bool TENO5 = false>
 __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
                                                   : (sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32))
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
     static_assert(ORDER == 5 || (ORDER == 7 && !PF), "WENO7: face-independent coefficients");
+    static_assert(!TENO5 || (ORDER == 5 && sizeof(T) == 8 && !PF), "TENO: FP64 WENO5, face-independent");
     using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
                                       typename MarchEngine<T>::type>;
     constexpr int PUSH0 = ORDER == 7 ? 7 : 6;             // tile position of the cell pushed after face f0
@@ -309,12 +311,16 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
                 ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
+            } else if constexpr (TENO5) {
+                w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
+                ok = w.template face_teno<MPF>(a, L, R);
             } else {
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
                 ok = w.template face<MPF>(a, L, R);
             }
             if (!ok) {
                 if constexpr (ORDER == 7) march7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
+                else if constexpr (TENO5) march64_teno_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
                 else march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
             }
             if (u0 + lane < a.Nu) {
@@ -377,6 +383,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 T L, R;
                 bool ok;
                 if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
+                else if constexpr (TENO5) ok = w.template face_teno<MPF>(a, L, R);
                 else ok = w.template face<MPF>(a, L, R);
                 if (!ok) bad |= 1u << i;
                 Lg[i % G] = L;
@@ -410,6 +417,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     bad &= bad - 1;
                     T L, R;
                     if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
+                    else if constexpr (TENO5) march64_teno_redo<MPF>(a, col, f0 + i, L, R);
                     else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
@@ -457,7 +465,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
 // kernel with per-lane loads.
 template <typename T>
 int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const T* in, T* vL,
-                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms, int order = 5) {
+                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms, int order = 5, bool teno = false) {
     constexpr int ES = (int)sizeof(T);
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return 1003;
@@ -567,7 +575,24 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
         {{sweep_march_tma_kernel<true, 0, T, 0, false>, sweep_march_tma_kernel<true, 0, T, 1, false>},
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
-    if (order == 7) {
+    if (teno) {
+        // WENO5-TENO: FP64, face-independent coefficients
+        if constexpr (sizeof(T) == 8) {
+            if (a.ftab || order != 5) return 1003;
+            static const KFn tablet[2][2][2] = {
+                {{sweep_march_tma_kernel<false, 0, T, 0, false, 5, true>,
+                  sweep_march_tma_kernel<false, 0, T, 1, false, 5, true>},
+                 {sweep_march_tma_kernel<false, 1, T, 0, false, 5, true>,
+                  sweep_march_tma_kernel<false, 1, T, 1, false, 5, true>}},
+                {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, true>,
+                  sweep_march_tma_kernel<true, 0, T, 1, false, 5, true>},
+                 {sweep_march_tma_kernel<true, 1, T, 0, false, 5, true>,
+                  sweep_march_tma_kernel<true, 1, T, 1, false, 5, true>}}};
+            kfn = tablet[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+        } else {
+            return 1003;
+        }
+    } else if (order == 7) {
         // WENO7: face-independent coefficients
         if (a.ftab) return 1003;
         static const KFn table7[2][2][2] = {

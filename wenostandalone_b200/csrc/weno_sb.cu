@@ -332,6 +332,15 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
+    if constexpr (sizeof(T) == 8) {
+        if ((choice == 0 || choice == 3) && ucf && order == 5 && gr->scheme == WENO_SB_TENO &&
+            march_weights_ok(ucf)) {
+            const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
+            int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 5, true);
+            if (rc != WENO_SB_ERR_UNSUPPORTED)
+                return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (TENO)") : rc;
+        }
+    }
     if ((choice == 0 || choice == 3) && ucf && order == 7 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 7)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 7);
         int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 7);
