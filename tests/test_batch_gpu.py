@@ -14,7 +14,7 @@ from gpu_util import from_dev, nan_dev, rel_err, to_dev
 pytestmark = pytest.mark.gpu
 
 
-def _make_blocks(wsb, oracle_mod, n_blocks=14, seed=2024, lo=8, hi=40, vsizes=(2, 3, 5)):
+def _make_blocks(wsb, oracle_mod, n_blocks=14, seed=2024, lo=8, hi=40, vsizes=(2, 3, 5), uniform=False):
     import torch
     from wenostandalone_b200 import api, fields
     from test_parity_gpu import varying_coefficients
@@ -33,7 +33,10 @@ def _make_blocks(wsb, oracle_mod, n_blocks=14, seed=2024, lo=8, hi=40, vsizes=(2
         vf = fields.smooth_jump_field(m, n, p, nv, 6, seed=100 + i)
         if fp32:
             vf = vf.astype(np.float32).astype(np.float64)
-        coefs = varying_coefficients(order, g.nc(d), seed=200 + i)
+        # face-independent coefficients take the marching items (WENO5 / WENO7
+        # JS, WENO5 TENO in FP64); face-varying ones the per-face items
+        coefs = (fields.uniform_weno_coefficients(order, g.nc(d)) if uniform
+                 else varying_coefficients(order, g.nc(d), seed=200 + i))
         rs = oracle_mod.reshape(np.asfortranarray(vf), m, n, p, 6, d)
         Lr, Rr = oracle_mod.order1_copy(np.asfortranarray(vf), m, n, p, 6, d)
         Lr[:] = np.nan
@@ -68,11 +71,12 @@ def _check(entries, checks):
                 assert rel_err(got, ref) <= tol, (g, d, e["order"], fp32)
 
 
-def test_batch_matches_oracle_per_block(oracle_mod):
+@pytest.mark.parametrize("coefficients", ["varying", "uniform"])
+def test_batch_matches_oracle_per_block(oracle_mod, coefficients):
     import torch
     import wenostandalone_b200 as wsb
     from wenostandalone_b200 import api
-    entries, checks = _make_blocks(wsb, oracle_mod)
+    entries, checks = _make_blocks(wsb, oracle_mod, uniform=coefficients == "uniform")
     b = api.Batch(entries)
     try:
         for _ in range(2):

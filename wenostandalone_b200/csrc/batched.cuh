@@ -13,10 +13,21 @@
 // coefficients once for the item and reads its stencil straight from
 // global memory (the tile's columns are contiguous along the sweep for the
 // drop-in layout and for x; L1 serves the overlap of neighbouring faces).
+//
+// Entries whose coefficient arrays are the same on every face (checked when
+// the batch is built) and that a marching engine covers (WENO5 / WENO7 JS,
+// FP64 or FP32-bulk; WENO5 TENO, FP64) take marching items instead: an item
+// is one CTA-width group of columns, each thread marches its own column over
+// the core faces (sweep_march.cuh engines) with the entry's MarchArgs copied
+// to shared memory, so each face costs one new cell and one new difference
+// instead of a full stencil.
 #pragma once
+
+#include <type_traits>
 
 #include "weno_math.cuh"
 #include "sweep_generic.cuh"
+#include "sweep_march.cuh"
 
 namespace wsb {
 
@@ -33,9 +44,68 @@ struct BatchEntry {
     int o_first, nf;    // faces handled
     int n_jt;           // face tiles
     int TJ;             // faces per tile (<= blockDim.x)
-    long long n_groups; // column groups of U columns
+    long long n_groups; // column groups of U columns (marching: of blockDim.x columns)
     long long item0;    // first work item of this entry
+    int march;          // 0: per-face items; 1 + k: marching items with MarchArgs k of the batch
 };
+
+// One marching item: thread t marches column cg * blockDim.x + t over the
+// core faces 3 .. ns-4 (cells o+1 .. o+5 for WENO5, o .. o+6 for WENO7).
+template <typename T, int ORDER, bool TENO5, bool MPF>
+__device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry& e, long long cg) {
+    using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
+                                      std::conditional_t<sizeof(T) == 8, March64, March32>>;
+    const long long col = cg * blockDim.x + threadIdx.x;
+    if (col >= e.g.cols) return;
+    const long long ca = col % e.g.c1, t = col / e.g.c1;
+    const long long cb = t % e.g.c2, cv = t / e.g.c2;
+    const T* __restrict__ cp = (const T*)e.in + e.g.in_off + ca * e.g.sA + cb * e.g.sB + cv * e.g.sV;
+    const long long sJ = e.g.sJ;
+    T* __restrict__ oL = (T*)e.vL + e.g.ns * col;
+    T* __restrict__ oR = (T*)e.vR + e.g.ns * col;
+    auto ld = [&](long long J) { return __ldg(cp + J * sJ); };
+    const long long o0 = 3, o1 = e.g.ns - 3;
+    constexpr int PUSH = ORDER == 7 ? 7 : 6;  // cell pushed after face o: o + PUSH (at most ns + 2)
+    Engine w;
+    if constexpr (ORDER == 7) w.init(a, ld(o0), ld(o0 + 1), ld(o0 + 2), ld(o0 + 3), ld(o0 + 4), ld(o0 + 5), ld(o0 + 6));
+    else w.init(a, ld(o0 + 1), ld(o0 + 2), ld(o0 + 3), ld(o0 + 4), ld(o0 + 5));
+    for (long long o = o0; o < o1; ++o) {
+        const T n = ld(o + PUSH);
+        T L, R;
+        bool ok;
+        if constexpr (TENO5) ok = w.template face_teno<MPF>(a, L, R);
+        else ok = w.template face<MPF>(a, L, R);
+        if (!ok) {
+            if constexpr (ORDER == 7) {
+                if constexpr (sizeof(T) == 8) march64_7_redo<MPF>(a, cp, o, L, R);
+                else march32_7_redo<MPF>(a, cp, o, L, R);
+            } else if constexpr (TENO5) {
+                march64_teno_redo<MPF>(a, cp, o, L, R);
+            } else if constexpr (sizeof(T) == 8) {
+                march64_redo<MPF>(a, cp, o, L, R);
+            } else {
+                march32_redo<MPF>(a, cp, o, L, R);
+            }
+        }
+        oL[o] = L;
+        oR[o] = R;
+        w.push(a, n);
+    }
+}
+
+template <bool MPF>
+__device__ __forceinline__ void batch_march_dispatch(const MarchArgs& a, const BatchEntry& e, long long cg) {
+    if (e.fp32) {
+        if (e.order == 7) batch_march<float, 7, false, MPF>(a, e, cg);
+        else batch_march<float, 5, false, MPF>(a, e, cg);
+    } else if (e.order == 7) {
+        batch_march<double, 7, false, MPF>(a, e, cg);
+    } else if (e.wp.scheme == TENO) {
+        batch_march<double, 5, true, MPF>(a, e, cg);
+    } else {
+        batch_march<double, 5, false, MPF>(a, e, cg);
+    }
+}
 
 template <int ORDER, typename T>
 __device__ __forceinline__ void batch_item(const BatchEntry& e, long long grp, int jt, int U) {
@@ -99,9 +169,11 @@ __device__ __forceinline__ void batch_item(const BatchEntry& e, long long grp, i
 #endif
 __global__ void __launch_bounds__(256, WSB_BATCH_MIN_BLOCKS)
     batch_kernel(const BatchEntry* __restrict__ entries, int n_entries, long long n_items,
-                 unsigned long long* __restrict__ counter, int U) {
+                 unsigned long long* __restrict__ counter, int U, const MarchArgs* __restrict__ margs) {
     __shared__ long long s_item;
     __shared__ int s_entry;
+    __shared__ MarchArgs s_ma;   // marching items: the entry's arguments
+    int ma_loaded = -1;          // index of the MarchArgs in s_ma (same on every thread)
     while (true) {
         if (threadIdx.x == 0) {
             const long long it = (long long)atomicAdd(counter, 1ull);
@@ -124,6 +196,20 @@ __global__ void __launch_bounds__(256, WSB_BATCH_MIN_BLOCKS)
         if (it >= n_items) break;
         const BatchEntry& e = entries[ei];
         const long long local = it - e.item0;
+        if (e.march) {
+            const int k = e.march - 1;
+            if (k != ma_loaded) {
+                // every thread reaches this branch (the entry is the CTA's)
+                const unsigned* src = reinterpret_cast<const unsigned*>(margs + k);
+                unsigned* dst = reinterpret_cast<unsigned*>(&s_ma);
+                for (int q = threadIdx.x; q < (int)(sizeof(MarchArgs) / 4); q += blockDim.x) dst[q] = __ldg(src + q);
+                ma_loaded = k;
+                __syncthreads();
+            }
+            if (e.mp) batch_march_dispatch<true>(s_ma, e, local);
+            else batch_march_dispatch<false>(s_ma, e, local);
+            continue;
+        }
         const int jt = (int)(local % e.n_jt);
         const long long grp = local / e.n_jt;
         if (e.fp32) {

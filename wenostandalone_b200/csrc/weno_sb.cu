@@ -447,6 +447,8 @@ struct Batch {
     std::vector<weno_sb_block> blocks;
     std::vector<BatchEntry> entries;
     BatchEntry* d_entries = nullptr;
+    std::vector<MarchArgs> margs;     // marching entries' arguments (BatchEntry::march - 1)
+    MarchArgs* d_margs = nullptr;
     unsigned long long* d_counter = nullptr;
     long long n_items = 0;
     int threads = 128;  // face-tile width = CTA size
@@ -482,8 +484,8 @@ int batch_layout(Batch* B, int threads, int U) {
     long long item = 0;
     for (auto& e : B->entries) {
         e.TJ = threads;
-        e.n_jt = (e.nf + threads - 1) / threads;
-        e.n_groups = (e.g.cols + U - 1) / U;
+        e.n_jt = e.march ? 1 : (e.nf + threads - 1) / threads;
+        e.n_groups = e.march ? (e.g.cols + threads - 1) / threads : (e.g.cols + U - 1) / U;
         e.item0 = item;
         item += (long long)e.n_jt * e.n_groups;
     }
@@ -501,7 +503,7 @@ int batch_layout(Batch* B, int threads, int U) {
 int batch_enqueue(Batch* B, cudaStream_t st) {
     WSB_CUDA(cudaMemsetAsync(B->d_counter, 0, sizeof(unsigned long long), st));
     batch_kernel<<<B->grid, B->threads, 0, st>>>(B->d_entries, (int)B->entries.size(), B->n_items, B->d_counter,
-                                                 B->U);
+                                                 B->U, B->d_margs);
     return cuda_err(cudaGetLastError(), "batch launch");
 }
 
@@ -1017,6 +1019,48 @@ int weno_sb_checksum_noalloc(int dtype, const void* const* arrays, const int64_t
     return cuda_err(cudaGetLastError(), "checksum (no-alloc) launch");
 }
 
+// Face-independent coefficients of a batch block: reads its coefficient
+// arrays back once (batch set-up) and, when every face holds face 0's
+// values, writes them in the Coef<order> layout.  False otherwise.
+bool batch_coefs_uniform(const weno_sb_coefs& cf, long long nc, int order, double* ucf) {
+    if (nc < 1) return false;
+    std::vector<double> pL(nc * 15), pR(nc * 15), dL(5 * nc), dR(5 * nc), bc(nc * 30);
+    if (cudaMemcpy(pL.data(), cf.polyL, sizeof(double) * pL.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(pR.data(), cf.polyR, sizeof(double) * pR.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(dL.data(), cf.dL, sizeof(double) * dL.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(dR.data(), cf.dR, sizeof(double) * dR.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(bc.data(), cf.beta_coef, sizeof(double) * bc.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    // (nc, 5, S) arrays: face c of column (r, s) at c + nc (r + 5 s); (5, nc): r + 5 c
+    auto same_cols = [&](const std::vector<double>& a, int S) {
+        for (int k = 0; k < 5 * S; ++k)
+            for (long long c = 1; c < nc; ++c)
+                if (a[c + nc * k] != a[nc * k]) return false;
+        return true;
+    };
+    auto same_rows = [&](const std::vector<double>& a) {
+        for (long long c = 1; c < nc; ++c)
+            for (int r = 0; r < 5; ++r)
+                if (a[r + 5 * c] != a[r]) return false;
+        return true;
+    };
+    if (!same_cols(pL, 3) || !same_cols(pR, 3) || !same_cols(bc, 6) || !same_rows(dL) || !same_rows(dR)) return false;
+    weno_sb_face_coefs f{};
+    for (int r = 0; r < 5; ++r) {
+        for (int q = 0; q < 3; ++q) {
+            f.polyL[q][r] = pL[nc * (r + 5 * q)];
+            f.polyR[q][r] = pR[nc * (r + 5 * q)];
+        }
+        for (int q = 0; q < 6; ++q) f.beta_coef[q][r] = bc[nc * (r + 5 * q)];
+        f.dL[r] = dL[r];
+        f.dR[r] = dR[r];
+    }
+    build_ucf(order, &f, ucf);
+    return true;
+}
+
 int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
     WSB_FAULT("init");
     if (!blocks || n < 1 || !batch) return set_err(WENO_SB_ERR_ARG, "need at least one block and a batch pointer");
@@ -1051,16 +1095,34 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
         e.fp32 = b.dtype == WENO_SB_FP32;
         e.o_first = (b.order == 3) ? 0 : 3;
         e.nf = (int)((b.order == 3) ? e.g.ns : e.g.nc);
+        // marching items for the orders and weights a marching engine covers,
+        // when the block's coefficients are the same on every face
+        const bool js = b.grid.scheme == WENO_SB_JS;
+        const bool teno5 = b.grid.scheme == WENO_SB_TENO && b.order == 5 && b.dtype == WENO_SB_FP64;
+        double ucf[56];
+        if (kernel_choice() != 1 && (b.order == 5 || b.order == 7) && (js || teno5) &&
+            batch_coefs_uniform(b.coefs, e.g.nc, b.order, ucf) && march_weights_ok(ucf, b.order)) {
+            B->margs.push_back(make_march_args(e.g, b.v_in, b.vL, b.vR, e.wp, ucf, b.order));
+            e.march = (int)B->margs.size();
+        }
         B->blocks.push_back(b);
         B->entries.push_back(e);
     }
     int rc = cuda_err(cudaMalloc((void**)&B->d_entries, sizeof(BatchEntry) * n), "cudaMalloc");
     if (!rc) rc = cuda_err(cudaMalloc((void**)&B->d_counter, sizeof(unsigned long long)), "cudaMalloc");
+    if (!rc && !B->margs.empty()) {
+        rc = cuda_err(cudaMalloc((void**)&B->d_margs, sizeof(MarchArgs) * B->margs.size()), "cudaMalloc");
+        if (!rc)
+            rc = cuda_err(cudaMemcpy(B->d_margs, B->margs.data(), sizeof(MarchArgs) * B->margs.size(),
+                                     cudaMemcpyHostToDevice),
+                          "cudaMemcpy");
+    }
     if (!rc) rc = cuda_err(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!rc) rc = batch_layout(B, 128, 8);
     if (rc) {
         if (B->d_entries) cudaFree(B->d_entries);
         if (B->d_counter) cudaFree(B->d_counter);
+        if (B->d_margs) cudaFree(B->d_margs);
         if (B->cap) cudaStreamDestroy(B->cap);
         delete B;
         return rc;
@@ -1157,6 +1219,7 @@ int weno_sb_batch_destroy(int batch) {
     batch_release_graph(B);
     cudaFree(B->d_entries);
     cudaFree(B->d_counter);
+    if (B->d_margs) cudaFree(B->d_margs);
     cudaStreamDestroy(B->cap);
     {
         std::lock_guard<std::mutex> lk(g_batch_mu);
