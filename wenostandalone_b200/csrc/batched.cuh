@@ -15,8 +15,8 @@
 // drop-in layout and for x; L1 serves the overlap of neighbouring faces).
 //
 // Entries whose coefficient arrays are the same on every face (checked when
-// the batch is built) and that a marching engine covers (WENO5 / WENO7 JS,
-// FP64 or FP32-bulk; WENO5 TENO, FP64) take marching items instead: an item
+// the batch is built) and that a marching engine covers (WENO5 / WENO7 with
+// JS or TENO weights, FP64 or FP32-bulk) take marching items instead: an item
 // is one CTA-width group of columns, each thread marches its own column over
 // the core faces (sweep_march.cuh engines) with the entry's MarchArgs copied
 // to shared memory, so each face costs one new cell and one new difference
@@ -51,7 +51,7 @@ struct BatchEntry {
 
 // One marching item: thread t marches column cg * blockDim.x + t over the
 // core faces 3 .. ns-4 (cells o+1 .. o+5 for WENO5, o .. o+6 for WENO7).
-template <typename T, int ORDER, bool TENO5, bool MPF>
+template <typename T, int ORDER, bool TENOW, bool MPF>
 __device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry& e, long long cg) {
     using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
                                       std::conditional_t<sizeof(T) == 8, March64, March32>>;
@@ -73,14 +73,12 @@ __device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry
         const T n = ld(o + PUSH);
         T L, R;
         bool ok;
-        if constexpr (TENO5) ok = w.template face_teno<MPF>(a, L, R);
+        if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
         else ok = w.template face<MPF>(a, L, R);
         if (!ok) {
             if constexpr (ORDER == 7) {
                 if constexpr (sizeof(T) == 8) march64_7_redo<MPF>(a, cp, o, L, R);
                 else march32_7_redo<MPF>(a, cp, o, L, R);
-            } else if constexpr (TENO5) {
-                march64_teno_redo<MPF>(a, cp, o, L, R);
             } else if constexpr (sizeof(T) == 8) {
                 march64_redo<MPF>(a, cp, o, L, R);
             } else {
@@ -95,15 +93,22 @@ __device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry
 
 template <bool MPF>
 __device__ __forceinline__ void batch_march_dispatch(const MarchArgs& a, const BatchEntry& e, long long cg) {
+    // (the redo sequences take the weights from the arguments)
+    const bool teno = e.wp.scheme == TENO;
     if (e.fp32) {
-        if (e.order == 7) batch_march<float, 7, false, MPF>(a, e, cg);
-        else batch_march<float, 5, false, MPF>(a, e, cg);
+        if (e.order == 7) {
+            if (teno) batch_march<float, 7, true, MPF>(a, e, cg);
+            else batch_march<float, 7, false, MPF>(a, e, cg);
+        } else {
+            if (teno) batch_march<float, 5, true, MPF>(a, e, cg);
+            else batch_march<float, 5, false, MPF>(a, e, cg);
+        }
     } else if (e.order == 7) {
-        batch_march<double, 7, false, MPF>(a, e, cg);
-    } else if (e.wp.scheme == TENO) {
-        batch_march<double, 5, true, MPF>(a, e, cg);
+        if (teno) batch_march<double, 7, true, MPF>(a, e, cg);
+        else batch_march<double, 7, false, MPF>(a, e, cg);
     } else {
-        batch_march<double, 5, false, MPF>(a, e, cg);
+        if (teno) batch_march<double, 5, true, MPF>(a, e, cg);
+        else batch_march<double, 5, false, MPF>(a, e, cg);
     }
 }
 

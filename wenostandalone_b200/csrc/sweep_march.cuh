@@ -442,6 +442,88 @@ __device__ __forceinline__ double rcp1(double s) {
     return fma(r, fma(-s, r, 1.0), r);
 }
 
+// One-sided MP median of an FP64 engine's face (see March64::face), with the
+// side of each state given by the sign of its offset from v0.
+__device__ __forceinline__ void mp64_sided(double vm1, double v0, double vp1, double dm1, double d0, double mA,
+                                           double mB, bool posL, bool posR, double& L, double& R) {
+    const double kBetaMP = 4.0 / 3.0;
+    const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
+    {
+        const bool pos = posL;
+        const double UL = fma(-2.0, d0, v0);
+        const double MD = fma(-0.5, dm1 + mA, v0);
+        const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
+        const double Q1 = (pos == up_l) ? v0 : vm1;
+        const double Q2 = (pos == up_r) ? v0 : UL;
+        const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
+        L = mm_sel(mm_sel(L, A, !pos), B, !pos);
+    }
+    {
+        const bool pos = posR;
+        const double UL = fma(2.0, dm1, v0);
+        const double MD = fma(0.5, d0 - mB, v0);
+        const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
+        const double Q1 = (pos == up_r) ? vp1 : v0;
+        const double Q2 = (pos == up_l) ? UL : v0;
+        const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
+        R = mm_sel(mm_sel(R, A, !pos), B, !pos);
+    }
+}
+
+// The same in FP32 offset space (see March32::face): x = state - v0, with
+// b = v0 - vm1 = fm1 and c = vp1 - v0 = f0.
+__device__ __forceinline__ void mp32_sided(float fm1, float f0, float mA, float mB, float& xL, float& xR) {
+    const float kB = 4.0f / 3.0f;
+    {
+        const bool pos = xL >= 0.0f;
+        const float md = -0.5f * (fm1 + mA), ul = -2.0f * f0, lc = fmaf(kB, mB, -0.5f * f0), nb = -fm1;
+        const float A = pos ? fmaxf(fmaxf(0.0f, nb), md) : fminf(fminf(0.0f, nb), md);
+        const float B = pos ? fmaxf(fmaxf(0.0f, ul), lc) : fminf(fminf(0.0f, ul), lc);
+        xL = pos ? fminf(fminf(xL, A), B) : fmaxf(fmaxf(xL, A), B);
+    }
+    {
+        const bool pos = xR >= 0.0f;
+        const float md = -0.5f * (mB - f0), ul = 2.0f * fm1, lc = fmaf(kB, mA, 0.5f * fm1), nb = f0;
+        const float A = pos ? fmaxf(fmaxf(0.0f, nb), md) : fminf(fminf(0.0f, nb), md);
+        const float B = pos ? fmaxf(fmaxf(0.0f, ul), lc) : fminf(fminf(0.0f, ul), lc);
+        xR = pos ? fminf(fminf(xR, A), B) : fmaxf(fmaxf(xR, A), B);
+    }
+}
+
+// TENO weights of WENO5 (f90:578-606) for betas b0..b2: the cutoff flags
+// (alpha_k / sum alpha >= CT, alpha_k = (1 + tau / beta_k)^6,
+// tau = |beta_2 - beta_0|); false when the alpha sum leaves [1, 2^996)
+// (a zero beta, or ratios past 10^50).
+__device__ __forceinline__ bool teno5_keep(double b0, double b1, double b2, double ct, bool& k0, bool& k1, bool& k2) {
+    const double tau = fabs(b2 - b0);
+    const double t0 = fma(tau, rcp1(b0), 1.0), t1 = fma(tau, rcp1(b1), 1.0), t2 = fma(tau, rcp1(b2), 1.0);
+    const double x0 = t0 * t0, x1 = t1 * t1, x2 = t2 * t2;
+    const double al0 = x0 * x0 * x0, al1 = x1 * x1 * x1, al2 = x2 * x2 * x2;
+    const double s = (al0 + al1) + al2;
+    const double rs = rcp1(s);
+    k0 = !(al0 * rs < ct); k1 = !(al1 * rs < ct); k2 = !(al2 * rs < ct);
+    return mid_range_prod(s);
+}
+
+// TENO weights of WENO7 as the reference writes them (f90:1491-1506):
+// beta(4) = eps, tau = |beta(4) - beta(3)|, alpha_q = (1 + tau / beta_q)^6 for
+// q = 0..4, cutoff flags for q = 0..3, and alpha(4) kept in the final sums
+// (returned in a4).  False when the sums leave the reciprocal form's range.
+__device__ __forceinline__ bool teno7_keep(double b0, double b1, double b2, double b3, double eps, double ct, bool& k0,
+                                           bool& k1, bool& k2, bool& k3, double& a4) {
+    const double tau = fabs(eps - b3);
+    const double t0 = fma(tau, rcp1(b0), 1.0), t1 = fma(tau, rcp1(b1), 1.0), t2 = fma(tau, rcp1(b2), 1.0),
+                 t3 = fma(tau, rcp1(b3), 1.0), t4 = fma(tau, rcp1(eps), 1.0);
+    const double x0 = t0 * t0, x1 = t1 * t1, x2 = t2 * t2, x3 = t3 * t3, x4 = t4 * t4;
+    const double al0 = x0 * x0 * x0, al1 = x1 * x1 * x1, al2 = x2 * x2 * x2, al3 = x3 * x3 * x3;
+    a4 = x4 * x4 * x4;
+    const double s = ((al0 + al1) + (al2 + al3)) + a4;
+    const double rs = rcp1(s);
+    k0 = !(al0 * rs < ct); k1 = !(al1 * rs < ct); k2 = !(al2 * rs < ct); k3 = !(al3 * rs < ct);
+    // a4 >= 1; (S + a4)^2 must stay below 2^996 for the final reciprocal
+    return mid_range_prod(s) && mid_range(a4);
+}
+
 struct March64 {
     double vm1, v0, vp1, vp2;   // cells J-1 .. J+2
     double dm2, dm1, d0, dp1;   // d[k] = v[k+1] - v[k], k = J-2 .. J+1
@@ -645,7 +727,7 @@ __device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __re
     const double* p = col + (o + 1) * a.sJ;
     const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
                  vp2 = __ldg(p + 4 * a.sJ);
-    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, JS, a.wp.eps, 0.0, L, R);
+    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, a.wp.scheme, a.wp.eps, a.wp.teno_ct, L, R);
     if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
 }
 
@@ -666,7 +748,7 @@ struct March64_7 {
     double vm1, v0, vp1, vp2, vp3;        // cells J-1 .. J+3
     double dm3, dm2, dm1, d0, dp1, dp2;    // d[k] = v[k+1] - v[k], k = J-3 .. J+2
     double s1, s2, c12;                    // d[J+1]^2, d[J+2]^2, d[J+1] d[J+2]
-    double q0, q1, q2, q3;                 // beta_s(J)^2
+    double B0, B1, B2, B3;                 // beta_s(J)
     double n0a, n0b, n0c, n1a, n1b, n2a;   // beta_0(J+1 .. J+3), beta_1(J+1 .. J+2), beta_2(J+1)
     double e2, mA, mB;                     // d[J+1] - d[J]; minmods of the MP limiter
 
@@ -698,7 +780,7 @@ struct March64_7 {
         n2a = beta_row(a, 1, d0, dp1, dp2);
         n1b = beta_row(a, 2, d0, dp1, dp2);
         n0c = beta_row(a, 3, d0, dp1, dp2);
-        q0 = b0 * b0; q1 = b1 * b1; q2 = b2 * b2; q3 = b3 * b3;
+        B0 = b0; B1 = b1; B2 = b2; B3 = b3;
         const double em = dm1 - dm2, ez = d0 - dm1;
         e2 = dp1 - d0;
         mA = mm64(em, ez);
@@ -713,7 +795,7 @@ struct March64_7 {
         const double g1 = beta_row(a, 1, aa, ab, ae, s2, c12, s1);
         const double g2 = beta_row(a, 2, aa, ab, ae, s2, c12, s1);
         const double g3 = beta_row(a, 3, aa, ab, ae, s2, c12, s1);
-        q0 = n0a * n0a; q1 = n1a * n1a; q2 = n2a * n2a; q3 = g0 * g0;
+        B0 = n0a; B1 = n1a; B2 = n2a; B3 = g0;
         n0a = n0b; n0b = n0c; n0c = g3;
         n1a = n1b; n1b = g2;
         n2a = g1;
@@ -729,6 +811,7 @@ struct March64_7 {
     // out of range (the caller redoes the face).
     template <bool MPF>
     __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+        const double q0 = B0 * B0, q1 = B1 * B1, q2 = B2 * B2, q3 = B3 * B3;
         const double q01 = q0 * q1, q23 = q2 * q3;
         const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
         const double SL = fma(a.ucf[24], P0, fma(a.ucf[25], P1, fma(a.ucf[26], P2, a.ucf[27] * P3)));
@@ -777,8 +860,36 @@ struct March64_7 {
         }
         return ok;
     }
+    // WENO7-TENO (+ MP) state of face J, with the reference's alpha(4) in the
+    // sums (teno7_keep): L = (S_L v0 + E_L) / (S_L + alpha4), S_L = sum delta d,
+    // E_L = sum delta (kL . differences).
+    template <bool MPF>
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, double& L, double& R) const {
+        bool k0, k1, k2, k3;
+        double a4;
+        const bool ok0 = teno7_keep(B0, B1, B2, B3, a.wp.eps, a.wp.teno_ct, k0, k1, k2, k3, a4);
+        const double eL0 = fma(a.kL7[0], dm1, fma(a.kL7[1], dm2, a.kL7[2] * dm3));
+        const double eL1 = fma(a.kL7[3], d0, fma(a.kL7[4], dm1, a.kL7[5] * dm2));
+        const double eL2 = fma(a.kL7[6], dp1, fma(a.kL7[7], d0, a.kL7[8] * dm1));
+        const double eL3 = fma(a.kL7[9], dp2, fma(a.kL7[10], dp1, a.kL7[11] * d0));
+        const double eR0 = fma(a.kR7[0], dm1, fma(a.kR7[1], dm2, a.kR7[2] * dm3));
+        const double eR1 = fma(a.kR7[3], d0, fma(a.kR7[4], dm1, a.kR7[5] * dm2));
+        const double eR2 = fma(a.kR7[6], dp1, fma(a.kR7[7], d0, a.kR7[8] * dm1));
+        const double eR3 = fma(a.kR7[9], dp2, fma(a.kR7[10], dp1, a.kR7[11] * d0));
+        const double EL = ((k0 ? eL0 : 0.0) + (k1 ? eL1 : 0.0)) + ((k2 ? eL2 : 0.0) + (k3 ? eL3 : 0.0));
+        const double ER = ((k0 ? eR0 : 0.0) + (k1 ? eR1 : 0.0)) + ((k2 ? eR2 : 0.0) + (k3 ? eR3 : 0.0));
+        const double SL = ((k0 ? a.ucf[24] : 0.0) + (k1 ? a.ucf[25] : 0.0)) + ((k2 ? a.ucf[26] : 0.0) + (k3 ? a.ucf[27] : 0.0));
+        const double SR = ((k0 ? a.ucf[28] : 0.0) + (k1 ? a.ucf[29] : 0.0)) + ((k2 ? a.ucf[30] : 0.0) + (k3 ? a.ucf[31] : 0.0));
+        const double DL = SL + a4, DR = SR + a4;
+        const double p = DL * DR;
+        const bool ok = ok0 && mid_range_prod(p);
+        const double r = rcp1(p);
+        L = fma(SL, v0, EL) * (DR * r);
+        R = fma(SR, v0, ER) * (DL * r);
+        if constexpr (MPF) mp64_sided(vm1, v0, vp1, dm1, d0, mA, mB, sign_clear(L - v0), sign_clear(R - v0), L, R);
+        return ok;
+    }
 };
-
 // The reference sequence for one WENO7 face (cells o .. o+6 of the column).
 template <bool MPF>
 __device__ __noinline__ void march64_7_redo(const MarchArgs& a, const double* __restrict__ col, long long o,
@@ -787,20 +898,8 @@ __device__ __noinline__ void march64_7_redo(const MarchArgs& a, const double* __
     double v[7];
 #pragma unroll
     for (int q = 0; q < 7; ++q) v[q] = __ldg(col + (o + q) * a.sJ);
-    weno7_face<double>(v + 3, c, JS, a.wp.eps, 0.0, L, R);
+    weno7_face<double>(v + 3, c, a.wp.scheme, a.wp.eps, a.wp.teno_ct, L, R);
     if (MPF) mp_limit(v[1], v[2], v[3], v[4], v[5], L, R);
-}
-
-// The reference sequence for a TENO face (cells o+1 .. o+5).
-template <bool MPF>
-__device__ __noinline__ void march64_teno_redo(const MarchArgs& a, const double* __restrict__ col, long long o,
-                                               double& L, double& R) {
-    const Coef<5>& c = *reinterpret_cast<const Coef<5>*>(a.ucf);
-    const double* p = col + (o + 1) * a.sJ;
-    const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
-                 vp2 = __ldg(p + 4 * a.sJ);
-    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, TENO, a.wp.eps, a.wp.teno_ct, L, R);
-    if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
 }
 
 // The same for face-dependent coefficients: core face o - 3 of the arrays.
@@ -931,8 +1030,31 @@ struct March32 {
         R = v0 + xR;
         return ok;
     }
+    // FP32-bulk WENO5-TENO: flags and weights d_k delta_k / S from the FP64
+    // betas (teno5_keep), candidates and MP in FP32 (pivot on stencil 1).
+    template <bool MPF>
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, float& L, float& R) const {
+        bool k0, k1, k2;
+        const bool ok0 = teno5_keep(b0, b1, b2, a.wp.teno_ct, k0, k1, k2);
+        const double aL0 = k0 ? a.ucf[12] : 0.0, aL1 = k1 ? a.ucf[13] : 0.0, aL2 = k2 ? a.ucf[14] : 0.0;
+        const double aR0 = k0 ? a.ucf[15] : 0.0, aR1 = k1 ? a.ucf[16] : 0.0, aR2 = k2 ? a.ucf[17] : 0.0;
+        const double SL = (aL0 + aL1) + aL2, SR = (aR0 + aR1) + aR2;
+        const double p = SL * SR;
+        const bool ok = ok0 && mid_range_prod(p);
+        const double r = rcp1(p), gL = SR * r, gR = SL * r;
+        const float wL0 = __double2float_rn(aL0 * gL), wL2 = __double2float_rn(aL2 * gL),
+                    wR0 = __double2float_rn(aR0 * gR), wR2 = __double2float_rn(aR2 * gR);
+        const float eL0 = fmaf(a.pf2[0].x, fp1, a.pf2[1].x * f0), eR0 = fmaf(a.pf2[0].y, fp1, a.pf2[1].y * f0);
+        const float eL1 = fmaf(a.pf2[2].x, f0, a.pf2[3].x * fm1), eR1 = fmaf(a.pf2[2].y, f0, a.pf2[3].y * fm1);
+        const float eL2 = fmaf(a.pf2[4].x, fm1, a.pf2[5].x * fm2), eR2 = fmaf(a.pf2[4].y, fm1, a.pf2[5].y * fm2);
+        float xL = fmaf(wL0, eL0 - eL1, fmaf(wL2, eL2 - eL1, eL1));
+        float xR = fmaf(wR0, eR0 - eR1, fmaf(wR2, eR2 - eR1, eR1));
+        if constexpr (MPF) mp32_sided(fm1, f0, mA, mB, xL, xR);
+        L = v0 + xL;
+        R = v0 + xR;
+        return ok;
+    }
 };
-
 // The reference sequence for one FP32-bulk face (cells o+1 .. o+5).
 template <bool MPF>
 __device__ __noinline__ void march32_redo(const MarchArgs& a, const float* __restrict__ col, long long o, float& L,
@@ -954,8 +1076,8 @@ __device__ __noinline__ void march32_redo(const MarchArgs& a, const float* __res
     const float vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
                 vp2 = __ldg(p + 4 * a.sJ);
     double Ld, Rd;
-    weno5_face<float>(f2d_bits(vm2), f2d_bits(vm1), f2d_bits(v0), f2d_bits(vp1), f2d_bits(vp2), c, JS, a.wp.eps, 0.0,
-                      Ld, Rd);
+    weno5_face<float>(f2d_bits(vm2), f2d_bits(vm1), f2d_bits(v0), f2d_bits(vp1), f2d_bits(vp2), c, a.wp.scheme,
+                      a.wp.eps, a.wp.teno_ct, Ld, Rd);
     L = (float)Ld;
     R = (float)Rd;
     if (MPF) MP<float>::apply(vm2, vm1, v0, vp1, vp2, L, R);
@@ -972,7 +1094,7 @@ struct March32_7 {
     float fm3, fm2, fm1, f0, fp1, fp2;      // FP32 differences, k = J-3 .. J+2
     double Dp3;                             // vp3, widened
     double dp1, dp2, s1, s2, c12;           // FP64 d[J+1], d[J+2], their squares and product
-    double q0, q1, q2, q3;                  // beta_s(J)^2
+    double B0, B1, B2, B3;                  // beta_s(J)
     double n0a, n0b, n0c, n1a, n1b, n2a;    // as March64_7
     float e2, mA, mB;
 
@@ -995,7 +1117,7 @@ struct March32_7 {
         n2a = March64_7::beta_row(a, 1, d0, dp1, dp2);
         n1b = March64_7::beta_row(a, 2, d0, dp1, dp2);
         n0c = March64_7::beta_row(a, 3, d0, dp1, dp2);
-        q0 = b0 * b0; q1 = b1 * b1; q2 = b2 * b2; q3 = b3 * b3;
+        B0 = b0; B1 = b1; B2 = b2; B3 = b3;
         const float em = fm1 - fm2, ez = f0 - fm1;
         e2 = fp1 - f0;
         mA = mm32(em, ez);
@@ -1010,7 +1132,7 @@ struct March32_7 {
         const double g1 = March64_7::beta_row(a, 1, aa, ab, ae, s2, c12, s1);
         const double g2 = March64_7::beta_row(a, 2, aa, ab, ae, s2, c12, s1);
         const double g3 = March64_7::beta_row(a, 3, aa, ab, ae, s2, c12, s1);
-        q0 = n0a * n0a; q1 = n1a * n1a; q2 = n2a * n2a; q3 = g0 * g0;
+        B0 = n0a; B1 = n1a; B2 = n2a; B3 = g0;
         n0a = n0b; n0b = n0c; n0c = g3;
         n1a = n1b; n1b = g2;
         n2a = g1;
@@ -1026,6 +1148,7 @@ struct March32_7 {
 
     template <bool MPF>
     __device__ __forceinline__ bool face(const MarchArgs& a, float& L, float& R) const {
+        const double q0 = B0 * B0, q1 = B1 * B1, q2 = B2 * B2, q3 = B3 * B3;
         const double q01 = q0 * q1, q23 = q2 * q3;
         const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
         const double aL0 = a.ucf[24] * P0, aL2 = a.ucf[26] * P2, aL3 = a.ucf[27] * P3;
@@ -1071,8 +1194,48 @@ struct March32_7 {
         R = v0 + xR;
         return ok;
     }
+    // FP32-bulk WENO7-TENO with the reference's alpha(4) (teno7_keep): the
+    // state is W v0 + sum w_s e_s with W = S / (S + alpha4), w_s = delta_s d_s /
+    // (S + alpha4) from FP64, candidates and MP in FP32.
+    template <bool MPF>
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, float& L, float& R) const {
+        bool k0, k1, k2, k3;
+        double a4;
+        const bool ok0 = teno7_keep(B0, B1, B2, B3, a.wp.eps, a.wp.teno_ct, k0, k1, k2, k3, a4);
+        const double aL0 = k0 ? a.ucf[24] : 0.0, aL1 = k1 ? a.ucf[25] : 0.0, aL2 = k2 ? a.ucf[26] : 0.0,
+                     aL3 = k3 ? a.ucf[27] : 0.0;
+        const double aR0 = k0 ? a.ucf[28] : 0.0, aR1 = k1 ? a.ucf[29] : 0.0, aR2 = k2 ? a.ucf[30] : 0.0,
+                     aR3 = k3 ? a.ucf[31] : 0.0;
+        const double SL = (aL0 + aL1) + (aL2 + aL3), SR = (aR0 + aR1) + (aR2 + aR3);
+        const double DL = SL + a4, DR = SR + a4;
+        const double p = DL * DR;
+        const bool ok = ok0 && mid_range_prod(p);
+        const double r = rcp1(p), gL = DR * r, gR = DL * r;
+        const float wL0 = __double2float_rn(aL0 * gL), wL1 = __double2float_rn(aL1 * gL),
+                    wL2 = __double2float_rn(aL2 * gL), wL3 = __double2float_rn(aL3 * gL),
+                    WL = __double2float_rn(SL * gL);
+        const float wR0 = __double2float_rn(aR0 * gR), wR1 = __double2float_rn(aR1 * gR),
+                    wR2 = __double2float_rn(aR2 * gR), wR3 = __double2float_rn(aR3 * gR),
+                    WR = __double2float_rn(SR * gR);
+        const float eL0 = fmaf(a.pf7[9], fm1, fmaf(a.pf7[10], fm2, a.pf7[11] * fm3));
+        const float eL1 = fmaf(a.pf7[6], f0, fmaf(a.pf7[7], fm1, a.pf7[8] * fm2));
+        const float eL2 = fmaf(a.pf7[3], fp1, fmaf(a.pf7[4], f0, a.pf7[5] * fm1));
+        const float eL3 = fmaf(a.pf7[0], fp2, fmaf(a.pf7[1], fp1, a.pf7[2] * f0));
+        const float eR0 = fmaf(a.pf7[21], fm1, fmaf(a.pf7[22], fm2, a.pf7[23] * fm3));
+        const float eR1 = fmaf(a.pf7[18], f0, fmaf(a.pf7[19], fm1, a.pf7[20] * fm2));
+        const float eR2 = fmaf(a.pf7[15], fp1, fmaf(a.pf7[16], f0, a.pf7[17] * fm1));
+        const float eR3 = fmaf(a.pf7[12], fp2, fmaf(a.pf7[13], fp1, a.pf7[14] * f0));
+        L = fmaf(WL, v0, fmaf(wL0, eL0, fmaf(wL1, eL1, fmaf(wL2, eL2, wL3 * eL3))));
+        R = fmaf(WR, v0, fmaf(wR0, eR0, fmaf(wR1, eR1, fmaf(wR2, eR2, wR3 * eR3))));
+        if constexpr (MPF) {
+            float xL = L - v0, xR = R - v0;
+            mp32_sided(fm1, f0, mA, mB, xL, xR);
+            L = v0 + xL;
+            R = v0 + xR;
+        }
+        return ok;
+    }
 };
-
 // The reference sequence for one WENO7 face, FP32 storage (FP64 arithmetic).
 template <bool MPF>
 __device__ __noinline__ void march32_7_redo(const MarchArgs& a, const float* __restrict__ col, long long o, float& L,
@@ -1086,7 +1249,7 @@ __device__ __noinline__ void march32_7_redo(const MarchArgs& a, const float* __r
         v[q] = f[q];
     }
     double Ld, Rd;
-    weno7_face<double>(v + 3, c, JS, a.wp.eps, 0.0, Ld, Rd);
+    weno7_face<double>(v + 3, c, a.wp.scheme, a.wp.eps, a.wp.teno_ct, Ld, Rd);
     L = (float)Ld;
     R = (float)Rd;
     if (MPF) MP<float>::apply(f[1], f[2], f[3], f[4], f[5], L, R);

@@ -155,9 +155,9 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col,
 #endif
 // PF: face-dependent coefficients from the per-face table a.ftab (FP64).
 // ORDER 7: the WENO7 engine (face-independent coefficients); face f reads
-// cells f .. f+6 and pushes cell f+7.  TENO: WENO5 TENO weights (FP64,
-// face-independent coefficients).
-template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5, bool TENO5 = false>
+// cells f .. f+6 and pushes cell f+7.  TENOW: TENO weights (the engines'
+// face_teno; face-independent coefficients).
+template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5, bool TENOW = false>
 __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
                                                   : (sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32))
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
     static_assert(ORDER == 5 || (ORDER == 7 && !PF), "WENO7: face-independent coefficients");
-    static_assert(!TENO5 || (ORDER == 5 && sizeof(T) == 8 && !PF), "TENO: FP64 WENO5, face-independent");
+    static_assert(!TENOW || !PF, "TENO: face-independent coefficients");
     using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
                                       typename MarchEngine<T>::type>;
     constexpr int PUSH0 = ORDER == 7 ? 7 : 6;             // tile position of the cell pushed after face f0
@@ -306,12 +306,13 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 // face 3 reads cells 3 .. 9: cell 3 lies before tile 0 (cells 4 .. 11)
                 const T c3 = __ldg(column(u0, wv, vv) + 3 * a.sJ);
                 w.init(a, c3, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
-                ok = w.template face<MPF>(a, L, R);
+                if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
+                else ok = w.template face<MPF>(a, L, R);
             } else if constexpr (PF) {
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
                 ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
-            } else if constexpr (TENO5) {
+            } else if constexpr (TENOW) {
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
                 ok = w.template face_teno<MPF>(a, L, R);
             } else {
@@ -319,8 +320,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 ok = w.template face<MPF>(a, L, R);
             }
             if (!ok) {
+                // (the redo sequences take the weights from the arguments)
                 if constexpr (ORDER == 7) march7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
-                else if constexpr (TENO5) march64_teno_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
                 else march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
             }
             if (u0 + lane < a.Nu) {
@@ -383,7 +384,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 T L, R;
                 bool ok;
                 if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
-                else if constexpr (TENO5) ok = w.template face_teno<MPF>(a, L, R);
+                else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
                 else ok = w.template face<MPF>(a, L, R);
                 if (!ok) bad |= 1u << i;
                 Lg[i % G] = L;
@@ -417,7 +418,6 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     bad &= bad - 1;
                     T L, R;
                     if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
-                    else if constexpr (TENO5) march64_teno_redo<MPF>(a, col, f0 + i, L, R);
                     else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
@@ -576,22 +576,26 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     if (teno) {
-        // WENO5-TENO: FP64, face-independent coefficients
-        if constexpr (sizeof(T) == 8) {
-            if (a.ftab || order != 5) return 1003;
-            static const KFn tablet[2][2][2] = {
-                {{sweep_march_tma_kernel<false, 0, T, 0, false, 5, true>,
-                  sweep_march_tma_kernel<false, 0, T, 1, false, 5, true>},
-                 {sweep_march_tma_kernel<false, 1, T, 0, false, 5, true>,
-                  sweep_march_tma_kernel<false, 1, T, 1, false, 5, true>}},
-                {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, true>,
-                  sweep_march_tma_kernel<true, 0, T, 1, false, 5, true>},
-                 {sweep_march_tma_kernel<true, 1, T, 0, false, 5, true>,
-                  sweep_march_tma_kernel<true, 1, T, 1, false, 5, true>}}};
-            kfn = tablet[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
-        } else {
-            return 1003;
-        }
+        // TENO weights, WENO5 or WENO7: face-independent coefficients
+        if (a.ftab) return 1003;
+        static const KFn tablet[2][2][2][2] = {
+            {{{sweep_march_tma_kernel<false, 0, T, 0, false, 5, true>,
+               sweep_march_tma_kernel<false, 0, T, 1, false, 5, true>},
+              {sweep_march_tma_kernel<false, 1, T, 0, false, 5, true>,
+               sweep_march_tma_kernel<false, 1, T, 1, false, 5, true>}},
+             {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, true>,
+               sweep_march_tma_kernel<true, 0, T, 1, false, 5, true>},
+              {sweep_march_tma_kernel<true, 1, T, 0, false, 5, true>,
+               sweep_march_tma_kernel<true, 1, T, 1, false, 5, true>}}},
+            {{{sweep_march_tma_kernel<false, 0, T, 0, false, 7, true>,
+               sweep_march_tma_kernel<false, 0, T, 1, false, 7, true>},
+              {sweep_march_tma_kernel<false, 1, T, 0, false, 7, true>,
+               sweep_march_tma_kernel<false, 1, T, 1, false, 7, true>}},
+             {{sweep_march_tma_kernel<true, 0, T, 0, false, 7, true>,
+               sweep_march_tma_kernel<true, 0, T, 1, false, 7, true>},
+              {sweep_march_tma_kernel<true, 1, T, 0, false, 7, true>,
+               sweep_march_tma_kernel<true, 1, T, 1, false, 7, true>}}}};
+        kfn = tablet[order == 7 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     } else if (order == 7) {
         // WENO7: face-independent coefficients
         if (a.ftab) return 1003;

@@ -332,14 +332,12 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if (!ucf) cp = CoefPtrs{cf->polyL, cf->polyR, cf->dL, cf->dR, cf->beta_coef};
     WenoParams wp{gr->scheme, gr->weno_eps, gr->teno_CT};
     const int choice = kernel_choice();
-    if constexpr (sizeof(T) == 8) {
-        if ((choice == 0 || choice == 3) && ucf && order == 5 && gr->scheme == WENO_SB_TENO &&
-            march_weights_ok(ucf)) {
-            const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
-            int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 5, true);
-            if (rc != WENO_SB_ERR_UNSUPPORTED)
-                return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (TENO)") : rc;
-        }
+    if ((choice == 0 || choice == 3) && ucf && (order == 5 || order == 7) && gr->scheme == WENO_SB_TENO &&
+        march_weights_ok(ucf, order)) {
+        const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, order);
+        int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, true);
+        if (rc != WENO_SB_ERR_UNSUPPORTED)
+            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (TENO)") : rc;
     }
     if ((choice == 0 || choice == 3) && ucf && order == 7 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 7)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 7);
@@ -1098,9 +1096,9 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
         // marching items for the orders and weights a marching engine covers,
         // when the block's coefficients are the same on every face
         const bool js = b.grid.scheme == WENO_SB_JS;
-        const bool teno5 = b.grid.scheme == WENO_SB_TENO && b.order == 5 && b.dtype == WENO_SB_FP64;
+        const bool teno = b.grid.scheme == WENO_SB_TENO;
         double ucf[56];
-        if (kernel_choice() != 1 && (b.order == 5 || b.order == 7) && (js || teno5) &&
+        if (kernel_choice() != 1 && (b.order == 5 || b.order == 7) && (js || teno) &&
             batch_coefs_uniform(b.coefs, e.g.nc, b.order, ucf) && march_weights_ok(ucf, b.order)) {
             B->margs.push_back(make_march_args(e.g, b.v_in, b.vL, b.vR, e.wp, ucf, b.order));
             e.march = (int)B->margs.size();
