@@ -385,10 +385,10 @@ def test_full_size_weno5_mp(wsb, oracle_mod, entry):
         torch.cuda.empty_cache()
 
 
-@pytest.mark.parametrize("order,scheme", [(5, 0), (7, 0), (5, 3), (7, 3)])
+@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3), (7, 3)])
 def test_mid_size_uniform_entry(wsb, oracle_mod, order, scheme):
-    """96^3 x 4 (several segments per column, every tile shape), WENO5 / WENO7
-    with JS and TENO weights, + MP, through the face-independent entry, drop-in and
+    """96^3 x 4 (several segments per column, every tile shape), WENO3 / WENO5 /
+    WENO7 with JS and WENO5 / WENO7 with TENO weights, + MP, through the face-independent entry, drop-in and
     folded, against the oracle at 1e-12 per array (TENO: the cutoff may flip
     on borderline faces, as in test_reconstruction_parity)."""
     import torch

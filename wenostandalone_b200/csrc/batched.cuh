@@ -53,8 +53,10 @@ struct BatchEntry {
 // core faces 3 .. ns-4 (cells o+1 .. o+5 for WENO5, o .. o+6 for WENO7).
 template <typename T, int ORDER, bool TENOW, bool MPF>
 __device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry& e, long long cg) {
-    using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
-                                      std::conditional_t<sizeof(T) == 8, March64, March32>>;
+    using Engine = std::conditional_t<
+        ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
+        std::conditional_t<ORDER == 3, std::conditional_t<sizeof(T) == 8, March64_3, March32_3>,
+                           std::conditional_t<sizeof(T) == 8, March64, March32>>>;
     const long long col = cg * blockDim.x + threadIdx.x;
     if (col >= e.g.cols) return;
     const long long ca = col % e.g.c1, t = col / e.g.c1;
@@ -64,7 +66,8 @@ __device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry
     T* __restrict__ oL = (T*)e.vL + e.g.ns * col;
     T* __restrict__ oR = (T*)e.vR + e.g.ns * col;
     auto ld = [&](long long J) { return __ldg(cp + J * sJ); };
-    const long long o0 = 3, o1 = e.g.ns - 3;
+    // WENO3 writes every face (MP on the core faces), the others the core faces
+    const long long o0 = ORDER == 3 ? 0 : 3, o1 = ORDER == 3 ? e.g.ns : e.g.ns - 3;
     constexpr int PUSH = ORDER == 7 ? 7 : 6;  // cell pushed after face o: o + PUSH (at most ns + 2)
     Engine w;
     if constexpr (ORDER == 7) w.init(a, ld(o0), ld(o0 + 1), ld(o0 + 2), ld(o0 + 3), ld(o0 + 4), ld(o0 + 5), ld(o0 + 6));
@@ -74,9 +77,12 @@ __device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry
         T L, R;
         bool ok;
         if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
+        else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, o >= 3 && o <= e.g.ns - 4);
         else ok = w.template face<MPF>(a, L, R);
         if (!ok) {
-            if constexpr (ORDER == 7) {
+            if constexpr (ORDER == 3) {
+                march3_redo<MPF, T>(a, cp, o, L, R);
+            } else if constexpr (ORDER == 7) {
                 if constexpr (sizeof(T) == 8) march64_7_redo<MPF>(a, cp, o, L, R);
                 else march32_7_redo<MPF>(a, cp, o, L, R);
             } else if constexpr (sizeof(T) == 8) {

@@ -1255,6 +1255,135 @@ __device__ __noinline__ void march32_7_redo(const MarchArgs& a, const float* __r
     if (MPF) MP<float>::apply(f[1], f[2], f[3], f[4], f[5], L, R);
 }
 
+// ---------------------------------------------------------------------
+// WENO3-JS (+ MP) marching engines, face-independent coefficients (Coef<3>
+// layout in MarchArgs::ucf: polyL 0..1, polyR 2..3, dL 4..5, dR 6..7,
+// beta 8..9; f90:416-468).  beta_0(J) = b0 d[J]^2 + eps, beta_1(J) =
+// b1 d[J-1]^2 + eps.  WENO3 writes every face of the sweep (the reference's
+// is1 range) and the fused MP limiter applies on the core faces only, so
+// face() takes that as an argument; the window is still cells J-2 .. J+2
+// for the limiter's minmods.
+// ---------------------------------------------------------------------
+struct March64_3 {
+    double vm1, v0, vp1, vp2;   // cells J-1 .. J+2
+    double dm1, d0, dp1;        // d[J-1], d[J], d[J+1]
+    double B0, B1;              // beta_0(J), beta_1(J)
+    double e2, mA, mB;
+
+    __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3, double c4) {
+        vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
+        const double dm2 = c1 - c0;
+        dm1 = c2 - c1; d0 = c3 - c2; dp1 = c4 - c3;
+        B0 = fma(a.ucf[8], d0 * d0, a.wp.eps);
+        B1 = fma(a.ucf[9], dm1 * dm1, a.wp.eps);
+        const double em = dm1 - dm2, ez = d0 - dm1;
+        e2 = dp1 - d0;
+        mA = mm64(em, ez);
+        mB = mm64(ez, e2);
+    }
+    __device__ __forceinline__ void push(const MarchArgs& a, double n) {
+        const double dn = n - vp2;
+        const double nB0 = fma(a.ucf[8], dp1 * dp1, a.wp.eps), nB1 = fma(a.ucf[9], d0 * d0, a.wp.eps);
+        const double ne2 = dn - dp1;
+        const double nmB = mm64(e2, ne2);
+        vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
+        dm1 = d0; d0 = dp1; dp1 = dn;
+        B0 = nB0; B1 = nB1;
+        e2 = ne2; mA = mB; mB = nmB;
+    }
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+        return face<MPF>(a, L, R, true);
+    }
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R, bool core) const {
+        const double P0 = B1 * B1, P1 = B0 * B0;
+        const double SL = fma(a.ucf[4], P0, a.ucf[5] * P1), SR = fma(a.ucf[6], P0, a.ucf[7] * P1);
+        const double EL = fma(P0, a.kL[0] * d0, P1 * (a.kL[1] * dm1));
+        const double ER = fma(P0, a.kR[0] * d0, P1 * (a.kR[1] * dm1));
+        const double p = SL * SR;
+        const bool ok = mid_range_prod(p);
+        const double r = rcp1(p);
+        L = fma(EL * SR, r, v0);
+        R = fma(ER * SL, r, v0);
+        if (MPF && core) mp64_sided(vm1, v0, vp1, dm1, d0, mA, mB, sign_clear(EL), sign_clear(ER), L, R);
+        return ok;
+    }
+};
+
+struct March32_3 {
+    float vm1, v0, vp1, vp2;    // cells J-1 .. J+2
+    float fm1, f0, fp1;         // FP32 differences
+    double Dp2, Dd0, Ddp1;      // vp2 widened; FP64 d[J], d[J+1]
+    double B0, B1;
+    float e2, mA, mB;
+
+    __device__ __forceinline__ void init(const MarchArgs& a, float c0, float c1, float c2, float c3, float c4) {
+        vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
+        const float fm2 = c1 - c0;
+        fm1 = c2 - c1; f0 = c3 - c2; fp1 = c4 - c3;
+        const double D1 = c1, D2 = c2, D3 = c3;
+        Dp2 = c4;
+        const double ddm1 = D2 - D1;
+        Dd0 = D3 - D2; Ddp1 = Dp2 - D3;
+        B0 = fma(a.ucf[8], Dd0 * Dd0, a.wp.eps);
+        B1 = fma(a.ucf[9], ddm1 * ddm1, a.wp.eps);
+        const float em = fm1 - fm2, ez = f0 - fm1;
+        e2 = fp1 - f0;
+        mA = mm32(em, ez);
+        mB = mm32(ez, e2);
+    }
+    __device__ __forceinline__ void push(const MarchArgs& a, float n) {
+        const double Dn = n;
+        const double dn = Dn - Dp2;
+        const double nB0 = fma(a.ucf[8], Ddp1 * Ddp1, a.wp.eps), nB1 = fma(a.ucf[9], Dd0 * Dd0, a.wp.eps);
+        const float fn = n - vp2;
+        const float ne2 = fn - fp1;
+        const float nmB = mm32(e2, ne2);
+        vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
+        fm1 = f0; f0 = fp1; fp1 = fn;
+        Dp2 = Dn; Dd0 = Ddp1; Ddp1 = dn;
+        B0 = nB0; B1 = nB1;
+        e2 = ne2; mA = mB; mB = nmB;
+    }
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, float& L, float& R) const {
+        return face<MPF>(a, L, R, true);
+    }
+    template <bool MPF>
+    __device__ __forceinline__ bool face(const MarchArgs& a, float& L, float& R, bool core) const {
+        const double P0 = B1 * B1, P1 = B0 * B0;
+        const double aL0 = a.ucf[4] * P0, aR0 = a.ucf[6] * P0;
+        const double SL = fma(a.ucf[5], P1, aL0), SR = fma(a.ucf[7], P1, aR0);
+        const double p = SL * SR;
+        const bool ok = mid_range_prod(p);
+        const double r = rcp1(p);
+        const float wL0 = __double2float_rn(aL0 * (SR * r)), wR0 = __double2float_rn(aR0 * (SL * r));
+        const float eL0 = a.pf2[0].x * f0, eL1 = a.pf2[1].x * fm1;
+        const float eR0 = a.pf2[0].y * f0, eR1 = a.pf2[1].y * fm1;
+        float xL = fmaf(wL0, eL0 - eL1, eL1), xR = fmaf(wR0, eR0 - eR1, eR1);
+        if (MPF && core) mp32_sided(fm1, f0, mA, mB, xL, xR);
+        L = v0 + xL;
+        R = v0 + xR;
+        return ok;
+    }
+};
+
+// The reference sequence for one WENO3 face (cells o+1 .. o+5; MP on the
+// core faces).
+template <bool MPF, typename T>
+__device__ __noinline__ void march3_redo(const MarchArgs& a, const T* __restrict__ col, long long o, T& L, T& R) {
+    const Coef<3>& c = *reinterpret_cast<const Coef<3>*>(a.ucf);
+    const T* p = col + (o + 1) * a.sJ;
+    const T vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
+            vp2 = __ldg(p + 4 * a.sJ);
+    double Ld, Rd;
+    weno3_face((double)vm1, (double)v0, (double)vp1, c, a.wp.scheme, a.wp.eps, Ld, Rd);
+    L = (T)Ld;
+    R = (T)Rd;
+    if (MPF && o >= 3 && o <= a.ns - 4) MP<T>::apply(vm2, vm1, v0, vp1, vp2, L, R);
+}
+
 #ifndef WSB_MARCH64_MIN_BLOCKS
 #define WSB_MARCH64_MIN_BLOCKS 3
 #endif
@@ -1369,6 +1498,15 @@ inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, v
     a.n_ut = (a.Nu + 31) / 32;
     if (!ucf) return a;  // face-dependent coefficients: the caller sets ftab and cp
     for (int q = 0; q < 56; ++q) a.ucf[q] = ucf[q];
+    if (order == 3) {
+        // Coef<3>: polyL 0..1, polyR 2..3, dL 4..5, dR 6..7
+        for (int r = 0; r < 2; ++r) {
+            a.kL[r] = ucf[4 + r] * ucf[r];
+            a.kR[r] = ucf[6 + r] * ucf[2 + r];
+            a.pf2[r] = make_float2((float)ucf[r], (float)ucf[2 + r]);
+        }
+        return a;
+    }
     if (order == 7) {
         for (int s = 0; s < 4; ++s)
             for (int t = 0; t < 3; ++t) {

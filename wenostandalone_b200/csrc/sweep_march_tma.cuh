@@ -168,10 +168,13 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
-    static_assert(ORDER == 5 || (ORDER == 7 && !PF), "WENO7: face-independent coefficients");
+    static_assert(ORDER == 5 || (ORDER != 5 && !PF), "WENO3 / WENO7: face-independent coefficients");
     static_assert(!TENOW || !PF, "TENO: face-independent coefficients");
-    using Engine = std::conditional_t<ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
-                                      typename MarchEngine<T>::type>;
+    using Engine = std::conditional_t<
+        ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
+        std::conditional_t<ORDER == 3, std::conditional_t<sizeof(T) == 8, March64_3, March32_3>,
+                           typename MarchEngine<T>::type>>;
+    static_assert(ORDER != 3 || (!PF && !TENOW), "WENO3: JS, face-independent coefficients");
     constexpr int PUSH0 = ORDER == 7 ? 7 : 6;             // tile position of the cell pushed after face f0
     extern __shared__ __align__(1024) unsigned char smem_mt[];
     unsigned char* base = smem_mt + ((1024u - (smem_u32(smem_mt) & 1023u)) & 1023u);
@@ -192,7 +195,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     T* __restrict__ outL = (T*)a.vL;
     T* __restrict__ outR = (T*)a.vR;
     const long long nwarps = (long long)gridDim.x * kTmaWarps;
-    const int o_last = (int)a.ns - 3;         // one past the last core face
+    // faces written: the core faces 3 .. ns-4 (chunks from face 4, face 3 by
+    // the prologue), or every face 0 .. ns-1 for WENO3 (chunks from face 0)
+    const int o_last = ORDER == 3 ? (int)a.ns : (int)a.ns - 3;  // one past the last face
     unsigned n_issued = 0, n_waited = 0;      // tiles requested / completed (waited on) by this warp
     unsigned n_chunks = 0;                    // output chunks stored by this warp
     bool failed = false;
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
         const int wv = (int)(tt % a.Nw);
         const int vv = (int)(tt / a.Nw);
         const int u0 = ut * 32;
-        const int f_start = 4 + sg * a.seg;                       // 4 mod 8
+        const int f_start = (ORDER == 3 ? 0 : 4) + sg * a.seg;    // 4 mod 8 (WENO3: 0 mod 8)
         int f_end = f_start + a.seg;
         if (f_end > o_last) f_end = o_last;
         const int nch = f_end > f_start ? (f_end - f_start + F - 1) / F : 0;
@@ -298,7 +303,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
         if (!wait_tile(k0)) { failed = true; break; }
 
         Engine w;
-        if (sg == 0) {
+        if (sg == 0 && ORDER != 3) {
             // face 3 (cells 4..8 = tile positions 0..4), plain stores
             T L, R;
             bool ok;
@@ -385,6 +390,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 bool ok;
                 if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
+                else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, f0 + i >= 3 && f0 + i <= o_last - 4);
                 else ok = w.template face<MPF>(a, L, R);
                 if (!ok) bad |= 1u << i;
                 Lg[i % G] = L;
@@ -418,12 +424,13 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     bad &= bad - 1;
                     T L, R;
                     if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(a, col, f0 + i, L, R);
                     else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
             }
-            const int i_last = o_last - 1 - f0;  // the last core face, when in this chunk
+            const int i_last = ORDER == 3 ? -1 : o_last - 1 - f0;  // the last core face, when in this chunk
             if (i_last >= 0 && i_last < F && u0 + lane < a.Nu) {
                 // outside the store map's extent (see launch_march_tma)
                 const long long oi = (o_last - 1) + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
@@ -530,7 +537,9 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     // 16-byte steps, so the face extent is ns - 4 (a 16-byte multiple):
     // faces up to ns-5 are stored by the TMA unit, the last core face ns-4
     // with plain stores, and the non-core faces ns-3 .. ns-1 are never written.
-    cuuint64_t od[4] = {(cuuint64_t)(g.ns - 4), (cuuint64_t)g.c1, (cuuint64_t)g.c2, (cuuint64_t)g.nv};
+    // (WENO3 writes every face: extent ns)
+    cuuint64_t od[4] = {(cuuint64_t)(order == 3 ? g.ns : g.ns - 4), (cuuint64_t)g.c1, (cuuint64_t)g.c2,
+                        (cuuint64_t)g.nv};
     cuuint64_t os[3] = {(cuuint64_t)g.ns * ES, (cuuint64_t)(g.ns * g.c1) * ES, (cuuint64_t)(g.ns * g.c1 * g.c2) * ES};
     cuuint32_t ob[4] = {kTmaF, 1, 1, 1};
     // lanes run along the output axis the march arguments chose (oU == ns: c1, else c2)
@@ -546,7 +555,7 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     // the lane axis must be the one the march arguments chose
     if ((t.kind == 1) != (a.sU == 1)) return 1003;
     // segments over faces [4, ns-3), a multiple of 8 faces each
-    const long long nf4 = g.ns - 7;
+    const long long nf4 = order == 3 ? g.ns : g.ns - 7;  // faces in the chunked range
     const long long cols = (long long)a.n_ut * a.Nw * a.NV;
 #ifndef WSB_MTMA_ITEMS_PER_WARP
 #define WSB_MTMA_ITEMS_PER_WARP 8  // target work items per resident warp (200^3: two segments per column)
@@ -596,6 +605,15 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
               {sweep_march_tma_kernel<true, 1, T, 0, false, 7, true>,
                sweep_march_tma_kernel<true, 1, T, 1, false, 7, true>}}}};
         kfn = tablet[order == 7 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+    } else if (order == 3) {
+        // WENO3: JS, face-independent coefficients
+        if (a.ftab) return 1003;
+        static const KFn table3[2][2][2] = {
+            {{sweep_march_tma_kernel<false, 0, T, 0, false, 3>, sweep_march_tma_kernel<false, 0, T, 1, false, 3>},
+             {sweep_march_tma_kernel<false, 1, T, 0, false, 3>, sweep_march_tma_kernel<false, 1, T, 1, false, 3>}},
+            {{sweep_march_tma_kernel<true, 0, T, 0, false, 3>, sweep_march_tma_kernel<true, 0, T, 1, false, 3>},
+             {sweep_march_tma_kernel<true, 1, T, 0, false, 3>, sweep_march_tma_kernel<true, 1, T, 1, false, 3>}}};
+        kfn = table3[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     } else if (order == 7) {
         // WENO7: face-independent coefficients
         if (a.ftab) return 1003;

@@ -288,7 +288,7 @@ int kernel_choice() {
 // sign of the weighted candidate sum, which holds for non-negative ideal
 // weights (Coef<5> layout: dL, dR at 12..17; Coef<7>: at 24..31).
 bool march_weights_ok(const double* ucf, int order = 5) {
-    const int q0 = order == 7 ? 24 : 12, q1 = order == 7 ? 32 : 18;
+    const int q0 = order == 7 ? 24 : (order == 3 ? 4 : 12), q1 = order == 7 ? 32 : (order == 3 ? 8 : 18);
     for (int q = q0; q < q1; ++q)
         if (!(ucf[q] >= 0.0)) return false;
     return true;
@@ -338,6 +338,12 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
         int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, true);
         if (rc != WENO_SB_ERR_UNSUPPORTED)
             return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (TENO)") : rc;
+    }
+    if ((choice == 0 || choice == 3) && ucf && order == 3 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 3)) {
+        const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 3);
+        int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 3);
+        if (rc != WENO_SB_ERR_UNSUPPORTED)
+            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (WENO3)") : rc;
     }
     if ((choice == 0 || choice == 3) && ucf && order == 7 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 7)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 7);
@@ -1098,6 +1104,9 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
         const bool js = b.grid.scheme == WENO_SB_JS;
         const bool teno = b.grid.scheme == WENO_SB_TENO;
         double ucf[56];
+        // (WENO3 stays on per-face items: its one-thread-per-column march
+        // reads x columns uncoalesced and measured slower than the per-face
+        // items, whose stencils are cheap)
         if (kernel_choice() != 1 && (b.order == 5 || b.order == 7) && (js || teno) &&
             batch_coefs_uniform(b.coefs, e.g.nc, b.order, ucf) && march_weights_ok(ucf, b.order)) {
             B->margs.push_back(make_march_args(e.g, b.v_in, b.vL, b.vR, e.wp, ucf, b.order));
