@@ -176,7 +176,7 @@ __device__ __forceinline__ void batch_item(const BatchEntry& e, long long grp, i
 
 // Persistent kernel: CTAs take items from *counter until n_items.
 #ifndef WSB_BATCH_MIN_BLOCKS
-#define WSB_BATCH_MIN_BLOCKS 2  // 2 CTAs of 256 per SM (128 registers; the WENO7 paths spill a little, still faster)
+#define WSB_BATCH_MIN_BLOCKS 2  // 2 CTAs of 256 per SM (128 registers; the marching paths spill a little, still faster than 168-255)
 #endif
 __global__ void __launch_bounds__(256, WSB_BATCH_MIN_BLOCKS)
     batch_kernel(const BatchEntry* __restrict__ entries, int n_entries, long long n_items,
