@@ -36,20 +36,42 @@ ORDER = 5
 METRIC = "WENO5 face-states/s at 199^3 x 8 vars (FP64 WENO5-JS + MP, x/y/z sweeps)"
 
 
-def face_states_per_dir(m=None, nv=NV, buff=BUFF):
+SCHEME = "js"
+
+
+def face_states_per_dir(m=None, nv=NV, buff=BUFF, order=None):
+    """Face states one sweep writes: vL and vR on the NC core faces (WENO3:
+    on every face of the sweep, the reference's is1 range)."""
     m = M if m is None else m
+    order = ORDER if order is None else order
     N = m + 2 * buff + 1
-    return 2 * (N - 6) * N * N * nv
+    return 2 * (N if order == 3 else N - 6) * N * N * nv
 
 
-def alg_bytes_per_sweep(m=None, nv=NV, buff=BUFF, elem=8, order=ORDER):
+def alg_bytes_per_sweep(m=None, nv=NV, buff=BUFF, elem=8, order=None):
     """Algorithmic HBM bytes of one fused sweep: read the (NC+2H)-long
-    stencil window of every column once, write vL and vR on the NC core faces."""
+    stencil window of every column once, write vL and vR on the NC core faces
+    (WENO3: the N+2 cells of its 3-point stencils, vL and vR on all N faces)."""
     m = M if m is None else m
+    order = ORDER if order is None else order
     N = m + 2 * buff + 1
+    if order == 3:
+        return (N + 2) * N * N * nv * elem + 2 * N * N * N * nv * elem
     NC = N - 6
     H = max((order - 1) // 2, 2)
     return (NC + 2 * H) * N * N * nv * elem + 2 * NC * N * N * nv * elem
+
+
+def family():
+    return f"WENO{ORDER}-{'TENO' if SCHEME == 'teno' else 'JS'}"
+
+
+def main_metric(fp32_main):
+    """The headline metric (WENO5-JS, FP64); other families and FP32-bulk name themselves."""
+    m = METRIC
+    if ORDER != 5 or SCHEME != "js":
+        m = m.replace("WENO5 face-states", f"WENO{ORDER} face-states").replace("WENO5-JS", family())
+    return m.replace("FP64", "FP32-bulk") if fp32_main else m
 
 
 def load_peaks():
@@ -202,7 +224,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     wsb.lib()
 
-    g = wsb.Grid(M, M, M, NV, BUFF)
+    g = wsb.Grid(M, M, M, NV, BUFF, scheme=wsb.TENO if SCHEME == "teno" else wsb.JS)
     vf_host = fields.smooth_jump_field(M, M, M, NV, BUFF, seed=rank)
     v = torch.from_numpy(vf_host.ravel(order="F")).to(dev)
     coefs = [tuple(torch.from_numpy(c.ravel(order="F")).to(dev)
@@ -329,13 +351,13 @@ def run_ours(args):
 
     if rank == 0:
         line = {
-            "metric": METRIC.replace("FP64", "FP32-bulk") if fp32_main else METRIC, "value": value, "unit": "face-states/s", "n_gpus": ws, "steps": K,
+            "metric": main_metric(fp32_main), "value": value, "unit": "face-states/s", "n_gpus": ws, "steps": K,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32-bulk" if fp32_main else "f64",
             "data": "synthetic",
-            "config": {"workload": ("FP32-bulk WENO5-JS + MP (FP64 beta and weights), x/y/z sweeps of FP32 "
+            "config": {"workload": (f"FP32-bulk {family()} + MP (FP64 beta and weights), x/y/z sweeps of FP32 "
                                     "v_rs_ws" if fp32_main else
-                                    "FP64 WENO5-JS + MP fused, x/y/z sweeps reading v_vf directly "
+                                    f"FP64 {family()} + MP fused, x/y/z sweeps reading v_vf directly "
                                     "(reshape folded)") + f", {M + 1}^3 cells x 8 vars, buff_size 6",
                        "m=n=p": M, "v_size": NV, "buff_size": BUFF,
                        "coefficients": ("uniform-grid WENO5-JS values as per-face device arrays (weno_sb_weno_dev)"
@@ -352,7 +374,7 @@ def run_ours(args):
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
                          "alg_bytes_per_launch": ab, "launch_ms": dk_ms,
-                         "traffic": None if (fp32_main or pf_main or M != 199) else read_traffic()},
+                         "traffic": None if (fp32_main or pf_main or M != 199 or ORDER != 5 or SCHEME != "js") else read_traffic()},
             "per_sweep_ms": [s / K for s in sums],
             # the per-face form launches the table build and the sweep
             "gpu_launches": (6 if pf_main else 3) * K,
@@ -788,12 +810,22 @@ def main():
     ap.add_argument("--m", type=int, default=199, help="cells per axis minus one (m=n=p); 199 = 200^3")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="fp32: time the FP32-bulk form as the main step (no extras)")
+    ap.add_argument("--order", type=int, choices=[3, 5, 7], default=5,
+                    help="reconstruction order of the main step (5 is the headline metric; others skip the extras)")
+    ap.add_argument("--scheme", choices=["js", "teno"], default="js",
+                    help="nonlinear weights of the main step (teno: teno_CT 1e-5; WENO5 / WENO7 only)")
     ap.add_argument("--coefficients", choices=["uniform", "arrays"], default="uniform",
                     help="arrays: the main step passes the coefficients as per-face device arrays "
                          "(weno_sb_weno_dev, the drop-in form) instead of one face-independent set")
     args = ap.parse_args()
-    global M
+    global M, ORDER, SCHEME
     M = args.m
+    ORDER = args.order
+    SCHEME = args.scheme
+    if ORDER == 3 and SCHEME == "teno":
+        ap.error("WENO3 has no TENO weights (f90:392-475)")
+    if ORDER != 5 or SCHEME != "js":
+        args.no_extras = True
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
