@@ -1,29 +1,30 @@
-// sweep_march.cuh -- WENO5-JS (+MP) sweep that marches along the sweep axis.
+// sweep_march.cuh -- marching WENO engines: WENO3 / WENO5 / WENO7 (+MP)
+// along the sweep axis, and the WENO5 marching kernel with per-lane loads.
 //
 // The face-parallel kernels (sweep_pipe.cuh, sweep_tma.cuh) give every
 // thread one face and recompute, for each face, everything its stencil
 // shares with the neighbouring faces: 4 differences, the products in the 3
 // smoothness indicators, 3 second differences and 2 minmods of the MP
 // limiter (and, for FP32-bulk storage, 5 widenings to FP64).  Consecutive
-// faces overlap in 4 of their 5 stencil cells, so here a thread owns one
-// column of the sweep and walks along it: per face it loads one new cell,
-// forms one new difference (FP64, plus its FP32 twin for FP32-bulk), one
-// new square and one new cross product, one new second difference and one
-// new minmod, and slides the rest along in registers.
+// faces overlap in all but one of their stencil cells, so here a thread owns
+// one column of the sweep and walks along it: per face it loads one new
+// cell, forms one new difference (FP64, plus its FP32 twin for FP32-bulk),
+// the new products of the smoothness indicators it enters, one new second
+// difference and one new minmod, and slides the rest along in registers.
 //
-// Work item: 32 adjacent columns (one warp; lanes take consecutive values
-// of the cross axis with unit stride when the sweep is strided, so the
-// folded y/z sweeps load 32 consecutive x per instruction) by a segment of
-// faces.  Face states go to a per-warp shared-memory tile [F faces][33] and
-// leave as F-face row segments, one coalesced store per column pair, so
-// the face-fastest vL/vR layout is written contiguously.  Only warp-level
-// synchronisation is used; nothing waits on another warp.
-//
-// Coefficients are face-independent (uniform grids, weno_sb_weno_uniform_dev)
-// and come from the kernel-parameter bank.  Arithmetic per face follows
-// weno_math.cuh: FP64 differences, beta and the one-reciprocal JS weights
-// (faithful fallback outside its range); FP64 or FP32 (FP32-bulk)
-// candidate polynomials; the MP limiter in the storage precision.
+// Engines (init / push / face, and face_teno for TENO weights):
+//   March64, March32       WENO5, FP64 / FP32-bulk
+//   March64_7, March32_7   WENO7
+//   March64_3, March32_3   WENO3 (every face written; MP on core faces)
+// The TMA kernel that drives them is sweep_march_tma.cuh; batched.cuh runs
+// them one column per thread.  Coefficients are face-independent and come
+// from the kernel-parameter bank (MarchArgs), except for the FP64 WENO5
+// kernel with a per-face table (march_face_table_kernel, FaceRow, BetaRow).
+// Arithmetic per face follows weno_math.cuh: FP64 differences, beta and the
+// one-reciprocal weights (the reference sequence redoes a face whose sums
+// leave the reciprocal form's range); FP64 or FP32 (FP32-bulk) candidate
+// polynomials; the MP limiter in the storage precision, one-sided on the
+// sign of the state's offset from v0.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -1,5 +1,7 @@
-// sweep_march_tma.cuh -- FP64 WENO5-JS (+MP) marching sweep with TMA
-// staging of its input cells and output face states.
+// sweep_march_tma.cuh -- the marching sweep (sweep_march.cuh engines: WENO3
+// / WENO5 / WENO7, JS or TENO weights, FP64 or FP32-bulk, face-independent
+// coefficients or, FP64 WENO5-JS, a per-face table) with TMA staging of its
+// input cells and output face states.
 //
 // The marching kernel of sweep_march.cuh spends, at 200^3 x 8, about as
 // much time waiting on its per-lane global loads (a few cells ahead in
