@@ -51,70 +51,99 @@ struct BatchEntry {
 
 // One marching item: thread t marches column cg * blockDim.x + t over the
 // core faces 3 .. ns-4 (cells o+1 .. o+5 for WENO5, o .. o+6 for WENO7).
+// Faces per output chunk of a marching item: each warp stages kBatchF faces
+// x 32 columns of vL and vR in shared memory and writes them back as
+// kBatchF-face segments of each column (64 bytes in FP64), so a store
+// instruction covers 4 columns instead of 32 (the face-fastest layout puts
+// neighbouring columns ns elements apart).
+constexpr int kBatchF = 8;
+
 template <typename T, int ORDER, bool TENOW, bool MPF>
-__device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry& e, long long cg) {
+__device__ __forceinline__ void batch_march(const MarchArgs& a, const BatchEntry& e, long long cg,
+                                            T (*tl)[kBatchF][33]) {
     using Engine = std::conditional_t<
         ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
         std::conditional_t<ORDER == 3, std::conditional_t<sizeof(T) == 8, March64_3, March32_3>,
                            std::conditional_t<sizeof(T) == 8, March64, March32>>>;
-    const long long col = cg * blockDim.x + threadIdx.x;
-    if (col >= e.g.cols) return;
+    const int lane = threadIdx.x & 31;
+    const long long wcol0 = cg * blockDim.x + (threadIdx.x & ~31);  // this warp's first column
+    if (wcol0 >= e.g.cols) return;                                   // (whole warp)
+    // lanes past the last column shadow it (loads stay in bounds, nothing is stored)
+    const long long col = min(wcol0 + lane, e.g.cols - 1);
     const long long ca = col % e.g.c1, t = col / e.g.c1;
     const long long cb = t % e.g.c2, cv = t / e.g.c2;
     const T* __restrict__ cp = (const T*)e.in + e.g.in_off + ca * e.g.sA + cb * e.g.sB + cv * e.g.sV;
-    const long long sJ = e.g.sJ;
-    T* __restrict__ oL = (T*)e.vL + e.g.ns * col;
-    T* __restrict__ oR = (T*)e.vR + e.g.ns * col;
-    auto ld = [&](long long J) { return __ldg(cp + J * sJ); };
+    const long long sJ = e.g.sJ, ns = e.g.ns, ncell = e.g.ns + 6;
+    T* __restrict__ outL = (T*)e.vL;
+    T* __restrict__ outR = (T*)e.vR;
+    auto ld = [&](long long J) { return J < ncell ? __ldg(cp + J * sJ) : T(0); };
     // WENO3 writes every face (MP on the core faces), the others the core faces
-    const long long o0 = ORDER == 3 ? 0 : 3, o1 = ORDER == 3 ? e.g.ns : e.g.ns - 3;
-    constexpr int PUSH = ORDER == 7 ? 7 : 6;  // cell pushed after face o: o + PUSH (at most ns + 2)
+    const long long o0 = ORDER == 3 ? 0 : 3, o1 = ORDER == 3 ? ns : ns - 3;
+    constexpr int PUSH = ORDER == 7 ? 7 : 6;  // cell pushed after face o: o + PUSH
     Engine w;
     if constexpr (ORDER == 7) w.init(a, ld(o0), ld(o0 + 1), ld(o0 + 2), ld(o0 + 3), ld(o0 + 4), ld(o0 + 5), ld(o0 + 6));
     else w.init(a, ld(o0 + 1), ld(o0 + 2), ld(o0 + 3), ld(o0 + 4), ld(o0 + 5));
-    for (long long o = o0; o < o1; ++o) {
-        const T n = ld(o + PUSH);
-        T L, R;
-        bool ok;
-        if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
-        else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, o >= 3 && o <= e.g.ns - 4);
-        else ok = w.template face<MPF>(a, L, R);
-        if (!ok) {
-            if constexpr (ORDER == 3) {
-                march3_redo<MPF, T>(a, cp, o, L, R);
-            } else if constexpr (ORDER == 7) {
-                if constexpr (sizeof(T) == 8) march64_7_redo<MPF>(a, cp, o, L, R);
-                else march32_7_redo<MPF>(a, cp, o, L, R);
-            } else if constexpr (sizeof(T) == 8) {
-                march64_redo<MPF>(a, cp, o, L, R);
-            } else {
-                march32_redo<MPF>(a, cp, o, L, R);
+    const int fi = lane & (kBatchF - 1), cj = lane / kBatchF;
+    for (long long f0 = o0; f0 < o1; f0 += kBatchF) {
+        const int nF = (int)min((long long)kBatchF, o1 - f0);
+#pragma unroll 1
+        for (int i = 0; i < kBatchF; ++i) {
+            const long long o = f0 + i;  // faces past o1 (i >= nF) are computed and dropped
+            const T n = ld(o + PUSH);
+            T L, R;
+            bool ok;
+            if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
+            else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, o >= 3 && o <= ns - 4);
+            else ok = w.template face<MPF>(a, L, R);
+            if (!ok && i < nF) {
+                if constexpr (ORDER == 3) {
+                    march3_redo<MPF, T>(a, cp, o, L, R);
+                } else if constexpr (ORDER == 7) {
+                    if constexpr (sizeof(T) == 8) march64_7_redo<MPF>(a, cp, o, L, R);
+                    else march32_7_redo<MPF>(a, cp, o, L, R);
+                } else if constexpr (sizeof(T) == 8) {
+                    march64_redo<MPF>(a, cp, o, L, R);
+                } else {
+                    march32_redo<MPF>(a, cp, o, L, R);
+                }
+            }
+            tl[0][i][lane] = L;
+            tl[1][i][lane] = R;
+            w.push(a, n);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = cj; c < 32; c += 32 / kBatchF) {
+            const long long cc = wcol0 + c;
+            if (cc < e.g.cols && fi < nF) {
+                outL[cc * ns + f0 + fi] = tl[0][fi][c];
+                outR[cc * ns + f0 + fi] = tl[1][fi][c];
             }
         }
-        oL[o] = L;
-        oR[o] = R;
-        w.push(a, n);
+        __syncwarp();
     }
 }
 
 template <bool MPF>
-__device__ __forceinline__ void batch_march_dispatch(const MarchArgs& a, const BatchEntry& e, long long cg) {
+__device__ __forceinline__ void batch_march_dispatch(const MarchArgs& a, const BatchEntry& e, long long cg,
+                                                     double (*tile)[kBatchF][33]) {
+    float (*tile32)[kBatchF][33] = reinterpret_cast<float (*)[kBatchF][33]>(tile);
     // (the redo sequences take the weights from the arguments)
     const bool teno = e.wp.scheme == TENO;
     if (e.fp32) {
         if (e.order == 7) {
-            if (teno) batch_march<float, 7, true, MPF>(a, e, cg);
-            else batch_march<float, 7, false, MPF>(a, e, cg);
+            if (teno) batch_march<float, 7, true, MPF>(a, e, cg, tile32);
+            else batch_march<float, 7, false, MPF>(a, e, cg, tile32);
         } else {
-            if (teno) batch_march<float, 5, true, MPF>(a, e, cg);
-            else batch_march<float, 5, false, MPF>(a, e, cg);
+            if (teno) batch_march<float, 5, true, MPF>(a, e, cg, tile32);
+            else batch_march<float, 5, false, MPF>(a, e, cg, tile32);
         }
     } else if (e.order == 7) {
-        if (teno) batch_march<double, 7, true, MPF>(a, e, cg);
-        else batch_march<double, 7, false, MPF>(a, e, cg);
+        if (teno) batch_march<double, 7, true, MPF>(a, e, cg, tile);
+        else batch_march<double, 7, false, MPF>(a, e, cg, tile);
     } else {
-        if (teno) batch_march<double, 5, true, MPF>(a, e, cg);
-        else batch_march<double, 5, false, MPF>(a, e, cg);
+        if (teno) batch_march<double, 5, true, MPF>(a, e, cg, tile);
+        else batch_march<double, 5, false, MPF>(a, e, cg, tile);
     }
 }
 
@@ -184,6 +213,8 @@ __global__ void __launch_bounds__(256, WSB_BATCH_MIN_BLOCKS)
     __shared__ long long s_item;
     __shared__ int s_entry;
     __shared__ MarchArgs s_ma;   // marching items: the entry's arguments
+    // marching items: per warp, vL / vR of kBatchF faces x 32 columns (8 warps of 256 threads)
+    __shared__ double s_tile[8][2][kBatchF][33];
     int ma_loaded = -1;          // index of the MarchArgs in s_ma (same on every thread)
     while (true) {
         if (threadIdx.x == 0) {
@@ -217,8 +248,9 @@ __global__ void __launch_bounds__(256, WSB_BATCH_MIN_BLOCKS)
                 ma_loaded = k;
                 __syncthreads();
             }
-            if (e.mp) batch_march_dispatch<true>(s_ma, e, local);
-            else batch_march_dispatch<false>(s_ma, e, local);
+            double(*tile)[kBatchF][33] = s_tile[threadIdx.x >> 5];
+            if (e.mp) batch_march_dispatch<true>(s_ma, e, local, tile);
+            else batch_march_dispatch<false>(s_ma, e, local, tile);
             continue;
         }
         const int jt = (int)(local % e.n_jt);
