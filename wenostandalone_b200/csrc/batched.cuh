@@ -15,8 +15,9 @@
 // drop-in layout and for x; L1 serves the overlap of neighbouring faces).
 //
 // Entries whose coefficient arrays are the same on every face (checked when
-// the batch is built) and that a marching engine covers (WENO5 / WENO7 with
-// JS or TENO weights, FP64 or FP32-bulk) take marching items instead: an item
+// the batch is built) and that a marching engine covers (WENO3 with JS
+// weights, WENO5 / WENO7 with JS or TENO weights; FP64 or FP32-bulk) take
+// marching items instead: an item
 // is one CTA-width group of columns, each thread marches its own column over
 // the core faces (sweep_march.cuh engines) with the entry's MarchArgs copied
 // to shared memory, so each face costs one new cell and one new difference
@@ -130,6 +131,11 @@ __device__ __forceinline__ void batch_march_dispatch(const MarchArgs& a, const B
     float (*tile32)[kBatchF][33] = reinterpret_cast<float (*)[kBatchF][33]>(tile);
     // (the redo sequences take the weights from the arguments)
     const bool teno = e.wp.scheme == TENO;
+    if (e.order == 3) {
+        if (e.fp32) batch_march<float, 3, false, MPF>(a, e, cg, tile32);
+        else batch_march<double, 3, false, MPF>(a, e, cg, tile);
+        return;
+    }
     if (e.fp32) {
         if (e.order == 7) {
             if (teno) batch_march<float, 7, true, MPF>(a, e, cg, tile32);

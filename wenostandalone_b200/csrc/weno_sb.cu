@@ -1104,10 +1104,7 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
         const bool js = b.grid.scheme == WENO_SB_JS;
         const bool teno = b.grid.scheme == WENO_SB_TENO;
         double ucf[56];
-        // (WENO3 stays on per-face items: its one-thread-per-column march
-        // reads x columns uncoalesced and measured slower than the per-face
-        // items, whose stencils are cheap)
-        if (kernel_choice() != 1 && (b.order == 5 || b.order == 7) && (js || teno) &&
+        if (kernel_choice() != 1 && ((b.order == 5 || b.order == 7) && (js || teno) || (b.order == 3 && js)) &&
             batch_coefs_uniform(b.coefs, e.g.nc, b.order, ucf) && march_weights_ok(ucf, b.order)) {
             B->margs.push_back(make_march_args(e.g, b.v_in, b.vL, b.vR, e.wp, ucf, b.order));
             e.march = (int)B->margs.size();
