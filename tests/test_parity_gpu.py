@@ -148,18 +148,28 @@ def test_reconstruction_parity(wsb, oracle_mod, order, scheme, folded, mp, kerne
                 assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
 
 
+def _check(Lg, Rg, Lr, Rr, scheme, what):
+    if scheme == 3:
+        for got, ref in ((Lg, Lr), (Rg, Rr)):
+            assert np.array_equal(np.isnan(got), np.isnan(ref)), what
+            assert _flip_fraction(np.nan_to_num(got), np.nan_to_num(ref), TOL64) <= 1e-4, what
+    else:
+        eL, eR = rel_err(Lg, Lr), rel_err(Rg, Rr)
+        assert eL <= TOL64 and eR <= TOL64, (what, eL, eR)
+
+
 @pytest.mark.parametrize("kernel", ["auto", "march", "tma", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
-@pytest.mark.parametrize("order", [3, 5, 7])
-def test_face_varying_coefficients(wsb, oracle_mod, order, folded, mp, kernel):
+@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3)])
+def test_face_varying_coefficients(wsb, oracle_mod, order, scheme, folded, mp, kernel):
     """Every face has its own coefficients: catches a kernel that reads
-    another face's (or one shared) coefficient set."""
+    another face's (or one shared) coefficient set.  WENO5 with TENO weights
+    too (the per-face table of the marching kernel; cutoff flips counted)."""
     for dims in GRIDS:
         for d in range(3):
-            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, order, 0, folded, mp, kernel, "varying")
-            eL, eR = rel_err(Lg, Lr), rel_err(Rg, Rr)
-            assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
+            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel, "varying")
+            _check(Lg, Rg, Lr, Rr, scheme, (dims, d))
 
 
 @pytest.mark.parametrize("kernel", ["auto", "march", "march_ldg", "tma", "cpasync", "generic"])
@@ -182,10 +192,11 @@ def test_uniform_entry_parity(wsb, oracle_mod, order, scheme, folded, mp, kernel
                 assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
 
 
+@pytest.mark.parametrize("scheme", [0, 3])
 @pytest.mark.parametrize("kind", ["negative", "negative_uniform"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
-def test_negative_ideal_weights(wsb, oracle_mod, kind, folded, mp):
+def test_negative_ideal_weights(wsb, oracle_mod, kind, folded, mp, scheme):
     """Ideal weights below zero on some faces (per-face arrays) or on all
     (face-independent entry): the marching kernels' one-sided MP median needs
     non-negative weights, so those faces are redone from the arrays and the
@@ -196,10 +207,9 @@ def test_negative_ideal_weights(wsb, oracle_mod, kind, folded, mp):
     entry = "uniform" if kind == "negative_uniform" else "arrays"
     for dims in GRIDS:
         for d in range(3):
-            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, 5, 0, folded, mp, "auto", kind, entry=entry,
+            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, 5, scheme, folded, mp, "auto", kind, entry=entry,
                                        smooth=True)
-            eL, eR = rel_err(Lg, Lr), rel_err(Rg, Rr)
-            assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
+            _check(Lg, Rg, Lr, Rr, scheme, (dims, d))
 
 
 def _cudart():

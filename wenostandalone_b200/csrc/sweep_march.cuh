@@ -29,6 +29,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "weno_math.cuh"
 #include "sweep_generic.cuh"
 
@@ -656,6 +658,10 @@ struct March64 {
     // sum leaves the range of the reciprocal form (the caller redoes the face).
     template <bool MPF>
     __device__ __forceinline__ bool face_teno(const MarchArgs& a, double& L, double& R) const {
+        return face_teno<MPF, ParamCoefs>(a, ParamCoefs{a}, L, R);
+    }
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, const C& c, double& L, double& R) const {
         const double tau = fabs(b2 - b0);
         const double t0 = fma(tau, rcp1(b0), 1.0), t1 = fma(tau, rcp1(b1), 1.0), t2 = fma(tau, rcp1(b2), 1.0);
         const double x0 = t0 * t0, x1 = t1 * t1, x2 = t2 * t2;
@@ -666,16 +672,19 @@ struct March64 {
         const bool s_ok = mid_range_prod(s);
         const double rs = rcp1(s), ct = a.wp.teno_ct;
         const bool k0 = !(al0 * rs < ct), k1 = !(al1 * rs < ct), k2 = !(al2 * rs < ct);
-        const double eL0 = fma(a.kL[1], d0, a.kL[0] * dp1), eL1 = fma(a.kL[3], dm1, a.kL[2] * d0),
-                     eL2 = fma(a.kL[5], dm2, a.kL[4] * dm1);
-        const double eR0 = fma(a.kR[1], d0, a.kR[0] * dp1), eR1 = fma(a.kR[3], dm1, a.kR[2] * d0),
-                     eR2 = fma(a.kR[5], dm2, a.kR[4] * dm1);
+        const double eL0 = fma(c.kL(1), d0, c.kL(0) * dp1), eL1 = fma(c.kL(3), dm1, c.kL(2) * d0),
+                     eL2 = fma(c.kL(5), dm2, c.kL(4) * dm1);
+        const double eR0 = fma(c.kR(1), d0, c.kR(0) * dp1), eR1 = fma(c.kR(3), dm1, c.kR(2) * d0),
+                     eR2 = fma(c.kR(5), dm2, c.kR(4) * dm1);
         const double EL = ((k0 ? eL0 : 0.0) + (k1 ? eL1 : 0.0)) + (k2 ? eL2 : 0.0);
         const double ER = ((k0 ? eR0 : 0.0) + (k1 ? eR1 : 0.0)) + (k2 ? eR2 : 0.0);
-        const double SL = ((k0 ? a.ucf[12] : 0.0) + (k1 ? a.ucf[13] : 0.0)) + (k2 ? a.ucf[14] : 0.0);
-        const double SR = ((k0 ? a.ucf[15] : 0.0) + (k1 ? a.ucf[16] : 0.0)) + (k2 ? a.ucf[17] : 0.0);
+        const double SL = ((k0 ? c.dL(0) : 0.0) + (k1 ? c.dL(1) : 0.0)) + (k2 ? c.dL(2) : 0.0);
+        const double SR = ((k0 ? c.dR(0) : 0.0) + (k1 ? c.dR(1) : 0.0)) + (k2 ? c.dR(2) : 0.0);
         const double p = SL * SR;
-        const bool ok = s_ok && mid_range_prod(p);
+        bool ok = s_ok && mid_range_prod(p);
+        // a per-face row marks a face with a negative ideal weight by a NaN in
+        // dL(0), which the cutoff may leave out of the sums: test it here
+        if constexpr (!std::is_same_v<C, ParamCoefs>) ok = ok && (c.dL(0) == c.dL(0));
         const double r = rcp1(p);
         L = fma(EL * SR, r, v0);
         R = fma(ER * SL, r, v0);
@@ -914,7 +923,7 @@ __device__ __noinline__ void march64_redo_faces(const MarchArgs& a, const double
     const double* p = col + (o + 1) * a.sJ;
     const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
                  vp2 = __ldg(p + 4 * a.sJ);
-    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, JS, a.wp.eps, 0.0, L, R);
+    weno5_face<double>(vm2, vm1, v0, vp1, vp2, c, a.wp.scheme, a.wp.eps, a.wp.teno_ct, L, R);
     if (MPF) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
 }
 

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
     static_assert(ORDER == 5 || (ORDER != 5 && !PF), "WENO3 / WENO7: face-independent coefficients");
-    static_assert(!TENOW || !PF, "TENO: face-independent coefficients");
+    static_assert(!TENOW || !PF || ORDER == 5, "TENO with a per-face table: WENO5");
     using Engine = std::conditional_t<
         ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
         std::conditional_t<ORDER == 3, std::conditional_t<sizeof(T) == 8, March64_3, March32_3>,
@@ -318,7 +318,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
             } else if constexpr (PF) {
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
-                ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
+                if constexpr (TENOW) ok = w.template face_teno<MPF>(a, FaceRow(row(3)), L, R);
+                else ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
             } else if constexpr (TENOW) {
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
                 ok = w.template face_teno<MPF>(a, L, R);
@@ -390,7 +391,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 }
                 T L, R;
                 bool ok;
-                if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
+                if constexpr (PF && TENOW) ok = w.template face_teno<MPF>(a, FaceRow(srow(kc, i)), L, R);
+                else if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
                 else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, f0 + i >= 3 && f0 + i <= o_last - 4);
                 else ok = w.template face<MPF>(a, L, R);
@@ -586,9 +588,19 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
         {{sweep_march_tma_kernel<true, 0, T, 0, false>, sweep_march_tma_kernel<true, 0, T, 1, false>},
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
-    if (teno) {
+    if (teno && a.ftab) {
+        // WENO5-TENO with the per-face table: FP64 with TMA input tiles
+        if constexpr (sizeof(T) == 8) {
+            if (ldr || order != 5) return 1003;
+            static const KFn ptablet[2][2] = {
+                {sweep_march_tma_kernel<false, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<false, 1, T, 0, true, 5, true>},
+                {sweep_march_tma_kernel<true, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<true, 1, T, 0, true, 5, true>}};
+            kfn = ptablet[mp ? 1 : 0][kind1 ? 1 : 0];
+        } else {
+            return 1003;
+        }
+    } else if (teno) {
         // TENO weights, WENO5 or WENO7: face-independent coefficients
-        if (a.ftab) return 1003;
         static const KFn tablet[2][2][2][2] = {
             {{{sweep_march_tma_kernel<false, 0, T, 0, false, 5, true>,
                sweep_march_tma_kernel<false, 0, T, 1, false, 5, true>},

@@ -301,7 +301,8 @@ bool march_weights_ok(const double* ucf, int order = 5) {
 // stream-ordered.  Returns WENO_SB_ERR_UNSUPPORTED when the layout does not
 // suit the kernel.
 int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const double* in,
-                       double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st) {
+                       double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st,
+                       bool teno = false) {
     if (!cp.polyL || !cp.polyR || !cp.dL || !cp.dR || !cp.beta) return WENO_SB_ERR_UNSUPPORTED;
     if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
     const int rows = (int)g.ns + 16;
@@ -311,7 +312,7 @@ int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool f
     MarchArgs a0 = make_march_args(g, in, vL, vR, wp, nullptr);
     a0.ftab = tab;
     a0.cp = cp;
-    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
+    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 5, teno);
     const cudaError_t le = cudaGetLastError();
     WSB_CUDA(cudaFreeAsync(tab, st));
     if (rc) return rc;
@@ -363,8 +364,9 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
     }
     if constexpr (sizeof(T) == 8) {
-        if ((choice == 0 || choice == 3) && !ucf && order == 5 && gr->scheme == WENO_SB_JS) {
-            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st);
+        if ((choice == 0 || choice == 3) && !ucf && order == 5 &&
+            (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) {
+            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme == WENO_SB_TENO);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc;
         }
     }
