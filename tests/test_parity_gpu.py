@@ -192,11 +192,12 @@ def test_uniform_entry_parity(wsb, oracle_mod, order, scheme, folded, mp, kernel
                 assert eL <= TOL64 and eR <= TOL64, (dims, d, eL, eR)
 
 
+@pytest.mark.parametrize("order", [5, 7])
 @pytest.mark.parametrize("scheme", [0, 3])
 @pytest.mark.parametrize("kind", ["negative", "negative_uniform"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
-def test_negative_ideal_weights(wsb, oracle_mod, kind, folded, mp, scheme):
+def test_negative_ideal_weights(wsb, oracle_mod, kind, folded, mp, scheme, order):
     """Ideal weights below zero on some faces (per-face arrays) or on all
     (face-independent entry): the marching kernels' one-sided MP median needs
     non-negative weights, so those faces are redone from the arrays and the
@@ -207,8 +208,8 @@ def test_negative_ideal_weights(wsb, oracle_mod, kind, folded, mp, scheme):
     entry = "uniform" if kind == "negative_uniform" else "arrays"
     for dims in GRIDS:
         for d in range(3):
-            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, 5, scheme, folded, mp, "auto", kind, entry=entry,
-                                       smooth=True)
+            Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, "auto", kind,
+                                       entry=entry, smooth=True)
             _check(Lg, Rg, Lr, Rr, scheme, (dims, d))
 
 

@@ -754,6 +754,62 @@ __device__ __noinline__ void march64_redo(const MarchArgs& a, const double* __re
 // Weights as March64: ideal weights folded into the candidate coefficients
 // (MarchArgs::kL7 / kR7), one reciprocal of S_L S_R, the one-sided MP median.
 // ---------------------------------------------------------------------
+// Coefficient sources of the WENO7 engine: ParamCoefs7 (kernel-parameter
+// bank) and Row7, one row of the per-face table read at each use (the rows
+// of a chunk sit in shared memory; reading them where they are used keeps
+// WENO7's already large register state from growing).  Row layout
+// (kFaceRow7 doubles): [0..11] kL7, [12..23] kR7, [24..27] dL, [28..31] dR,
+// [32 + 6r + q] the beta coefficients of row r that the triple pushed into
+// face f enters (stencil 3 - r of face f + r).
+constexpr int kFaceRow7 = 56;
+
+struct ParamCoefs7 {
+    const MarchArgs& a;
+    __device__ __forceinline__ double kL(int q) const { return a.kL7[q]; }
+    __device__ __forceinline__ double kR(int q) const { return a.kR7[q]; }
+    __device__ __forceinline__ double dL(int s) const { return a.ucf[24 + s]; }
+    __device__ __forceinline__ double dR(int s) const { return a.ucf[28 + s]; }
+    __device__ __forceinline__ double b(int r, int q) const { return a.ucf[32 + 6 * r + q]; }
+};
+
+struct Row7 {
+    const double* p;
+    __device__ __forceinline__ double kL(int q) const { return p[q]; }
+    __device__ __forceinline__ double kR(int q) const { return p[12 + q]; }
+    __device__ __forceinline__ double dL(int s) const { return p[24 + s]; }
+    __device__ __forceinline__ double dR(int s) const { return p[28 + s]; }
+    __device__ __forceinline__ double b(int r, int q) const { return p[32 + 6 * r + q]; }
+};
+
+// The WENO7 per-face table (rows f = 0 .. rows-1, core face c(f) =
+// clamp(f - 3, 0, nc - 1); f90:1462-1488 read polyL/R(j, r, s), d(r, j) and
+// beta_coef(j, r, s) at the core index): kL7[3s+t] = dL(s) polyL(c, 3-s, t),
+// kR7 likewise, dL, dR, and beta_coef(c(f + r), r, q).  A negative ideal
+// weight puts a NaN in dL(0), as march_face_table_kernel.
+__global__ void march_face_table7_kernel(CoefPtrs cp, long long nc, int rows, double* __restrict__ tab) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= rows) return;
+    auto core = [&](long long x) { x -= 3; return x < 0 ? 0 : (x > nc - 1 ? nc - 1 : x); };
+    const long long c = core(f);
+    double* row = tab + (long long)f * kFaceRow7;
+    bool neg = false;
+    for (int s = 0; s < 4; ++s) {
+        const double dl = cp.dL[s + 5 * c], dr = cp.dR[s + 5 * c];
+        neg |= !(dl >= 0.0) || !(dr >= 0.0);
+        for (int t = 0; t < 3; ++t) {
+            row[3 * s + t] = dl * cp.polyL[c + nc * ((3 - s) + 5 * t)];
+            row[12 + 3 * s + t] = dr * cp.polyR[c + nc * ((3 - s) + 5 * t)];
+        }
+        row[24 + s] = dl;
+        row[28 + s] = dr;
+    }
+    for (int r = 0; r < 4; ++r) {
+        const long long cr = core(f + r);
+        for (int q = 0; q < 6; ++q) row[32 + 6 * r + q] = cp.beta[cr + nc * (r + 5 * q)];
+    }
+    if (neg) row[24] = __longlong_as_double(0x7ff8000000000000LL);
+}
+
 struct March64_7 {
     double vm1, v0, vp1, vp2, vp3;        // cells J-1 .. J+3
     double dm3, dm2, dm1, d0, dp1, dp2;    // d[k] = v[k+1] - v[k], k = J-3 .. J+2
@@ -763,33 +819,50 @@ struct March64_7 {
     double e2, mA, mB;                     // d[J+1] - d[J]; minmods of the MP limiter
 
     // beta of coefficient row r from the products of a triple (a newest, e oldest)
+    template <class C>
+    __device__ __forceinline__ static double beta_row(const MarchArgs& a, const C& c, int r, double aa, double ab,
+                                                      double ae, double bb, double be, double ee) {
+        return fma(c.b(r, 0), aa, fma(c.b(r, 1), ab, fma(c.b(r, 2), ae,
+                   fma(c.b(r, 3), bb, fma(c.b(r, 4), be, fma(c.b(r, 5), ee, a.wp.eps))))));
+    }
+    template <class C>
+    __device__ __forceinline__ static double beta_row(const MarchArgs& a, const C& c, int r, double x, double y,
+                                                      double z) {
+        // triple (e, b, a) = (x, y, z)
+        return beta_row(a, c, r, z * z, z * y, z * x, y * y, y * x, x * x);
+    }
     __device__ __forceinline__ static double beta_row(const MarchArgs& a, int r, double aa, double ab, double ae,
                                                       double bb, double be, double ee) {
-        const int o = 32 + 6 * r;
-        return fma(a.ucf[o], aa, fma(a.ucf[o + 1], ab, fma(a.ucf[o + 2], ae,
-                   fma(a.ucf[o + 3], bb, fma(a.ucf[o + 4], be, fma(a.ucf[o + 5], ee, a.wp.eps))))));
+        return beta_row(a, ParamCoefs7{a}, r, aa, ab, ae, bb, be, ee);
     }
     __device__ __forceinline__ static double beta_row(const MarchArgs& a, int r, double x, double y, double z) {
-        // triple (e, b, a) = (x, y, z)
-        return beta_row(a, r, z * z, z * y, z * x, y * y, y * x, x * x);
+        return beta_row(a, ParamCoefs7{a}, r, x, y, z);
     }
 
-    // Window of face J from cells J-3 .. J+3.
+    // Window of face J from cells J-3 .. J+3; cm3 .. cz are the beta sources
+    // of the triples starting at d[J-3] .. d[J].
     __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3, double c4,
+                                         double c5, double c6) {
+        const ParamCoefs7 u{a};
+        init(a, u, u, u, u, c0, c1, c2, c3, c4, c5, c6);
+    }
+    template <class C3, class C2, class C1, class C0>
+    __device__ __forceinline__ void init(const MarchArgs& a, const C3& cm3, const C2& cm2, const C1& cm1,
+                                         const C0& cz, double c0, double c1, double c2, double c3, double c4,
                                          double c5, double c6) {
         vm1 = c2; v0 = c3; vp1 = c4; vp2 = c5; vp3 = c6;
         dm3 = c1 - c0; dm2 = c2 - c1; dm1 = c3 - c2; d0 = c4 - c3; dp1 = c5 - c4; dp2 = c6 - c5;
         s1 = dp1 * dp1; s2 = dp2 * dp2; c12 = dp1 * dp2;
-        const double b0 = beta_row(a, 3, dm3, dm2, dm1);               // T_{J-3}
-        const double b1 = beta_row(a, 2, dm2, dm1, d0);                // T_{J-2}
-        n0a = beta_row(a, 3, dm2, dm1, d0);
-        const double b2 = beta_row(a, 1, dm1, d0, dp1);                // T_{J-1}
-        n1a = beta_row(a, 2, dm1, d0, dp1);
-        n0b = beta_row(a, 3, dm1, d0, dp1);
-        const double b3 = beta_row(a, 0, d0, dp1, dp2);                // T_J
-        n2a = beta_row(a, 1, d0, dp1, dp2);
-        n1b = beta_row(a, 2, d0, dp1, dp2);
-        n0c = beta_row(a, 3, d0, dp1, dp2);
+        const double b0 = beta_row(a, cm3, 3, dm3, dm2, dm1);          // T_{J-3}
+        const double b1 = beta_row(a, cm2, 2, dm2, dm1, d0);           // T_{J-2}
+        n0a = beta_row(a, cm2, 3, dm2, dm1, d0);
+        const double b2 = beta_row(a, cm1, 1, dm1, d0, dp1);           // T_{J-1}
+        n1a = beta_row(a, cm1, 2, dm1, d0, dp1);
+        n0b = beta_row(a, cm1, 3, dm1, d0, dp1);
+        const double b3 = beta_row(a, cz, 0, d0, dp1, dp2);            // T_J
+        n2a = beta_row(a, cz, 1, d0, dp1, dp2);
+        n1b = beta_row(a, cz, 2, d0, dp1, dp2);
+        n0c = beta_row(a, cz, 3, d0, dp1, dp2);
         B0 = b0; B1 = b1; B2 = b2; B3 = b3;
         const double em = dm1 - dm2, ez = d0 - dm1;
         e2 = dp1 - d0;
@@ -797,14 +870,17 @@ struct March64_7 {
         mB = mm64(ez, e2);
     }
 
-    // Advance to face J+1; n is cell J+4.
-    __device__ __forceinline__ void push(const MarchArgs& a, double n) {
+    // Advance to face J+1; n is cell J+4; c is the beta source of the new
+    // triple (d[J+1], d[J+2], d[J+3]).
+    __device__ __forceinline__ void push(const MarchArgs& a, double n) { push(a, ParamCoefs7{a}, n); }
+    template <class C>
+    __device__ __forceinline__ void push(const MarchArgs& a, const C& c, double n) {
         const double dn = n - vp3;
         const double aa = dn * dn, ab = dn * dp2, ae = dn * dp1;       // T_{J+1}: a = dn, b = dp2, e = dp1
-        const double g0 = beta_row(a, 0, aa, ab, ae, s2, c12, s1);
-        const double g1 = beta_row(a, 1, aa, ab, ae, s2, c12, s1);
-        const double g2 = beta_row(a, 2, aa, ab, ae, s2, c12, s1);
-        const double g3 = beta_row(a, 3, aa, ab, ae, s2, c12, s1);
+        const double g0 = beta_row(a, c, 0, aa, ab, ae, s2, c12, s1);
+        const double g1 = beta_row(a, c, 1, aa, ab, ae, s2, c12, s1);
+        const double g2 = beta_row(a, c, 2, aa, ab, ae, s2, c12, s1);
+        const double g3 = beta_row(a, c, 3, aa, ab, ae, s2, c12, s1);
         B0 = n0a; B1 = n1a; B2 = n2a; B3 = g0;
         n0a = n0b; n0b = n0c; n0c = g3;
         n1a = n1b; n1b = g2;
@@ -821,20 +897,24 @@ struct March64_7 {
     // out of range (the caller redoes the face).
     template <bool MPF>
     __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+        return face<MPF, ParamCoefs7>(a, ParamCoefs7{a}, L, R);
+    }
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool face(const MarchArgs& a, const C& c, double& L, double& R) const {
         const double q0 = B0 * B0, q1 = B1 * B1, q2 = B2 * B2, q3 = B3 * B3;
         const double q01 = q0 * q1, q23 = q2 * q3;
         const double P0 = q1 * q23, P1 = q0 * q23, P2 = q01 * q3, P3 = q01 * q2;
-        const double SL = fma(a.ucf[24], P0, fma(a.ucf[25], P1, fma(a.ucf[26], P2, a.ucf[27] * P3)));
-        const double SR = fma(a.ucf[28], P0, fma(a.ucf[29], P1, fma(a.ucf[30], P2, a.ucf[31] * P3)));
+        const double SL = fma(c.dL(0), P0, fma(c.dL(1), P1, fma(c.dL(2), P2, c.dL(3) * P3)));
+        const double SR = fma(c.dR(0), P0, fma(c.dR(1), P1, fma(c.dR(2), P2, c.dR(3) * P3)));
         // stencil s: (a, b, e) = (d[J+s-1], d[J+s-2], d[J+s-3])
-        const double eL0 = fma(a.kL7[0], dm1, fma(a.kL7[1], dm2, a.kL7[2] * dm3));
-        const double eL1 = fma(a.kL7[3], d0, fma(a.kL7[4], dm1, a.kL7[5] * dm2));
-        const double eL2 = fma(a.kL7[6], dp1, fma(a.kL7[7], d0, a.kL7[8] * dm1));
-        const double eL3 = fma(a.kL7[9], dp2, fma(a.kL7[10], dp1, a.kL7[11] * d0));
-        const double eR0 = fma(a.kR7[0], dm1, fma(a.kR7[1], dm2, a.kR7[2] * dm3));
-        const double eR1 = fma(a.kR7[3], d0, fma(a.kR7[4], dm1, a.kR7[5] * dm2));
-        const double eR2 = fma(a.kR7[6], dp1, fma(a.kR7[7], d0, a.kR7[8] * dm1));
-        const double eR3 = fma(a.kR7[9], dp2, fma(a.kR7[10], dp1, a.kR7[11] * d0));
+        const double eL0 = fma(c.kL(0), dm1, fma(c.kL(1), dm2, c.kL(2) * dm3));
+        const double eL1 = fma(c.kL(3), d0, fma(c.kL(4), dm1, c.kL(5) * dm2));
+        const double eL2 = fma(c.kL(6), dp1, fma(c.kL(7), d0, c.kL(8) * dm1));
+        const double eL3 = fma(c.kL(9), dp2, fma(c.kL(10), dp1, c.kL(11) * d0));
+        const double eR0 = fma(c.kR(0), dm1, fma(c.kR(1), dm2, c.kR(2) * dm3));
+        const double eR1 = fma(c.kR(3), d0, fma(c.kR(4), dm1, c.kR(5) * dm2));
+        const double eR2 = fma(c.kR(6), dp1, fma(c.kR(7), d0, c.kR(8) * dm1));
+        const double eR3 = fma(c.kR(9), dp2, fma(c.kR(10), dp1, c.kR(11) * d0));
         const double EL = fma(P0, eL0, fma(P1, eL1, fma(P2, eL2, P3 * eL3)));
         const double ER = fma(P0, eR0, fma(P1, eR1, fma(P2, eR2, P3 * eR3)));
         const double p = SL * SR;
@@ -900,6 +980,22 @@ struct March64_7 {
         return ok;
     }
 };
+// The reference sequence for one WENO7 face with face-dependent
+// coefficients: core face o - 3 of the arrays.
+template <bool MPF>
+__device__ __noinline__ void march64_7_redo_faces(const MarchArgs& a, const double* __restrict__ col, long long o,
+                                                  double& L, double& R) {
+    Coef<7> c;
+    long long ci = o - 3;
+    ci = ci < 0 ? 0 : (ci > a.nc - 1 ? a.nc - 1 : ci);
+    c.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, ci);
+    double v[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) v[q] = __ldg(col + (o + q) * a.sJ);
+    weno7_face<double>(v + 3, c, a.wp.scheme, a.wp.eps, a.wp.teno_ct, L, R);
+    if (MPF) mp_limit(v[1], v[2], v[3], v[4], v[5], L, R);
+}
+
 // The reference sequence for one WENO7 face (cells o .. o+6 of the column).
 template <bool MPF>
 __device__ __noinline__ void march64_7_redo(const MarchArgs& a, const double* __restrict__ col, long long o,

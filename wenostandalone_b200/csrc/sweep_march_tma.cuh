@@ -70,8 +70,10 @@ constexpr int kTmaOut = WSB_MTMA_OUTBUF;
 #endif
 constexpr int kPfStages = WSB_MTMA_PF_STAGES;
 constexpr int kPfOut = WSB_MTMA_PF_OUTBUF;
-constexpr int kPfRowBytes = (kTmaF + 1) * kFaceRow * 8;  // rows f0 .. f0 + 8 of a chunk
-static_assert(kPfRowBytes % 16 == 0, "bulk copies move 16-byte multiples");
+// rows f0 .. f0 + 8 of a chunk (WENO5 / WENO7 table rows)
+__host__ __device__ constexpr int pf_row_doubles(int order) { return order == 7 ? kFaceRow7 : kFaceRow; }
+__host__ __device__ constexpr int pf_chunk_bytes(int order) { return (kTmaF + 1) * pf_row_doubles(order) * 8; }
+static_assert(pf_chunk_bytes(5) % 16 == 0 && pf_chunk_bytes(7) % 16 == 0, "bulk copies move 16-byte multiples");
 static_assert(WSB_MTMA_PF_STAGES <= 4 && WSB_MTMA_PF_STAGES >= 2, "stages of the per-face kernels");
 #ifndef WSB_MTMA_WARPS
 #define WSB_MTMA_WARPS 4        // warps per CTA (each with its own pipeline)
@@ -170,7 +172,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
-    static_assert(ORDER == 5 || (ORDER != 5 && !PF), "WENO3 / WENO7: face-independent coefficients");
+    static_assert(ORDER != 3 || !PF, "WENO3: face-independent coefficients");
+    static_assert(ORDER != 7 || !PF || (!TENOW && sizeof(T) == 8), "WENO7 per-face table: FP64, JS");
+    constexpr int RW = pf_row_doubles(ORDER), RB = pf_chunk_bytes(ORDER);  // per-face table rows
     static_assert(!TENOW || !PF || ORDER == 5, "TENO with a per-face table: WENO5");
     using Engine = std::conditional_t<
         ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
@@ -207,9 +211,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     auto tile_ptr = [&](unsigned k) { return ring + (size_t)(k % S) * t.stage_bytes; };
     // per-face table rows (PF): in global memory, and the chunk's rows
     // staged with input tile k
-    auto row = [&](int f) { return a.ftab + (long long)f * kFaceRow; };
+    auto row = [&](int f) { return a.ftab + (long long)f * RW; };
     auto srow = [&](unsigned k, int i) {
-        return (const double*)(wbase + t.rows_off + (size_t)(k % S) * kPfRowBytes) + i * kFaceRow;
+        return (const double*)(wbase + t.rows_off + (size_t)(k % S) * RB) + i * RW;
     };
     // byte offset in a tile of position p (0..7) of this lane's column
     auto cell_off = [&](int p) -> unsigned {
@@ -229,10 +233,10 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 const int c0 = t.dimJ == 0 ? J0 : (t.dimU == 0 ? cU : cW);
                 const int c1 = t.dimJ == 1 ? J0 : (t.dimU == 1 ? cU : cW);
                 const int c2 = t.dimJ == 2 ? J0 : (t.dimU == 2 ? cU : cW);
-                mbar_arrive_expect_tx(bar, t.box_bytes + (PF ? (unsigned)kPfRowBytes : 0u));
+                mbar_arrive_expect_tx(bar, t.box_bytes + (PF ? (unsigned)RB : 0u));
                 tma_load_4d(tile_ptr(k), &tin, bar, c0, c1, c2, v);
                 // rows J0 .. J0 + 8: the faces of the chunk starting at face J0
-                if constexpr (PF) bulk_load_1d((void*)srow(k, 0), row(J0), kPfRowBytes, bar);
+                if constexpr (PF) bulk_load_1d((void*)srow(k, 0), row(J0), RB, bar);
             }
         } else {
             // each lane copies its own column's cells; cells past the end of
@@ -312,9 +316,15 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
             if constexpr (ORDER == 7) {
                 // face 3 reads cells 3 .. 9: cell 3 lies before tile 0 (cells 4 .. 11)
                 const T c3 = __ldg(column(u0, wv, vv) + 3 * a.sJ);
-                w.init(a, c3, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
-                if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
-                else ok = w.template face<MPF>(a, L, R);
+                if constexpr (PF) {
+                    w.init(a, Row7{row(0)}, Row7{row(1)}, Row7{row(2)}, Row7{row(3)}, c3, cell(k0, 0), cell(k0, 1),
+                           cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
+                    ok = w.template face<MPF>(a, Row7{row(3)}, L, R);
+                } else {
+                    w.init(a, c3, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
+                    if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
+                    else ok = w.template face<MPF>(a, L, R);
+                }
             } else if constexpr (PF) {
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
@@ -329,7 +339,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
             }
             if (!ok) {
                 // (the redo sequences take the weights from the arguments)
-                if constexpr (ORDER == 7) march7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
+                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(a, column(u0, wv, vv), 3, L, R);
+                else if constexpr (ORDER == 7) march7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
                 else march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
             }
             if (u0 + lane < a.Nu) {
@@ -337,11 +348,15 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 outL[oi] = L;
                 outR[oi] = R;
             }
-            if constexpr (ORDER == 7) w.push(a, cell(k0, 6));
+            if constexpr (ORDER == 7 && PF) w.push(a, Row7{row(4)}, cell(k0, 6));
+            else if constexpr (ORDER == 7) w.push(a, cell(k0, 6));
             else if constexpr (PF) w.push(a, BetaRow(row(4)), cell(k0, 5));
             else w.push(a, cell(k0, 5));
         } else {
-            if constexpr (ORDER == 7)
+            if constexpr (ORDER == 7 && PF)
+                w.init(a, Row7{row(f_start - 3)}, Row7{row(f_start - 2)}, Row7{row(f_start - 1)}, Row7{row(f_start)},
+                       cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5), cell(k0, 6));
+            else if constexpr (ORDER == 7)
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5), cell(k0, 6));
             else if constexpr (PF)
                 w.init(a, BetaRow(row(f_start - 2)), BetaRow(row(f_start - 1)), BetaRow(row(f_start)), cell(k0, 1),
@@ -391,7 +406,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 }
                 T L, R;
                 bool ok;
-                if constexpr (PF && TENOW) ok = w.template face_teno<MPF>(a, FaceRow(srow(kc, i)), L, R);
+                if constexpr (PF && ORDER == 7) ok = w.template face<MPF>(a, Row7{srow(kc, i)}, L, R);
+                else if constexpr (PF && TENOW) ok = w.template face_teno<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
                 else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, f0 + i >= 3 && f0 + i <= o_last - 4);
@@ -416,7 +432,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 T n;
                 if constexpr (KIND == 0) n = cg[pq % G];
                 else n = cell(kq, pq);
-                if constexpr (PF) w.push(a, BetaRow(srow(kc, i + 1)), n);
+                if constexpr (PF && ORDER == 7) w.push(a, Row7{srow(kc, i + 1)}, n);
+                else if constexpr (PF) w.push(a, BetaRow(srow(kc, i + 1)), n);
                 else w.push(a, n);
             }
             const int nF = f_end - f0 < F ? f_end - f0 : F;
@@ -427,7 +444,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
+                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(a, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
                     else if constexpr (ORDER == 3) march3_redo<MPF, T>(a, col, f0 + i, L, R);
                     else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
@@ -579,7 +597,8 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     const int out_bytes = (pf ? kPfOut : kTmaOut) * 2 * 32 * kTmaF * ES;
     t.ring_off = out_bytes;
     t.rows_off = out_bytes + nst * t.stage_bytes;
-    t.warp_bytes = ((t.rows_off + (pf ? nst * kPfRowBytes : 0) + 1023) / 1024) * 1024;
+    t.warp_bytes = ((t.rows_off + (pf ? nst * (order == 7 ? pf_chunk_bytes(7) : pf_chunk_bytes(5)) : 0) + 1023) /
+                    1024) * 1024;
     const size_t smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * nst * 8;
     using KFn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, MarchArgs, MarchTmaArgs);
     static const KFn table[2][2][2] = {
@@ -628,9 +647,19 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
             {{sweep_march_tma_kernel<true, 0, T, 0, false, 3>, sweep_march_tma_kernel<true, 0, T, 1, false, 3>},
              {sweep_march_tma_kernel<true, 1, T, 0, false, 3>, sweep_march_tma_kernel<true, 1, T, 1, false, 3>}}};
         kfn = table3[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+    } else if (order == 7 && a.ftab) {
+        // WENO7-JS with the per-face table: FP64 with TMA input tiles
+        if constexpr (sizeof(T) == 8) {
+            if (ldr) return 1003;
+            static const KFn ptable7[2][2] = {
+                {sweep_march_tma_kernel<false, 0, T, 0, true, 7>, sweep_march_tma_kernel<false, 1, T, 0, true, 7>},
+                {sweep_march_tma_kernel<true, 0, T, 0, true, 7>, sweep_march_tma_kernel<true, 1, T, 0, true, 7>}};
+            kfn = ptable7[mp ? 1 : 0][kind1 ? 1 : 0];
+        } else {
+            return 1003;
+        }
     } else if (order == 7) {
         // WENO7: face-independent coefficients
-        if (a.ftab) return 1003;
         static const KFn table7[2][2][2] = {
             {{sweep_march_tma_kernel<false, 0, T, 0, false, 7>, sweep_march_tma_kernel<false, 0, T, 1, false, 7>},
              {sweep_march_tma_kernel<false, 1, T, 0, false, 7>, sweep_march_tma_kernel<false, 1, T, 1, false, 7>}},

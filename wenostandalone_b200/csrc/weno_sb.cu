@@ -294,25 +294,26 @@ bool march_weights_ok(const double* ucf, int order = 5) {
     return true;
 }
 
-// FP64 WENO5-JS marching sweep with face-dependent coefficient arrays: the
-// per-face table (one 224-byte row per face; ns + 16 rows: the kernel stages
-// rows f0 .. f0 + 8 with every input tile, and its last tile starts below
-// ns + 5) is built on the stream, used by the TMA marching kernel and freed
-// stream-ordered.  Returns WENO_SB_ERR_UNSUPPORTED when the layout does not
-// suit the kernel.
+// FP64 marching sweep with face-dependent coefficient arrays (WENO5 with JS
+// or TENO weights, WENO7-JS): the per-face table (one row per face, 224 bytes
+// for WENO5, 448 for WENO7; ns + 16 rows: the kernel stages rows f0 .. f0 + 8
+// with every input tile, and its last tile starts below ns + 5) is built on
+// the stream, used by the TMA marching kernel and freed stream-ordered.
+// Returns WENO_SB_ERR_UNSUPPORTED when the layout does not suit the kernel.
 int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const double* in,
                        double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st,
-                       bool teno = false) {
+                       bool teno = false, int order = 5) {
     if (!cp.polyL || !cp.polyR || !cp.dL || !cp.dR || !cp.beta) return WENO_SB_ERR_UNSUPPORTED;
     if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
     const int rows = (int)g.ns + 16;
     double* tab = nullptr;
-    WSB_CUDA(cudaMallocAsync((void**)&tab, sizeof(double) * kFaceRow * (size_t)rows, st));
-    march_face_table_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
+    WSB_CUDA(cudaMallocAsync((void**)&tab, sizeof(double) * (order == 7 ? kFaceRow7 : kFaceRow) * (size_t)rows, st));
+    if (order == 7) march_face_table7_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
+    else march_face_table_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
     MarchArgs a0 = make_march_args(g, in, vL, vR, wp, nullptr);
     a0.ftab = tab;
     a0.cp = cp;
-    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 5, teno);
+    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, teno);
     const cudaError_t le = cudaGetLastError();
     WSB_CUDA(cudaFreeAsync(tab, st));
     if (rc) return rc;
@@ -364,9 +365,11 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
     }
     if constexpr (sizeof(T) == 8) {
-        if ((choice == 0 || choice == 3) && !ucf && order == 5 &&
-            (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) {
-            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme == WENO_SB_TENO);
+        if ((choice == 0 || choice == 3) && !ucf &&
+            ((order == 5 && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) ||
+             (order == 7 && gr->scheme == WENO_SB_JS))) {
+            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme == WENO_SB_TENO,
+                                        order);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc;
         }
     }
