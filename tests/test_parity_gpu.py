@@ -161,11 +161,12 @@ def _check(Lg, Rg, Lr, Rr, scheme, what):
 @pytest.mark.parametrize("kernel", ["auto", "march", "tma", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
-@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3)])
+@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3), (7, 3)])
 def test_face_varying_coefficients(wsb, oracle_mod, order, scheme, folded, mp, kernel):
     """Every face has its own coefficients: catches a kernel that reads
-    another face's (or one shared) coefficient set.  WENO5 with TENO weights
-    too (the per-face table of the marching kernel; cutoff flips counted)."""
+    another face's (or one shared) coefficient set.  WENO5 / WENO7 with TENO
+    weights too (the per-face table of the marching kernel; cutoff flips
+    counted)."""
     for dims in GRIDS:
         for d in range(3):
             Lg, Rg, Lr, Rr = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel, "varying")

@@ -955,24 +955,30 @@ struct March64_7 {
     // E_L = sum delta (kL . differences).
     template <bool MPF>
     __device__ __forceinline__ bool face_teno(const MarchArgs& a, double& L, double& R) const {
+        return face_teno<MPF, ParamCoefs7>(a, ParamCoefs7{a}, L, R);
+    }
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, const C& c, double& L, double& R) const {
         bool k0, k1, k2, k3;
         double a4;
         const bool ok0 = teno7_keep(B0, B1, B2, B3, a.wp.eps, a.wp.teno_ct, k0, k1, k2, k3, a4);
-        const double eL0 = fma(a.kL7[0], dm1, fma(a.kL7[1], dm2, a.kL7[2] * dm3));
-        const double eL1 = fma(a.kL7[3], d0, fma(a.kL7[4], dm1, a.kL7[5] * dm2));
-        const double eL2 = fma(a.kL7[6], dp1, fma(a.kL7[7], d0, a.kL7[8] * dm1));
-        const double eL3 = fma(a.kL7[9], dp2, fma(a.kL7[10], dp1, a.kL7[11] * d0));
-        const double eR0 = fma(a.kR7[0], dm1, fma(a.kR7[1], dm2, a.kR7[2] * dm3));
-        const double eR1 = fma(a.kR7[3], d0, fma(a.kR7[4], dm1, a.kR7[5] * dm2));
-        const double eR2 = fma(a.kR7[6], dp1, fma(a.kR7[7], d0, a.kR7[8] * dm1));
-        const double eR3 = fma(a.kR7[9], dp2, fma(a.kR7[10], dp1, a.kR7[11] * d0));
+        const double eL0 = fma(c.kL(0), dm1, fma(c.kL(1), dm2, c.kL(2) * dm3));
+        const double eL1 = fma(c.kL(3), d0, fma(c.kL(4), dm1, c.kL(5) * dm2));
+        const double eL2 = fma(c.kL(6), dp1, fma(c.kL(7), d0, c.kL(8) * dm1));
+        const double eL3 = fma(c.kL(9), dp2, fma(c.kL(10), dp1, c.kL(11) * d0));
+        const double eR0 = fma(c.kR(0), dm1, fma(c.kR(1), dm2, c.kR(2) * dm3));
+        const double eR1 = fma(c.kR(3), d0, fma(c.kR(4), dm1, c.kR(5) * dm2));
+        const double eR2 = fma(c.kR(6), dp1, fma(c.kR(7), d0, c.kR(8) * dm1));
+        const double eR3 = fma(c.kR(9), dp2, fma(c.kR(10), dp1, c.kR(11) * d0));
         const double EL = ((k0 ? eL0 : 0.0) + (k1 ? eL1 : 0.0)) + ((k2 ? eL2 : 0.0) + (k3 ? eL3 : 0.0));
         const double ER = ((k0 ? eR0 : 0.0) + (k1 ? eR1 : 0.0)) + ((k2 ? eR2 : 0.0) + (k3 ? eR3 : 0.0));
-        const double SL = ((k0 ? a.ucf[24] : 0.0) + (k1 ? a.ucf[25] : 0.0)) + ((k2 ? a.ucf[26] : 0.0) + (k3 ? a.ucf[27] : 0.0));
-        const double SR = ((k0 ? a.ucf[28] : 0.0) + (k1 ? a.ucf[29] : 0.0)) + ((k2 ? a.ucf[30] : 0.0) + (k3 ? a.ucf[31] : 0.0));
+        const double SL = ((k0 ? c.dL(0) : 0.0) + (k1 ? c.dL(1) : 0.0)) + ((k2 ? c.dL(2) : 0.0) + (k3 ? c.dL(3) : 0.0));
+        const double SR = ((k0 ? c.dR(0) : 0.0) + (k1 ? c.dR(1) : 0.0)) + ((k2 ? c.dR(2) : 0.0) + (k3 ? c.dR(3) : 0.0));
         const double DL = SL + a4, DR = SR + a4;
         const double p = DL * DR;
-        const bool ok = ok0 && mid_range_prod(p);
+        bool ok = ok0 && mid_range_prod(p);
+        // a per-face row's NaN mark (negative ideal weight) may be cut from the sums
+        if constexpr (!std::is_same_v<C, ParamCoefs7>) ok = ok && (c.dL(0) == c.dL(0));
         const double r = rcp1(p);
         L = fma(SL, v0, EL) * (DR * r);
         R = fma(SR, v0, ER) * (DL * r);

@@ -173,9 +173,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
     static_assert(ORDER != 3 || !PF, "WENO3: face-independent coefficients");
-    static_assert(ORDER != 7 || !PF || (!TENOW && sizeof(T) == 8), "WENO7 per-face table: FP64, JS");
+    static_assert(ORDER != 7 || !PF || sizeof(T) == 8, "WENO7 per-face table: FP64");
     constexpr int RW = pf_row_doubles(ORDER), RB = pf_chunk_bytes(ORDER);  // per-face table rows
-    static_assert(!TENOW || !PF || ORDER == 5, "TENO with a per-face table: WENO5");
+    static_assert(!TENOW || !PF || ORDER != 3, "TENO with a per-face table: WENO5 / WENO7");
     using Engine = std::conditional_t<
         ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
         std::conditional_t<ORDER == 3, std::conditional_t<sizeof(T) == 8, March64_3, March32_3>,
@@ -319,7 +319,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 if constexpr (PF) {
                     w.init(a, Row7{row(0)}, Row7{row(1)}, Row7{row(2)}, Row7{row(3)}, c3, cell(k0, 0), cell(k0, 1),
                            cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
-                    ok = w.template face<MPF>(a, Row7{row(3)}, L, R);
+                    if constexpr (TENOW) ok = w.template face_teno<MPF>(a, Row7{row(3)}, L, R);
+                    else ok = w.template face<MPF>(a, Row7{row(3)}, L, R);
                 } else {
                     w.init(a, c3, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
                     if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
@@ -406,7 +407,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 }
                 T L, R;
                 bool ok;
-                if constexpr (PF && ORDER == 7) ok = w.template face<MPF>(a, Row7{srow(kc, i)}, L, R);
+                if constexpr (PF && ORDER == 7 && TENOW) ok = w.template face_teno<MPF>(a, Row7{srow(kc, i)}, L, R);
+                else if constexpr (PF && ORDER == 7) ok = w.template face<MPF>(a, Row7{srow(kc, i)}, L, R);
                 else if constexpr (PF && TENOW) ok = w.template face_teno<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
@@ -608,13 +610,15 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     if (teno && a.ftab) {
-        // WENO5-TENO with the per-face table: FP64 with TMA input tiles
+        // TENO with the per-face table (WENO5, WENO7): FP64 with TMA input tiles
         if constexpr (sizeof(T) == 8) {
-            if (ldr || order != 5) return 1003;
-            static const KFn ptablet[2][2] = {
-                {sweep_march_tma_kernel<false, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<false, 1, T, 0, true, 5, true>},
-                {sweep_march_tma_kernel<true, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<true, 1, T, 0, true, 5, true>}};
-            kfn = ptablet[mp ? 1 : 0][kind1 ? 1 : 0];
+            if (ldr) return 1003;
+            static const KFn ptablet[2][2][2] = {
+                {{sweep_march_tma_kernel<false, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<false, 1, T, 0, true, 5, true>},
+                 {sweep_march_tma_kernel<true, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<true, 1, T, 0, true, 5, true>}},
+                {{sweep_march_tma_kernel<false, 0, T, 0, true, 7, true>, sweep_march_tma_kernel<false, 1, T, 0, true, 7, true>},
+                 {sweep_march_tma_kernel<true, 0, T, 0, true, 7, true>, sweep_march_tma_kernel<true, 1, T, 0, true, 7, true>}}};
+            kfn = ptablet[order == 7 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0];
         } else {
             return 1003;
         }

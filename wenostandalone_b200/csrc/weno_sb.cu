@@ -294,8 +294,8 @@ bool march_weights_ok(const double* ucf, int order = 5) {
     return true;
 }
 
-// FP64 marching sweep with face-dependent coefficient arrays (WENO5 with JS
-// or TENO weights, WENO7-JS): the per-face table (one row per face, 224 bytes
+// FP64 marching sweep with face-dependent coefficient arrays (WENO5 and
+// WENO7, JS or TENO weights): the per-face table (one row per face, 224 bytes
 // for WENO5, 448 for WENO7; ns + 16 rows: the kernel stages rows f0 .. f0 + 8
 // with every input tile, and its last tile starts below ns + 5) is built on
 // the stream, used by the TMA marching kernel and freed stream-ordered.
@@ -366,8 +366,7 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     }
     if constexpr (sizeof(T) == 8) {
         if ((choice == 0 || choice == 3) && !ucf &&
-            ((order == 5 && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) ||
-             (order == 7 && gr->scheme == WENO_SB_JS))) {
+            (order == 5 || order == 7) && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) {
             int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme == WENO_SB_TENO,
                                         order);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc;
