@@ -1376,6 +1376,55 @@ __device__ __noinline__ void march32_7_redo(const MarchArgs& a, const float* __r
 // face() takes that as an argument; the window is still cells J-2 .. J+2
 // for the limiter's minmods.
 // ---------------------------------------------------------------------
+// Coefficient sources of the FP64 WENO3 engine: ParamCoefs3 (kernel
+// parameters) and Row3, one row of the WENO3 per-face table (kFaceRow3
+// doubles: [0..1] kL, [2..3] kR, [4..5] dL, [6..7] dR, [8..9] beta_coef of
+// the face; a push into face f reads row f).
+constexpr int kFaceRow3 = 12;
+
+struct ParamCoefs3 {
+    const MarchArgs& a;
+    __device__ __forceinline__ double kL(int q) const { return a.kL[q]; }
+    __device__ __forceinline__ double kR(int q) const { return a.kR[q]; }
+    __device__ __forceinline__ double dL(int r) const { return a.ucf[4 + r]; }
+    __device__ __forceinline__ double dR(int r) const { return a.ucf[6 + r]; }
+    __device__ __forceinline__ double b(int r) const { return a.ucf[8 + r]; }
+};
+
+struct Row3 {
+    const double* p;
+    __device__ __forceinline__ double kL(int q) const { return p[q]; }
+    __device__ __forceinline__ double kR(int q) const { return p[2 + q]; }
+    __device__ __forceinline__ double dL(int r) const { return p[4 + r]; }
+    __device__ __forceinline__ double dR(int r) const { return p[6 + r]; }
+    __device__ __forceinline__ double b(int r) const { return p[8 + r]; }
+};
+
+// The WENO3 per-face table (f90:416-468: polyL/R(j, r, 0), d(r, j),
+// beta_coef(j, r, 0) at the core index c(f) = clamp(f - 3, 0, nc - 1), the
+// convention of every kernel here for the faces outside the core): kL[r] =
+// dL(r) polyL(c, r, 0), kR likewise, dL, dR, beta_coef(c, r, 0).  A negative
+// ideal weight puts a NaN in dL(0).
+__global__ void march_face_table3_kernel(CoefPtrs cp, long long nc, int rows, double* __restrict__ tab) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= rows) return;
+    long long c = f - 3;
+    c = c < 0 ? 0 : (c > nc - 1 ? nc - 1 : c);
+    double* row = tab + (long long)f * kFaceRow3;
+    bool neg = false;
+    for (int r = 0; r < 2; ++r) {
+        const double dl = cp.dL[r + 5 * c], dr = cp.dR[r + 5 * c];
+        neg |= !(dl >= 0.0) || !(dr >= 0.0);
+        row[r] = dl * cp.polyL[c + nc * r];
+        row[2 + r] = dr * cp.polyR[c + nc * r];
+        row[4 + r] = dl;
+        row[6 + r] = dr;
+        row[8 + r] = cp.beta[c + nc * r];
+    }
+    row[10] = row[11] = 0.0;
+    if (neg) row[4] = __longlong_as_double(0x7ff8000000000000LL);
+}
+
 struct March64_3 {
     double vm1, v0, vp1, vp2;   // cells J-1 .. J+2
     double dm1, d0, dp1;        // d[J-1], d[J], d[J+1]
@@ -1383,19 +1432,28 @@ struct March64_3 {
     double e2, mA, mB;
 
     __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3, double c4) {
+        init(a, ParamCoefs3{a}, c0, c1, c2, c3, c4);
+    }
+    // c: the coefficients of face J
+    template <class C>
+    __device__ __forceinline__ void init(const MarchArgs& a, const C& c, double c0, double c1, double c2, double c3,
+                                         double c4) {
         vm1 = c1; v0 = c2; vp1 = c3; vp2 = c4;
         const double dm2 = c1 - c0;
         dm1 = c2 - c1; d0 = c3 - c2; dp1 = c4 - c3;
-        B0 = fma(a.ucf[8], d0 * d0, a.wp.eps);
-        B1 = fma(a.ucf[9], dm1 * dm1, a.wp.eps);
+        B0 = fma(c.b(0), d0 * d0, a.wp.eps);
+        B1 = fma(c.b(1), dm1 * dm1, a.wp.eps);
         const double em = dm1 - dm2, ez = d0 - dm1;
         e2 = dp1 - d0;
         mA = mm64(em, ez);
         mB = mm64(ez, e2);
     }
-    __device__ __forceinline__ void push(const MarchArgs& a, double n) {
+    __device__ __forceinline__ void push(const MarchArgs& a, double n) { push(a, ParamCoefs3{a}, n); }
+    // c: the coefficients of face J+1
+    template <class C>
+    __device__ __forceinline__ void push(const MarchArgs& a, const C& c, double n) {
         const double dn = n - vp2;
-        const double nB0 = fma(a.ucf[8], dp1 * dp1, a.wp.eps), nB1 = fma(a.ucf[9], d0 * d0, a.wp.eps);
+        const double nB0 = fma(c.b(0), dp1 * dp1, a.wp.eps), nB1 = fma(c.b(1), d0 * d0, a.wp.eps);
         const double ne2 = dn - dp1;
         const double nmB = mm64(e2, ne2);
         vm1 = v0; v0 = vp1; vp1 = vp2; vp2 = n;
@@ -1409,10 +1467,14 @@ struct March64_3 {
     }
     template <bool MPF>
     __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R, bool core) const {
+        return face<MPF, ParamCoefs3>(a, ParamCoefs3{a}, L, R, core);
+    }
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool face(const MarchArgs& a, const C& c, double& L, double& R, bool core) const {
         const double P0 = B1 * B1, P1 = B0 * B0;
-        const double SL = fma(a.ucf[4], P0, a.ucf[5] * P1), SR = fma(a.ucf[6], P0, a.ucf[7] * P1);
-        const double EL = fma(P0, a.kL[0] * d0, P1 * (a.kL[1] * dm1));
-        const double ER = fma(P0, a.kR[0] * d0, P1 * (a.kR[1] * dm1));
+        const double SL = fma(c.dL(0), P0, c.dL(1) * P1), SR = fma(c.dR(0), P0, c.dR(1) * P1);
+        const double EL = fma(P0, c.kL(0) * d0, P1 * (c.kL(1) * dm1));
+        const double ER = fma(P0, c.kR(0) * d0, P1 * (c.kR(1) * dm1));
         const double p = SL * SR;
         const bool ok = mid_range_prod(p);
         const double r = rcp1(p);
@@ -1480,6 +1542,21 @@ struct March32_3 {
         return ok;
     }
 };
+
+// The same with face-dependent coefficient arrays (core face clamp(o - 3)).
+template <bool MPF>
+__device__ __noinline__ void march3_redo_faces(const MarchArgs& a, const double* __restrict__ col, long long o,
+                                               double& L, double& R) {
+    Coef<3> c;
+    long long ci = o - 3;
+    ci = ci < 0 ? 0 : (ci > a.nc - 1 ? a.nc - 1 : ci);
+    c.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.nc, ci);
+    const double* p = col + (o + 1) * a.sJ;
+    const double vm2 = __ldg(p), vm1 = __ldg(p + a.sJ), v0 = __ldg(p + 2 * a.sJ), vp1 = __ldg(p + 3 * a.sJ),
+                 vp2 = __ldg(p + 4 * a.sJ);
+    weno3_face(vm1, v0, vp1, c, a.wp.scheme, a.wp.eps, L, R);
+    if (MPF && o >= 3 && o <= a.ns - 4) mp_limit(vm2, vm1, v0, vp1, vp2, L, R);
+}
 
 // The reference sequence for one WENO3 face (cells o+1 .. o+5; MP on the
 // core faces).

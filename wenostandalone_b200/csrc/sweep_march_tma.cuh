@@ -71,9 +71,12 @@ constexpr int kTmaOut = WSB_MTMA_OUTBUF;
 constexpr int kPfStages = WSB_MTMA_PF_STAGES;
 constexpr int kPfOut = WSB_MTMA_PF_OUTBUF;
 // rows f0 .. f0 + 8 of a chunk (WENO5 / WENO7 table rows)
-__host__ __device__ constexpr int pf_row_doubles(int order) { return order == 7 ? kFaceRow7 : kFaceRow; }
+__host__ __device__ constexpr int pf_row_doubles(int order) {
+    return order == 7 ? kFaceRow7 : (order == 3 ? kFaceRow3 : kFaceRow);
+}
 __host__ __device__ constexpr int pf_chunk_bytes(int order) { return (kTmaF + 1) * pf_row_doubles(order) * 8; }
-static_assert(pf_chunk_bytes(5) % 16 == 0 && pf_chunk_bytes(7) % 16 == 0, "bulk copies move 16-byte multiples");
+static_assert(pf_chunk_bytes(3) % 16 == 0 && pf_chunk_bytes(5) % 16 == 0 && pf_chunk_bytes(7) % 16 == 0,
+              "bulk copies move 16-byte multiples");
 static_assert(WSB_MTMA_PF_STAGES <= 4 && WSB_MTMA_PF_STAGES >= 2, "stages of the per-face kernels");
 #ifndef WSB_MTMA_WARPS
 #define WSB_MTMA_WARPS 4        // warps per CTA (each with its own pipeline)
@@ -172,7 +175,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
     constexpr int XW = sizeof(T) == 8 ? 34 : 36;          // KIND 1 tile width
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
-    static_assert(ORDER != 3 || !PF, "WENO3: face-independent coefficients");
+    static_assert(ORDER != 3 || !PF || (sizeof(T) == 8 && !TENOW), "WENO3 per-face table: FP64, JS");
     static_assert(ORDER != 7 || !PF || sizeof(T) == 8, "WENO7 per-face table: FP64");
     constexpr int RW = pf_row_doubles(ORDER), RB = pf_chunk_bytes(ORDER);  // per-face table rows
     static_assert(!TENOW || !PF || ORDER != 3, "TENO with a per-face table: WENO5 / WENO7");
@@ -180,7 +183,6 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
         ORDER == 7, std::conditional_t<sizeof(T) == 8, March64_7, March32_7>,
         std::conditional_t<ORDER == 3, std::conditional_t<sizeof(T) == 8, March64_3, March32_3>,
                            typename MarchEngine<T>::type>>;
-    static_assert(ORDER != 3 || (!PF && !TENOW), "WENO3: JS, face-independent coefficients");
     constexpr int PUSH0 = ORDER == 7 ? 7 : 6;             // tile position of the cell pushed after face f0
     extern __shared__ __align__(1024) unsigned char smem_mt[];
     unsigned char* base = smem_mt + ((1024u - (smem_u32(smem_mt) & 1023u)) & 1023u);
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
                     else ok = w.template face<MPF>(a, L, R);
                 }
-            } else if constexpr (PF) {
+            } else if constexpr (PF && ORDER == 5) {
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
                 if constexpr (TENOW) ok = w.template face_teno<MPF>(a, FaceRow(row(3)), L, R);
@@ -354,7 +356,9 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
             else if constexpr (PF) w.push(a, BetaRow(row(4)), cell(k0, 5));
             else w.push(a, cell(k0, 5));
         } else {
-            if constexpr (ORDER == 7 && PF)
+            if constexpr (ORDER == 3 && PF)
+                w.init(a, Row3{row(f_start)}, cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
+            else if constexpr (ORDER == 7 && PF)
                 w.init(a, Row7{row(f_start - 3)}, Row7{row(f_start - 2)}, Row7{row(f_start - 1)}, Row7{row(f_start)},
                        cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5), cell(k0, 6));
             else if constexpr (ORDER == 7)
@@ -407,12 +411,14 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 }
                 T L, R;
                 bool ok;
-                if constexpr (PF && ORDER == 7 && TENOW) ok = w.template face_teno<MPF>(a, Row7{srow(kc, i)}, L, R);
+                if constexpr (ORDER == 3 && PF)
+                    ok = w.template face<MPF>(a, Row3{srow(kc, i)}, L, R, f0 + i >= 3 && f0 + i <= o_last - 4);
+                else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, f0 + i >= 3 && f0 + i <= o_last - 4);
+                else if constexpr (PF && ORDER == 7 && TENOW) ok = w.template face_teno<MPF>(a, Row7{srow(kc, i)}, L, R);
                 else if constexpr (PF && ORDER == 7) ok = w.template face<MPF>(a, Row7{srow(kc, i)}, L, R);
                 else if constexpr (PF && TENOW) ok = w.template face_teno<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
-                else if constexpr (ORDER == 3) ok = w.template face<MPF>(a, L, R, f0 + i >= 3 && f0 + i <= o_last - 4);
                 else ok = w.template face<MPF>(a, L, R);
                 if (!ok) bad |= 1u << i;
                 Lg[i % G] = L;
@@ -435,6 +441,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 if constexpr (KIND == 0) n = cg[pq % G];
                 else n = cell(kq, pq);
                 if constexpr (PF && ORDER == 7) w.push(a, Row7{srow(kc, i + 1)}, n);
+                else if constexpr (PF && ORDER == 3) w.push(a, Row3{srow(kc, i + 1)}, n);
                 else if constexpr (PF) w.push(a, BetaRow(srow(kc, i + 1)), n);
                 else w.push(a, n);
             }
@@ -448,6 +455,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     T L, R;
                     if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(a, col, f0 + i, L, R);
                     else if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(a, col, f0 + i, L, R);
                     else if constexpr (ORDER == 3) march3_redo<MPF, T>(a, col, f0 + i, L, R);
                     else march_redo<MPF, PF>(a, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
@@ -599,8 +607,7 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     const int out_bytes = (pf ? kPfOut : kTmaOut) * 2 * 32 * kTmaF * ES;
     t.ring_off = out_bytes;
     t.rows_off = out_bytes + nst * t.stage_bytes;
-    t.warp_bytes = ((t.rows_off + (pf ? nst * (order == 7 ? pf_chunk_bytes(7) : pf_chunk_bytes(5)) : 0) + 1023) /
-                    1024) * 1024;
+    t.warp_bytes = ((t.rows_off + (pf ? nst * pf_chunk_bytes(order) : 0) + 1023) / 1024) * 1024;
     const size_t smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * nst * 8;
     using KFn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, MarchArgs, MarchTmaArgs);
     static const KFn table[2][2][2] = {
@@ -642,9 +649,19 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
               {sweep_march_tma_kernel<true, 1, T, 0, false, 7, true>,
                sweep_march_tma_kernel<true, 1, T, 1, false, 7, true>}}}};
         kfn = tablet[order == 7 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+    } else if (order == 3 && a.ftab) {
+        // WENO3-JS with the per-face table: FP64 with TMA input tiles
+        if constexpr (sizeof(T) == 8) {
+            if (ldr) return 1003;
+            static const KFn ptable3[2][2] = {
+                {sweep_march_tma_kernel<false, 0, T, 0, true, 3>, sweep_march_tma_kernel<false, 1, T, 0, true, 3>},
+                {sweep_march_tma_kernel<true, 0, T, 0, true, 3>, sweep_march_tma_kernel<true, 1, T, 0, true, 3>}};
+            kfn = ptable3[mp ? 1 : 0][kind1 ? 1 : 0];
+        } else {
+            return 1003;
+        }
     } else if (order == 3) {
         // WENO3: JS, face-independent coefficients
-        if (a.ftab) return 1003;
         static const KFn table3[2][2][2] = {
             {{sweep_march_tma_kernel<false, 0, T, 0, false, 3>, sweep_march_tma_kernel<false, 0, T, 1, false, 3>},
              {sweep_march_tma_kernel<false, 1, T, 0, false, 3>, sweep_march_tma_kernel<false, 1, T, 1, false, 3>}},

@@ -295,8 +295,8 @@ bool march_weights_ok(const double* ucf, int order = 5) {
 }
 
 // FP64 marching sweep with face-dependent coefficient arrays (WENO5 and
-// WENO7, JS or TENO weights): the per-face table (one row per face, 224 bytes
-// for WENO5, 448 for WENO7; ns + 16 rows: the kernel stages rows f0 .. f0 + 8
+// WENO7 with JS or TENO weights, WENO3-JS): the per-face table (one row per
+// face, 224 bytes for WENO5, 448 for WENO7, 96 for WENO3; ns + 16 rows: the kernel stages rows f0 .. f0 + 8
 // with every input tile, and its last tile starts below ns + 5) is built on
 // the stream, used by the TMA marching kernel and freed stream-ordered.
 // Returns WENO_SB_ERR_UNSUPPORTED when the layout does not suit the kernel.
@@ -307,8 +307,9 @@ int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool f
     if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
     const int rows = (int)g.ns + 16;
     double* tab = nullptr;
-    WSB_CUDA(cudaMallocAsync((void**)&tab, sizeof(double) * (order == 7 ? kFaceRow7 : kFaceRow) * (size_t)rows, st));
+    WSB_CUDA(cudaMallocAsync((void**)&tab, sizeof(double) * pf_row_doubles(order) * (size_t)rows, st));
     if (order == 7) march_face_table7_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
+    else if (order == 3) march_face_table3_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
     else march_face_table_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
     MarchArgs a0 = make_march_args(g, in, vL, vR, wp, nullptr);
     a0.ftab = tab;
@@ -366,7 +367,8 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     }
     if constexpr (sizeof(T) == 8) {
         if ((choice == 0 || choice == 3) && !ucf &&
-            (order == 5 || order == 7) && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) {
+            (((order == 5 || order == 7) && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) ||
+             (order == 3 && gr->scheme == WENO_SB_JS))) {
             int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme == WENO_SB_TENO,
                                         order);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc;
