@@ -510,7 +510,7 @@ def test_fp32_bulk_smooth_error(wsb, oracle_mod, order, d, entry):
     """FP32-bulk (FP32 fields and face states, FP32 stencil sums, FP64 beta and
     normalisation) on smooth data vs the FP64 oracle on the FP64 field:
     max-norm relative error <= 1e-6 per array (per-face coefficient arrays,
-    and the face-independent entry, which takes the marching kernel for WENO5)."""
+    and the face-independent entry, which takes the marching kernels)."""
     for mx, rms in _fp32_case(wsb, oracle_mod, order, d, mp=False, entry=entry):
         assert mx <= 1e-6 and rms <= 1e-7, (mx, rms)
 
