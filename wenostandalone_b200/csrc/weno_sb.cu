@@ -299,7 +299,8 @@ bool march_weights_ok(const double* ucf, int order = 5) {
 // face, 224 bytes for WENO5, 448 for WENO7, 96 for WENO3; ns + 16 rows: the kernel stages rows f0 .. f0 + 8
 // with every input tile, and its last tile starts below ns + 5) is built on
 // the stream, used by the TMA marching kernel and freed stream-ordered.
-// Returns WENO_SB_ERR_UNSUPPORTED when the layout does not suit the kernel.
+// Returns WENO_SB_ERR_UNSUPPORTED when the layout does not suit the kernel
+// or the table cannot be allocated.
 int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const double* in,
                        double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st,
                        bool teno = false, int order = 5) {
@@ -307,7 +308,12 @@ int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool f
     if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
     const int rows = (int)g.ns + 16;
     double* tab = nullptr;
-    WSB_CUDA(cudaMallocAsync((void**)&tab, sizeof(double) * pf_row_doubles(order) * (size_t)rows, st));
+    // no stream-ordered allocation available (or no memory): the caller
+    // falls back to the one-thread-per-face kernels, which need no table
+    if (cudaMallocAsync((void**)&tab, sizeof(double) * pf_row_doubles(order) * (size_t)rows, st) != cudaSuccess) {
+        cudaGetLastError();
+        return WENO_SB_ERR_UNSUPPORTED;
+    }
     if (order == 7) march_face_table7_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
     else if (order == 3) march_face_table3_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
     else march_face_table_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
