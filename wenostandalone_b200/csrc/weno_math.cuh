@@ -103,7 +103,6 @@ struct Coef<7> {
     }
 };
 
-__device__ __forceinline__ bool normal_pos(double s) { return s > 1e-300 && s < 1e300; }
 
 // True when s is positive with 2^-498 <= s < 2^498 (an integer test on the
 // exponent field, so it costs no FP64 issue slot).  Two such values have a
