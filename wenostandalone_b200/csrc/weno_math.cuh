@@ -103,7 +103,6 @@ struct Coef<7> {
     }
 };
 
-
 // True when s is positive with 2^-498 <= s < 2^498 (an integer test on the
 // exponent field, so it costs no FP64 issue slot).  Two such values have a
 // product that is a normal number.
