@@ -332,9 +332,11 @@ def run_ours(args):
         e2e = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev)
         e2e_full = measure_e2e(g, vf_host, coefs, max(2, min(K, 5)), dev, full_download=True)
 
-    # the other workloads of the path (adjoint, batched blocks, mixed precision)
+    # the other workloads of the path (adjoint, batched blocks, mixed precision):
+    # single-GPU measurements, taken in one-GPU runs only (with several ranks
+    # the others would wait for rank 0 at the closing barrier)
     adjoint = batched = mixed = families = None
-    if not args.no_extras and rank == 0 and not fp32_main:
+    if not args.no_extras and rank == 0 and ws == 1 and not fp32_main:
         Kx = max(3, min(K, 10))
         adjoint = measure_adjoint(dev, Kx)
         torch.cuda.empty_cache()
