@@ -801,6 +801,18 @@ def measure_mixed_precision(dev, K):
     return res
 
 
+def run_only(args):
+    """One side measurement (the adjoint or the batched blocks) alone on
+    cuda:0 with K = --steps timed steps: its result as one JSON line."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    fn = {"adjoint": measure_adjoint, "batched": measure_batched}[args.only]
+    res = fn(dev, max(1, args.steps))
+    print(json.dumps({"measurement": args.only, **res}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -819,7 +831,12 @@ def main():
     ap.add_argument("--coefficients", choices=["uniform", "arrays"], default="uniform",
                     help="arrays: the main step passes the coefficients as per-face device arrays "
                          "(weno_sb_weno_dev, the drop-in form) instead of one face-independent set")
+    ap.add_argument("--only", choices=["adjoint", "batched"], default=None,
+                    help="run only this side measurement on cuda:0 and print its JSON line "
+                         "(a short command whose kernels can be profiled alone)")
     args = ap.parse_args()
+    if args.only:
+        return run_only(args)
     global M, ORDER, SCHEME
     M = args.m
     ORDER = args.order
