@@ -138,6 +138,12 @@ int weno_sb_initialize_weno(int handle, int dir);
 int weno_sb_weno(int handle, int dir, int order, unsigned flags);
 /* s_preserve_monotonicity (f90:1544-1615) on vL/vR_dir, in place. */
 int weno_sb_preserve_monotonicity(int handle, int dir);
+/* Adjoint of weno_sb_weno(handle, dir, order, flags) for order 3/5/7 -- no
+ * counterpart in the reference.  Reads the handle's v_rs_ws_dir (or v_vf
+ * with WENO_SB_F_FOLDED) and coefficients; gL, gR (face layout) and gv
+ * (layout of the input) are device pointers of the caller.  See
+ * weno_sb_vjp_dev for the flags and the meaning of gv.  FP64 handles. */
+int weno_sb_vjp(int handle, int dir, int order, unsigned flags, const double *gL, const double *gR, double *gv);
 /* f_checksum (f90:1617-1620): sum(|a|) of one array, computed on the GPU. */
 int weno_sb_checksum(int handle, int which, double *result);
 /* Wait for all work queued on the handle's stream; also reports a device
@@ -212,8 +218,9 @@ int weno_sb_checksum_dev(int dtype, const void *arr, int64_t n, void *scratch,
  * scratch is a static device array of 16 x 592 doubles (74 KB) in the
  * library, held on every GPU that loads it until exit: count > 16 is
  * rejected with WENO_SB_ERR_ARG.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls share the one array, so calls that overlap
+ * array's device address (cudaGetSymbolAddress), and so does the first call
+ * after the device's context changes (cudaDeviceReset); make those calls
+ * before any stream capture.  All calls share the one array, so calls that overlap
  * on the GPU (different streams, or host threads) race; each call rewrites
  * every partial it reads, so nothing needs clearing between calls. */
 int weno_sb_checksum_noalloc(int dtype, const void *const *arrays, const int64_t *n, int count,

@@ -54,6 +54,8 @@ def lib() -> ctypes.CDLL:
         L.wo_reconstruct.argtypes = [i, i, i, i, i, i, ctypes.c_double, ctypes.c_double,
                                      dp, dp, dp, dp, dp, dp, dp, dp]
         L.wo_reconstruct.restype = i
+        L.wo_teno_margin.argtypes = [i, i, i, i, i, ctypes.c_double, ctypes.c_double, dp, dp, dp]
+        L.wo_teno_margin.restype = i
         L.wo_preserve_monotonicity.argtypes = [i, i, i, i, dp, dp, dp]
         L.wo_preserve_monotonicity.restype = i
         L.wo_checksum.argtypes = [ctypes.c_longlong, dp]
@@ -148,6 +150,19 @@ def reconstruct(rs, coefs, order, scheme=JS, eps=1e-16, teno_ct=1e-5, vL=None, v
                               _p(rs), _p(pL), _p(pR), _p(dL), _p(dR), _p(bc), _p(vL), _p(vR))
     assert rc == 0, rc
     return vL, vR
+
+
+def teno_margin(rs, coefs, order, eps=1e-16, teno_ct=1e-5):
+    """Per face of the sweep output layout: min over the TENO cutoff tests of
+    |omega_q - CT| / CT (f90:578-590 for WENO5, f90:1491-1506 for WENO7),
+    +inf outside the core.  A cutoff decision can only differ between two
+    correct implementations where this is at rounding level."""
+    ns6, c1, c2, nv = rs.shape
+    out = np.empty((ns6 - 6, c1, c2, nv), order="F")
+    rc = lib().wo_teno_margin(ns6 - 6, c1, c2, nv, order, float(eps), float(teno_ct), _p(rs),
+                              _p(np.asfortranarray(coefs[4])), _p(out))
+    assert rc == 0, rc
+    return out
 
 
 def preserve_monotonicity(rs, vL, vR):

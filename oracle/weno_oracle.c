@@ -452,6 +452,81 @@ int wo_reconstruct(int ns_, int c1_, int c2_, int nv_, int order, int scheme,
 }
 
 /* ------------------------------------------------------------------ */
+/* TENO cutoff margin (checker support, no reference counterpart): per   */
+/* core face, min over the cutoff tests of |omega_q - CT| / CT, with     */
+/* beta, alpha and omega formed exactly as weno5_point (f90:545-550,     */
+/* 578-590) and weno7_point (f90:1462-1473, 1491-1506) form them.  A     */
+/* GPU result may differ from the oracle's only where this margin is at  */
+/* rounding level (the cutoff decision can go either way there).         */
+/* Faces outside the core get +inf.                                      */
+/* ------------------------------------------------------------------ */
+int wo_teno_margin(int ns_, int c1_, int c2_, int nv_, int order, double eps, double teno_ct,
+                   const double *v_rs_ws, const double *bc, double *margin) {
+    const long long ns = ns_, c1 = c1_, c2 = c2_, nv = nv_;
+    const long long nc = ns - 6;
+    if (nc < 1 || c1 < 1 || c2 < 1 || nv < 1) return -1;
+    if (order != 5 && order != 7) return -2;
+    const long long rows = c1 * c2 * nv;
+#pragma omp parallel for schedule(static) num_threads(NTHR)
+    for (long long r = 0; r < rows; ++r) {
+        const double *in = v_rs_ws + (ns + 6) * r;
+        double *mg = margin + ns * r;
+        for (long long o = 0; o < ns; ++o) mg[o] = INFINITY;
+        for (long long o = 3; o <= ns - 4; ++o) {
+            const double *v = in + o + 3;
+            const long long c = o - 3;
+            double best = INFINITY;
+            if (order == 5) {
+                const double dvd_p1 = v[2] - v[1], dvd_0 = v[1] - v[0];
+                const double dvd_m1 = v[0] - v[-1], dvd_m2 = v[-1] - v[-2];
+                const double b0 = BC(bc, c, 0, 0) * dvd_p1 * dvd_p1 + BC(bc, c, 0, 1) * dvd_p1 * dvd_0
+                                  + BC(bc, c, 0, 2) * dvd_0 * dvd_0 + eps;
+                const double b1 = BC(bc, c, 1, 0) * dvd_0 * dvd_0 + BC(bc, c, 1, 1) * dvd_0 * dvd_m1
+                                  + BC(bc, c, 1, 2) * dvd_m1 * dvd_m1 + eps;
+                const double b2 = BC(bc, c, 2, 0) * dvd_m1 * dvd_m1 + BC(bc, c, 2, 1) * dvd_m1 * dvd_m2
+                                  + BC(bc, c, 2, 2) * dvd_m2 * dvd_m2 + eps;
+                const double tau = fabs(b2 - b0);
+                const double a[3] = {pow(1.0 + tau / b0, 6.0), pow(1.0 + tau / b1, 6.0),
+                                     pow(1.0 + tau / b2, 6.0)};
+                const double s = a[0] + a[1] + a[2];
+                for (int q = 0; q < 3; ++q) {
+                    const double m = fabs(a[q] / s - teno_ct) / teno_ct;
+                    if (!(m >= best)) best = m;
+                }
+            } else {
+                double D6[6];
+                double *D = D6 + 3;
+                D[2] = v[3] - v[2]; D[1] = v[2] - v[1]; D[0] = v[1] - v[0];
+                D[-1] = v[0] - v[-1]; D[-2] = v[-1] - v[-2]; D[-3] = v[-2] - v[-3];
+#define BETA7M(r, a, b, e)                                                                         \
+    (BC(bc, c, r, 0) * a * a + BC(bc, c, r, 1) * a * b + BC(bc, c, r, 2) * a * e                 \
+     + BC(bc, c, r, 3) * b * b + BC(bc, c, r, 4) * b * e + BC(bc, c, r, 5) * e * e + eps)
+                double beta[5];
+                beta[3] = BETA7M(0, D[2], D[1], D[0]);
+                beta[2] = BETA7M(1, D[1], D[0], D[-1]);
+                beta[1] = BETA7M(2, D[0], D[-1], D[-2]);
+                beta[0] = BETA7M(3, D[-1], D[-2], D[-3]);
+                beta[4] = eps;
+#undef BETA7M
+                const double tau = fabs(beta[4] - beta[3]);
+                double alpha[5], s = 0.0;
+                for (int q = 0; q <= 4; ++q) {
+                    const double a3 = pow(1.0 + tau / beta[q], 3.0);
+                    alpha[q] = a3 * a3;
+                }
+                s = alpha[0] + alpha[1] + alpha[2] + alpha[3] + alpha[4];
+                for (int q = 0; q <= 3; ++q) {
+                    const double m = fabs(alpha[q] / s - teno_ct) / teno_ct;
+                    if (!(m >= best)) best = m;
+                }
+            }
+            mg[o] = best;
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* f90:1544-1615  s_preserve_monotonicity (core faces, in place)        */
 /* ------------------------------------------------------------------ */
 static inline double fsign(double a, double b) { return copysign(fabs(a), b); }

@@ -37,6 +37,8 @@ int wo_reconstruct(int ns, int c1, int c2, int nv, int order, int scheme,
                    double eps, double teno_ct, const double *v_rs_ws,
                    const double *polyL, const double *polyR, const double *dL,
                    const double *dR, const double *beta, double *vL, double *vR);
+int wo_teno_margin(int ns, int c1, int c2, int nv, int order, double eps, double teno_ct,
+                   const double *v_rs_ws, const double *beta, double *margin);
 int wo_preserve_monotonicity(int ns, int c1, int c2, int nv,
                              const double *v_rs_ws, double *vL, double *vR);
 double wo_checksum(long long n, const double *a);

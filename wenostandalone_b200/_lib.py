@@ -50,7 +50,7 @@ EXPORTED = [
     "weno_sb_version", "weno_sb_last_error_string", "weno_sb_extents",
     "weno_sb_init", "weno_sb_finalize", "weno_sb_upload", "weno_sb_download",
     "weno_sb_array_info", "weno_sb_initialize_weno", "weno_sb_weno",
-    "weno_sb_preserve_monotonicity", "weno_sb_checksum", "weno_sb_sync",
+    "weno_sb_preserve_monotonicity", "weno_sb_vjp", "weno_sb_checksum", "weno_sb_sync",
     "weno_sb_stream", "weno_sb_reshape_dev", "weno_sb_order1_dev",
     "weno_sb_weno_dev", "weno_sb_weno_uniform_dev", "weno_sb_vjp_dev", "weno_sb_preserve_monotonicity_dev",
     "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev", "weno_sb_check_device",
@@ -123,6 +123,7 @@ def lib() -> ctypes.CDLL:
         "weno_sb_initialize_weno": ([i32, i32], i32),
         "weno_sb_weno": ([i32, i32, i32, u32], i32),
         "weno_sb_preserve_monotonicity": ([i32, i32], i32),
+        "weno_sb_vjp": ([i32, i32, i32, u32, vp, vp, vp], i32),
         "weno_sb_checksum": ([i32, i32, dp], i32),
         "weno_sb_sync": ([i32], i32),
         "weno_sb_stream": ([i32, ctypes.POINTER(ctypes.c_void_p)], i32),

@@ -308,10 +308,20 @@ int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool f
     if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
     const int rows = (int)g.ns + 16;
     double* tab = nullptr;
+    // an error left by an earlier call is reported, not cleared by the
+    // allocation's own error handling below
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) return cuda_err(cudaGetLastError(), "error pending before the per-face table");
     // no stream-ordered allocation available (or no memory): the caller
-    // falls back to the one-thread-per-face kernels, which need no table
-    if (cudaMallocAsync((void**)&tab, sizeof(double) * pf_row_doubles(order) * (size_t)rows, st) != cudaSuccess) {
+    // falls back to the one-thread-per-face kernels, which need no table;
+    // during a stream capture the failed allocation has invalidated the
+    // capture, so its error is returned instead
+    const cudaError_t ae = cudaMallocAsync((void**)&tab, sizeof(double) * pf_row_doubles(order) * (size_t)rows, st);
+    if (ae != cudaSuccess) {
         cudaGetLastError();
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+            return cuda_err(ae, "per-face table allocation during stream capture");
         return WENO_SB_ERR_UNSUPPORTED;
     }
     if (order == 7) march_face_table7_kernel<<<(rows + 127) / 128, 128, 0, st>>>(cp, g.nc, rows, tab);
@@ -959,6 +969,24 @@ int weno_sb_weno(int handle, int dir, int order, unsigned flags) {
                             H->arr[WENO_SB_A_VR(dir)], H->stream);
 }
 
+int weno_sb_vjp(int handle, int dir, int order, unsigned flags, const double* gL, const double* gR, double* gv) {
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    int rc = check_dir(dir);
+    if (rc) return rc;
+    if (H->precision != WENO_SB_FP64) return set_err(WENO_SB_ERR_UNSUPPORTED, "the adjoint is FP64 (FP32-bulk handle)");
+    const void* in = (flags & WENO_SB_F_FOLDED) ? H->arr[WENO_SB_A_V_VF] : H->arr[WENO_SB_A_RS(dir)];
+    bool uni = true;
+    for (int k = 0; k < 5; ++k) uni = uni && H->coef_uniform[dir][k];
+    if (uni && getenv("WENO_SB_PER_FACE") == nullptr)
+        return weno_sb_vjp_dev(&H->grid, dir, order, flags, (const double*)in, nullptr, &H->face0[dir], gL, gR, gv,
+                               H->stream);
+    weno_sb_coefs cf{(const double*)H->arr[WENO_SB_A_POLYL(dir)], (const double*)H->arr[WENO_SB_A_POLYR(dir)],
+                     (const double*)H->arr[WENO_SB_A_DL(dir)], (const double*)H->arr[WENO_SB_A_DR(dir)],
+                     (const double*)H->arr[WENO_SB_A_BETA(dir)]};
+    return weno_sb_vjp_dev(&H->grid, dir, order, flags, (const double*)in, &cf, nullptr, gL, gR, gv, H->stream);
+}
+
 int weno_sb_preserve_monotonicity(int handle, int dir) {
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
@@ -985,12 +1013,42 @@ int weno_sb_checksum(int handle, int which, double* result) {
 // up to kNoAllocMaxArrays arrays (74 KB), resident on every GPU that loads
 // the library until the process exits.  Host code may not use the symbol
 // as a device address: the address comes from cudaGetSymbolAddress, looked
-// up once per device on that device's first call.
+// up on a device's first call and again whenever the device's current
+// context is a different one (after cudaDeviceReset the module loads anew,
+// possibly at another address).  Contexts are told apart by cuCtxGetId,
+// which never repeats within a process.
 static constexpr int kNoAllocMaxArrays = 16;
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxArrays * kSumBlocks];
 static constexpr int kNoAllocMaxDevices = 64;
 static std::mutex g_noalloc_mu;
 static double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+static unsigned long long g_noalloc_ctx[kNoAllocMaxDevices] = {};
+
+// Id of the calling thread's current context, 0 when there is none or the
+// driver entry points are unavailable.
+static unsigned long long current_context_id() {
+    typedef CUresult (*GetCurrentFn)(CUcontext*);
+    typedef CUresult (*GetIdFn)(CUcontext, unsigned long long*);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrentFn)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetIdFn)p;
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 int weno_sb_checksum_noalloc(int dtype, const void* const* arrays, const int64_t* n, int count,
                              double* d_results, void* stream) {
@@ -1013,11 +1071,15 @@ int weno_sb_checksum_noalloc(int dtype, const void* const* arrays, const int64_t
     double* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        // a thread with no current context yet (the runtime creates it on
+        // first use) gets one from the lookup below, and its id after it
+        const unsigned long long ctx = current_context_id();
+        if (!g_noalloc_addr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
             if (e != cudaSuccess) return cuda_err(e, "cudaGetSymbolAddress(g_noalloc_partials)");
             g_noalloc_addr[dev] = (double*)p;
+            g_noalloc_ctx[dev] = current_context_id();
         }
         scratch = g_noalloc_addr[dev];
     }
