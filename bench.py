@@ -152,15 +152,41 @@ def dist_init():
     return rank, ws, local, dist
 
 
-def cpu_reference_run(steps, warmup, sample_nv=2, quiet=False):
-    """Time the oracle (CPU restatement of the reference path) on all host
-    threads: x/y/z WENO5-JS + MP from the reshaped fields, on a sample of
-    `sample_nv` of the 8 variables (same grid, same per-variable work)."""
+def cpu_info():
+    """Host CPU model, logical CPUs available to this process and the OpenMP
+    binding in force (stated beside every CPU number)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        avail = len(os.sched_getaffinity(0))
+    except AttributeError:
+        avail = os.cpu_count() or 1
+    return {"model": model, "nproc": avail, "OMP_PROC_BIND": os.environ.get("OMP_PROC_BIND", ""),
+            "OMP_PLACES": os.environ.get("OMP_PLACES", "")}
+
+
+def cpu_reference_run(steps, warmup, sample_nv=NV, quiet=False):
+    """Time the oracle (CPU restatement of the reference path, built -O3 like
+    the reference's CPU recipe, f90:33-36) on all host threads: x/y/z
+    WENO5-JS + MP from the reshaped fields of `sample_nv` of the 8 variables
+    (all 8 by default: the bench's own workload), `warmup` untimed and
+    `steps` timed steps (the reference's protocol is warmup 5, bench >= 10)."""
+    # thread binding for the oracle's OpenMP runtime (read when it starts)
+    os.environ.setdefault("OMP_PROC_BIND", "spread")
+    os.environ.setdefault("OMP_PLACES", "threads")
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from wenostandalone_b200 import fields
     oracle.build()
-    threads = os.cpu_count() or 1
+    info = cpu_info()
+    threads = info["nproc"]
     oracle.set_threads(threads)
     vf = fields.smooth_jump_field(M, M, M, sample_nv, BUFF, seed=0)
     ins = []
@@ -169,6 +195,7 @@ def cpu_reference_run(steps, warmup, sample_nv=2, quiet=False):
         coefs = fields.uniform_weno_coefficients(5, rs.shape[0] - 12)
         L, R = oracle.order1_copy(vf, M, M, M, BUFF, d)
         ins.append((rs, coefs, L, R))
+    del vf
 
     def step():
         for rs, coefs, L, R in ins:
@@ -177,25 +204,32 @@ def cpu_reference_run(steps, warmup, sample_nv=2, quiet=False):
 
     for _ in range(warmup):
         step()
-    t0 = time.perf_counter()
-    for _ in range(steps):
+    times = []
+    for _ in range(max(steps, 1)):
+        t0 = time.perf_counter()
         step()
-    dt = (time.perf_counter() - t0) / max(steps, 1)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
     fs = 3 * face_states_per_dir(nv=sample_nv)
-    return {"value": fs / dt, "sec_per_step": dt, "cores": threads, "face_states": fs,
+    return {"value": fs / dt, "sec_per_step": dt, "median_sec_per_step": statistics.median(times),
+            "cores": threads, "face_states": fs, "cpu": info, "warmup": warmup, "steps": max(steps, 1),
             "sample": f"x/y/z WENO5-JS + MP on 200^3 cells x {sample_nv} of {NV} variables "
-                      f"({fs/1e6:.1f} M face states per step), from pre-reshaped fields"}
+                      f"({fs/1e6:.1f} M face states per step) from pre-reshaped fields, warmup {warmup}, "
+                      f"{max(steps, 1)} timed steps, {threads} OpenMP threads on {info['model']} "
+                      f"(OMP_PROC_BIND={info['OMP_PROC_BIND']}, OMP_PLACES={info['OMP_PLACES']}); "
+                      f"oracle built -O3 -ffp-contract=off"}
 
 
 def run_reference(args):
     rank, ws, _, dist = dist_init()
     if rank != 0:
         return 0
-    r = cpu_reference_run(args.steps, args.warmup)
+    r = cpu_reference_run(max(args.steps, 10), max(args.warmup, 5))
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "face-states/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "steps_run": r["steps"], "warmup_run": r["warmup"], "cpu": r["cpu"],
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "WENO5-JS + MP, x/y/z sweeps, 200^3 cells, FP64", "m=n=p": M,
                    "v_size": NV, "buff_size": BUFF},
@@ -349,7 +383,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu and not fp32_main:
-        cpu = cpu_reference_run(steps=1, warmup=0, sample_nv=1)
+        cpu = cpu_reference_run(steps=10, warmup=5)
 
     if rank == 0:
         line = {
@@ -402,7 +436,7 @@ def run_ours(args):
             line["families_200cubed"] = families
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "face-states/s", "cores": cpu["cores"],
-                                    "kind": "port", "sample": cpu["sample"]}
+                                    "kind": "port", "sample": cpu["sample"], "cpu": cpu["cpu"]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

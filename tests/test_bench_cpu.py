@@ -30,7 +30,9 @@ def _run(*args, timeout=600):
 
 
 def test_reference_arm_line():
-    r = _run("--impl", "reference", "--steps", "1", "--warmup", "0")
+    # a 64^3 block keeps the CPU suite short; the arm runs at least warmup 5
+    # and 10 timed steps whatever is asked
+    r = _run("--impl", "reference", "--steps", "1", "--warmup", "0", "--m", "63")
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
     assert line["impl"] == "reference"
@@ -40,6 +42,9 @@ def test_reference_arm_line():
     assert line["value"] > 0 and line["unit"] == "face-states/s" and line["higher_is_better"] is True
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["steps_run"] >= 10 and line["warmup_run"] >= 5
+    assert line["cpu"]["nproc"] >= 1 and line["cpu"]["model"]
+    assert "8 of 8 variables" in line["cpu_baseline"]["sample"]
 
 
 def test_weno3_teno_refused():
