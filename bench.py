@@ -263,7 +263,18 @@ def run_ours(args):
     v = torch.from_numpy(vf_host.ravel(order="F")).to(dev)
     coefs = [tuple(torch.from_numpy(c.ravel(order="F")).to(dev)
                    for c in fields.uniform_weno_coefficients(ORDER, g.nc(d))) for d in range(3)]
-    cstructs = [api.coefs_struct(c) for c in coefs]
+    # per-face coefficient arrays (weno_sb_weno_dev): those of a grid
+    # stretched along every axis (tanh refinement, cells up to 4x narrower,
+    # weno_sb_coefficients), or with --coefficients arrays the uniform-grid
+    # values repeated on every face
+    if args.coefficients == "arrays":
+        pf_coefs = coefs
+    else:
+        pf_coefs = [tuple(torch.from_numpy(np.asarray(c).ravel(order="F")).to(dev) for c in
+                          api.weno_coefficients(ORDER, api.stretched_boundaries(M + 1, BUFF, ratio=4.0,
+                                                                               centre=0.3 + 0.2 * d)))
+                    for d in range(3)]
+    cstructs = [api.coefs_struct(c) for c in pf_coefs]
     # the coefficients are face-independent (uniform grid): the sweeps take
     # them from the kernel-parameter bank through weno_sb_weno_uniform_dev
     faces = [api.face_coefs(fields.uniform_weno_coefficients(ORDER, g.nc(d))) for d in range(3)]
@@ -274,7 +285,7 @@ def run_ours(args):
     sp = int(stream.cuda_stream)
     flags = wsb.F_MP | wsb.F_FOLDED
     fp32_main = args.precision == "fp32"
-    pf_main = args.coefficients == "arrays" and not fp32_main
+    pf_main = args.coefficients in ("arrays", "stretched") and not fp32_main
     if fp32_main:
         # FP32-bulk as the timed step: FP32 v_rs_ws per direction (reshaped
         # once, before timing) and FP32 face states
@@ -350,7 +361,9 @@ def run_ours(args):
         torch.cuda.synchronize()
         pf_ms = e0.elapsed_time(e1) / K
         per_face = {"ms_per_step": pf_ms, "value": 3 * face_states_per_dir() / (pf_ms * 1e-3),
-                    "entry": "weno_sb_weno_dev (coefficient arrays read per face)"}
+                    "entry": "weno_sb_weno_dev (coefficient arrays read per face)",
+                    "coefficients": "WENO5-JS of a tanh-stretched grid on every axis (weno_sb_coefficients, "
+                                    "cells up to 4x narrower)"}
 
     # FP32-bulk variant (same sweeps, FP32 v_rs_ws field and face states)
     fp32 = None
@@ -397,7 +410,10 @@ def run_ours(args):
                                     "(reshape folded)") + f", {M + 1}^3 cells x 8 vars, buff_size 6",
                        "m=n=p": M, "v_size": NV, "buff_size": BUFF,
                        "coefficients": ("uniform-grid WENO5-JS values as per-face device arrays (weno_sb_weno_dev)"
-                                        if pf_main else "uniform-grid WENO5-JS"),
+                                        if args.coefficients == "arrays" else
+                                        "WENO5-JS of a tanh-stretched grid as per-face device arrays "
+                                        "(weno_sb_coefficients, weno_sb_weno_dev)" if pf_main else
+                                        "uniform-grid WENO5-JS"),
                        "field": "seeded smooth-plus-jump", "l2": "inputs (663 MB) and outputs (3.7 GB) exceed "
                                                                   "the 126 MB L2; no flush",
                        "parallelism": f"{ws} independent blocks (weak scaling, no collective)"},
@@ -862,9 +878,10 @@ def main():
                     help="reconstruction order of the main step (5 is the headline metric; others skip the extras)")
     ap.add_argument("--scheme", choices=["js", "teno"], default="js",
                     help="nonlinear weights of the main step (teno: teno_CT 1e-5; WENO5 / WENO7 only)")
-    ap.add_argument("--coefficients", choices=["uniform", "arrays"], default="uniform",
-                    help="arrays: the main step passes the coefficients as per-face device arrays "
-                         "(weno_sb_weno_dev, the drop-in form) instead of one face-independent set")
+    ap.add_argument("--coefficients", choices=["uniform", "arrays", "stretched"], default="uniform",
+                    help="arrays: the main step passes the uniform-grid coefficients as per-face device "
+                         "arrays (weno_sb_weno_dev, the drop-in form) instead of one face-independent set; "
+                         "stretched: per-face arrays of a tanh-stretched grid (weno_sb_coefficients)")
     ap.add_argument("--only", choices=["adjoint", "batched"], default=None,
                     help="run only this side measurement on cuda:0 and print its JSON line "
                          "(a short command whose kernels can be profiled alone)")

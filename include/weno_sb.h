@@ -226,6 +226,20 @@ int weno_sb_checksum_dev(int dtype, const void *arr, int64_t n, void *scratch,
 int weno_sb_checksum_noalloc(int dtype, const void *const *arrays, const int64_t *n, int count,
                              double *d_results, void *stream);
 
+/* Coefficients of WENO-JS reconstruction, order 3/5/7, for a grid with any
+ * cell widths -- MFC's s_compute_weno_coefficients, for which the reference
+ * substitutes synthetic values (f90:246-279).  x_cb[0..ns] are the cell
+ * boundaries along one sweep (ns = the direction's Ns, ghost cells
+ * included, increasing); the outputs are HOST arrays in the layouts above
+ * with NC = ns - 6 core faces (core face c is sweep cell c + 3), entries
+ * the order does not use set to 0.  Follows C.-W. Shu, ICASE Report 97-65
+ * (1997), sections 2.1-2.2 (stencil values from the primitive function,
+ * linear weights) and Jiang & Shu, JCP 126 (1996) (smoothness indicators).
+ * Host computation only (set-up time): upload the arrays, or pass them to
+ * weno_sb_weno_dev after copying them to the device. */
+int weno_sb_coefficients(int order, int64_t ns, const double *x_cb, double *polyL, double *polyR,
+                         double *dL, double *dR, double *beta_coef);
+
 /* ===================================================================== */
 /* Batches of uneven blocks (no counterpart in the reference, which runs   */
 /* one block): one persistent launch, captured in a CUDA graph.            */

@@ -90,6 +90,10 @@ def _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel, coef_
         coefs = varying_coefficients(order, nc, seed=d + 10 * order)
         coefs[2][1, ::7] = -0.05
         coefs[3][0, 3::7] = -0.02
+    elif coef_kind == "stretched":
+        # true WENO-JS coefficients of a tanh-stretched axis (weno_sb_coefficients)
+        cells = (m, n, p)[d] + 1
+        coefs = api.weno_coefficients(order, api.stretched_boundaries(cells, 6, ratio=4.0, centre=0.3 + 0.2 * d))
     elif coef_kind == "negative_uniform":
         coefs = fields.uniform_weno_coefficients(order, nc)
         coefs[2][1, :] = -0.05
@@ -160,6 +164,19 @@ def test_face_varying_coefficients(wsb, oracle_mod, order, scheme, folded, mp, k
     for dims in GRIDS:
         for d in range(3):
             Lg, Rg, Lr, Rr, mg = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel, "varying")
+            _check(Lg, Rg, Lr, Rr, scheme, (dims, d), mg)
+
+
+@pytest.mark.parametrize("mp", [False, True])
+@pytest.mark.parametrize("folded", [False, True])
+@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3), (7, 3)])
+def test_stretched_grid_coefficients(wsb, oracle_mod, order, scheme, folded, mp):
+    """Coefficients of a stretched grid from weno_sb_coefficients (every
+    face its own values, as MFC computes them for a non-uniform mesh)
+    through the per-face coefficient arrays: 1e-12 per array."""
+    for dims in GRIDS:
+        for d in range(3):
+            Lg, Rg, Lr, Rr, mg = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, "auto", "stretched")
             _check(Lg, Rg, Lr, Rr, scheme, (dims, d), mg)
 
 

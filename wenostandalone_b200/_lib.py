@@ -55,7 +55,7 @@ EXPORTED = [
     "weno_sb_weno_dev", "weno_sb_weno_uniform_dev", "weno_sb_vjp_dev", "weno_sb_preserve_monotonicity_dev",
     "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev", "weno_sb_check_device",
     "weno_sb_selftest_rcp", "weno_sb_selftest_timeout", "weno_sb_checksum_noalloc",
-    "weno_sb_batch_create", "weno_sb_batch_autotune", "weno_sb_batch_launch", "weno_sb_batch_destroy",
+    "weno_sb_coefficients", "weno_sb_batch_create", "weno_sb_batch_autotune", "weno_sb_batch_launch", "weno_sb_batch_destroy",
 ]
 
 
@@ -140,6 +140,7 @@ def lib() -> ctypes.CDLL:
         "weno_sb_selftest_rcp": ([vp, vp, vp, ctypes.c_int64, vp], i32),
         "weno_sb_selftest_timeout": ([ctypes.c_int64, vp], i32),
         "weno_sb_checksum_noalloc": ([i32, ctypes.POINTER(ctypes.c_void_p), i64p, i32, vp, vp], i32),
+        "weno_sb_coefficients": ([i32, ctypes.c_int64, vp, vp, vp, vp, vp, vp], i32),
         "weno_sb_batch_create": ([ctypes.POINTER(WenoBlock), i32, ctypes.POINTER(ctypes.c_int)], i32),
         "weno_sb_batch_autotune": ([i32, vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_double)], i32),

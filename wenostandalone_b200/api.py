@@ -381,3 +381,42 @@ class Batch:
                 lib().weno_sb_batch_destroy(self.handle)
         except Exception:
             pass
+
+
+def weno_coefficients(order: int, x_cb):
+    """(polyL, polyR, dL, dR, beta_coef) of WENO-JS for order 3/5/7 on the
+    grid whose cell boundaries along the sweep are ``x_cb`` (Ns + 1
+    increasing values, ghost cells included), as Fortran-ordered host arrays
+    of the harness layouts (NC = Ns - 6).  Computed by the library
+    (weno_sb_coefficients): MFC's s_compute_weno_coefficients, which the
+    reference replaces by synthetic values (f90:246-279)."""
+    x = np.ascontiguousarray(x_cb, dtype=np.float64)
+    ns = x.size - 1
+    nc = ns - 6
+    if nc < 1:
+        raise ValueError(f"need at least 7 cells (got {ns})")
+    pL = np.zeros((nc, 5, 3), order="F")
+    pR = np.zeros((nc, 5, 3), order="F")
+    dL = np.zeros((5, nc), order="F")
+    dR = np.zeros((5, nc), order="F")
+    bc = np.zeros((nc, 5, 6), order="F")
+    L.check(L.lib().weno_sb_coefficients(int(order), ns, x.ctypes.data, pL.ctypes.data, pR.ctypes.data,
+                                         dL.ctypes.data, dR.ctypes.data, bc.ctypes.data))
+    return pL, pR, dL, dR, bc
+
+
+def stretched_boundaries(cells: int, buff: int, ratio: float = 4.0, centre: float = 0.5, width: float = 0.1):
+    """Cell boundaries of one axis with `cells` interior cells on [0, 1] and
+    `buff` ghost cells per side (mirrored widths): a tanh refinement centred
+    on `centre`, whose cells are up to `ratio` times narrower there than
+    far away (the kind of grid MFC clusters around a feature).  Returns
+    cells + 2 buff + 1 increasing values (the sweep's Ns + 1 boundaries)."""
+    s = np.linspace(0.0, 1.0, 4097)
+    dens = 1.0 + (ratio - 1.0) * (1.0 - np.tanh((s - centre) / width) ** 2)
+    cum = np.concatenate([[0.0], np.cumsum(0.5 * (dens[1:] + dens[:-1]) * np.diff(s))])
+    cum /= cum[-1]
+    inner = np.interp(np.linspace(0.0, 1.0, cells + 1), cum, s)
+    w = np.diff(inner)
+    left = inner[0] - np.cumsum(w[:buff])[::-1]
+    right = inner[-1] + np.cumsum(w[::-1][:buff])
+    return np.concatenate([left, inner, right])

@@ -25,6 +25,7 @@
 #include "sweep_march.cuh"
 #include "sweep_march_tma.cuh"
 #include "vjp_march.cuh"
+#include "weno_coefficients.h"
 #include "weno_adjoint.cuh"
 #include "batched.cuh"
 
@@ -1006,6 +1007,24 @@ int weno_sb_checksum(int handle, int which, double* result) {
     if (rc) return rc;
     WSB_CUDA(cudaMemcpyAsync(result, H->sum_scratch + kSumBlocks, sizeof(double), cudaMemcpyDeviceToHost, H->stream));
     return cuda_err(cudaStreamSynchronize(H->stream), "checksum");
+}
+
+// ---------------- coefficients for arbitrary cell widths ----------------
+int weno_sb_coefficients(int order, int64_t ns, const double* x_cb, double* polyL, double* polyR, double* dL,
+                         double* dR, double* beta_coef) {
+    if (order != 3 && order != 5 && order != 7)
+        return set_err(WENO_SB_ERR_ARG, "order must be 3, 5 or 7 (got %d)", order);
+    if (ns < 7) return set_err(WENO_SB_ERR_ARG, "need at least 7 cells along the sweep (got %lld)", (long long)ns);
+    if (!x_cb || !polyL || !polyR || !dL || !dR || !beta_coef) return set_err(WENO_SB_ERR_ARG, "NULL pointer");
+    for (int64_t k = 0; k <= ns; ++k) {
+        if (!std::isfinite(x_cb[k])) return set_err(WENO_SB_ERR_ARG, "cell boundary %lld is not finite", (long long)k);
+        if (k > 0 && !(x_cb[k] > x_cb[k - 1]))
+            return set_err(WENO_SB_ERR_ARG, "cell boundaries must increase (x_cb[%lld] <= x_cb[%lld])", (long long)k,
+                           (long long)(k - 1));
+    }
+    if (wsb::coef::generate(order, ns, x_cb, polyL, polyR, dL, dR, beta_coef) != 0)
+        return set_err(WENO_SB_ERR_ARG, "degenerate stencil in the cell boundaries");
+    return 0;
 }
 
 // ---------------- checksum without allocation ----------------

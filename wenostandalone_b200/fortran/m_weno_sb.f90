@@ -235,6 +235,18 @@ module m_weno_sb
             type(c_ptr), value :: d_results, stream
         end function weno_sb_checksum_noalloc
 
+        !> WENO-JS coefficients of order 3/5/7 for any cell widths (MFC's
+        !! s_compute_weno_coefficients): x_cb(1:ns+1) the cell boundaries
+        !! along the sweep; host arrays in the harness layouts, NC = ns - 6
+        integer(c_int) function weno_sb_coefficients(order, ns, x_cb, polyL, polyR, dL, dR, beta_coef) &
+            bind(C, name='weno_sb_coefficients')
+            import :: c_int, c_int64_t, c_double
+            integer(c_int), value :: order
+            integer(c_int64_t), value :: ns
+            real(c_double), intent(in) :: x_cb(*)
+            real(c_double), intent(out) :: polyL(*), polyR(*), dL(*), dR(*), beta_coef(*)
+        end function weno_sb_coefficients
+
         ! ---- batches of uneven blocks (one persistent launch in a CUDA graph)
 
         integer(c_int) function weno_sb_batch_create(blocks, n, batch) bind(C, name='weno_sb_batch_create')
