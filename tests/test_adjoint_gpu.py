@@ -2,9 +2,10 @@
 
 Checked three ways: against forward-mode dual-number differentiation of the
 reference formulas (oracle/weno_oracle_ad.cpp) at 1e-9 max-norm relative (1e-8 for WENO3)
-error; against central finite differences (unit-norm direction, step 1e-4,
-smooth data, JS and TENO, with and without MP, cells near kinks held fixed)
-to 1e-6; and with torch.autograd.gradcheck through a ctypes autograd wrapper.
+error; against central finite differences (unit-norm direction, steps 1e-4
+and 1e-6, smooth data, JS and TENO, with and without MP, cells near kinks
+held fixed; per-face and marching adjoints) to 1e-6; and with
+torch.autograd.gradcheck through a ctypes autograd wrapper.
 """
 import numpy as np
 import pytest
@@ -155,20 +156,34 @@ def _mp_safe_cells(rs, L, R, margin=1e-3, half_width=2):
 
 # TENO7 is left out: the reference's beta(4) term (f90:1489-1491) outweighs
 # every stencil, so its faces and their gradient are identically zero.
-@pytest.mark.parametrize("order,scheme,mp", [(5, 0, False), (5, 0, True), (7, 0, False), (7, 0, True),
-                                             (5, 3, False), (5, 3, True)])
-def test_vjp_central_differences(wsb, oracle_mod, order, scheme, mp):
-    """<gv, dv> against (F(v+h dv) - F(v-h dv)) . g / 2h with h = 1e-4 along a
-    random unit-norm direction dv, on the smooth 128^3-cell, v_size=5 input,
-    cotangents N(0,1), JS or TENO (teno_CT=1e-5) weights.  dv is zero on the
-    cells whose stencils reach a kink: MP faces that _mp_bad_faces flags, and
-    TENO faces whose output changes when teno_CT moves by a factor of 2 (a
-    stencil within reach of the cutoff).  Bar: 1e-6 relative.
+FD_CASES = [(o, sc, mp, entry, 1e-4) for (o, sc, mp) in
+            [(5, 0, False), (5, 0, True), (7, 0, False), (7, 0, True), (5, 3, False), (5, 3, True)]
+            for entry in ("arrays", "uniform")]
+# the configuration's own step, on the benchmarked adjoint (WENO5-JS + MP)
+FD_CASES += [(5, 0, True, "uniform", 1e-6), (5, 0, True, "arrays", 1e-6)]
 
-    h: dv is spread over ~1e7 cells, so a cell moves by ~h * 3e-4, far inside
-    the 1e-3 limiter margin, and the O(h^2) truncation stays near 1e-9; the
-    rounding noise of the two forward sums (~1e-13 absolute) divided by 2h is
-    what a smaller h would amplify (h = 1e-6 puts it at the 1e-6 bar)."""
+
+@pytest.mark.parametrize("order,scheme,mp,entry,h", FD_CASES)
+def test_vjp_central_differences(wsb, oracle_mod, order, scheme, mp, entry, h):
+    """<gv, dv> against (F(v+h dv) - F(v-h dv)) . g / 2h along a unit-norm
+    direction dv, on the smooth 128^3-cell, v_size=5 input, cotangents
+    N(0,1), JS or TENO (teno_CT=1e-5) weights; the adjoint through the
+    per-face coefficient arrays (vjp_kernel) and through the face-independent
+    entry (for WENO5-JS + MP the marching adjoint, vjp_march_kernel, which
+    the bench times).  dv is zero on the cells whose stencils reach a kink:
+    MP faces that _mp_bad_faces flags, and TENO faces whose output changes
+    when teno_CT moves by a factor of 2 (a stencil within reach of the
+    cutoff).  Bar: 1e-6 relative.
+
+    Steps.  h = 1e-4 with dv random: a cell moves by ~h * 3e-4, far inside
+    the 1e-3 limiter margin, and the O(h^2) truncation stays near 1e-9.
+    h = 1e-6 (the configuration's step): each forward face state carries
+    ~1e-16 of rounding, which the difference quotient turns into ~5e-11 per
+    face and ~3e-7 after the ~4e7-term dot product with N(0,1) cotangents --
+    against |<gv, dv>| ~ 1 for a random dv that would sit at the bar.  So at
+    h = 1e-6 dv is the masked mix (gv + random) / norm, whose <gv, dv> is
+    ~|gv| / sqrt(2) ~ 3e3: the same rounding is then ~1e-10 relative, and the
+    truncation ~1e-12."""
     import torch
     from wenostandalone_b200 import api, fields
     m = 127
@@ -186,7 +201,10 @@ def test_vjp_central_differences(wsb, oracle_mod, order, scheme, mp):
         gL = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
         gR = torch.randn(n, generator=gen, device="cuda", dtype=torch.float64)
         gv = torch.empty_like(rs)
-        api.vjp(g, d, order, rs, coefs, gL, gR, gv, flags=flags)
+        if entry == "uniform":
+            api.vjp(g, d, order, rs, coefs_np, gL, gR, gv, flags=flags, uniform=True)
+        else:
+            api.vjp(g, d, order, rs, coefs, gL, gR, gv, flags=flags)
         dv = torch.randn(rs.numel(), generator=gen, device="cuda", dtype=torch.float64)
 
         def faces(grid):
@@ -202,12 +220,15 @@ def test_vjp_central_differences(wsb, oracle_mod, order, scheme, mp):
             bad |= (lo[0] != hi[0]) | (lo[1] != hi[1])
         if mp:
             bad |= _mp_bad_faces(rs_np, *faces(g))
+        mask = None
         if scheme == 3 or mp:
-            mask = _cells_clear_of(bad, rs_np.shape, hw)
-            assert mask.mean() > 0.3  # most of the smooth field is away from kinks
-            dv = dv * to_dev(mask.astype(np.float64))
+            mask = to_dev(_cells_clear_of(bad, rs_np.shape, hw).astype(np.float64))
+            assert float(mask.mean()) > 0.3  # most of the smooth field is away from kinks
+            dv = dv * mask
+        if h < 1e-5:
+            gdir = gv * mask if mask is not None else gv.clone()
+            dv = dv / torch.linalg.vector_norm(dv) + gdir / torch.linalg.vector_norm(gdir)
         dv = dv / torch.linalg.vector_norm(dv)
-        h = 1e-4
         outs = []
         for sgn in (1.0, -1.0):
             L = torch.zeros(n, dtype=torch.float64, device="cuda")
@@ -216,7 +237,7 @@ def test_vjp_central_differences(wsb, oracle_mod, order, scheme, mp):
             outs.append(float((L * gL).sum() + (R * gR).sum()))
         fd = (outs[0] - outs[1]) / (2 * h)
         an = float((gv * dv).sum())
-        assert abs(fd - an) <= 1e-6 * abs(an), (d, fd, an)
+        assert abs(fd - an) <= 1e-6 * abs(an), (d, entry, h, fd, an)
 
 
 def test_autograd_gradcheck_16cubed(wsb):
