@@ -679,8 +679,10 @@ def _batch_blocks(n_blocks=96, seed=96):
 
 def measure_batched(dev, K):
     """96 uneven blocks (x/y/z sweeps each, MP fused, folded input) as one
-    persistent launch in a CUDA graph with autotuned tiles, FP64 and
-    FP32-bulk; FP64 also as one launch per sweep for comparison."""
+    CUDA graph launch, run the way the autotuner picks (one persistent
+    kernel over all blocks, or per-block specialised sweeps on parallel
+    graph branches), FP64 and FP32-bulk; the other way and, FP64, one
+    launch per sweep for comparison."""
     import torch
 
     import wenostandalone_b200 as wsb
@@ -711,11 +713,22 @@ def measure_batched(dev, K):
         b = api.Batch(entries)
         try:
             t, u, tune_ms = b.autotune(stream=sp)
+            mode, _, _, nb = b.query()
             ms = _time_steps(lambda: b.launch(stream=sp), stream, K)
+            # the other way of running the batch, at its default layout
+            other = {}
+            if mode == 1:
+                b.configure(0, 128, 8, nb)
+                other["persistent_kernel_ms"] = _time_steps(lambda: b.launch(stream=sp), stream, K)
+            else:
+                b.configure(1, t, u, 8)
+                other["graph_of_sweeps_8_branches_ms"] = _time_steps(lambda: b.launch(stream=sp), stream, K)
         finally:
             b.close()
-        r = {"ms_per_step": ms, "value": fs / (ms * 1e-3), "face_states": fs, "tile": {"threads": t, "cols": u},
-             "launches_per_step": 1}
+        r = {"ms_per_step": ms, "value": fs / (ms * 1e-3), "face_states": fs,
+             "choice": ({"mode": "graph of specialised sweeps", "branches": nb} if mode == 1 else
+                        {"mode": "persistent kernel", "threads": t, "cols": u}),
+             "graph_launches_per_step": 1, **other}
         if dt == torch.float64:
             structs = [api.coefs_struct(e["coefs"]) for e in entries]
 

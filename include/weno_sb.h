@@ -256,14 +256,26 @@ typedef struct weno_sb_block {
     void *vL, *vR;         /* face states (device)                           */
 } weno_sb_block;
 
-/* Validate the blocks and build the device work list (allocates). */
+/* Validate the blocks and build the device work list (allocates).  The
+ * coefficient arrays are read back once here: blocks whose arrays hold the
+ * same values on every face get the face-independent kernels, so their
+ * coefficients must not change while the batch lives. */
 int weno_sb_batch_create(const weno_sb_block *blocks, int n, int *batch);
-/* Time the candidate tile shapes (CTA width x columns per work item) on
- * `stream` and keep the fastest; with WENO_SB_TUNE_CACHE naming a file,
- * a batch of the same composition reuses the recorded choice. */
+/* Time the ways of running the batch on `stream` and keep the fastest:
+ * mode 0, one persistent kernel over all blocks (candidate tile shapes:
+ * CTA width x columns per work item), and mode 1, every block's sweep by
+ * the sweep kernel specialised for it, spread over 1..16 parallel branches
+ * of the graph (candidate branch counts).  With WENO_SB_TUNE_CACHE naming a
+ * file, a batch of the same composition reuses the recorded choice.
+ * threads / cols_per_item report the persistent layout. */
 int weno_sb_batch_autotune(int batch, void *stream, int *threads, int *cols_per_item, double *best_ms);
-/* Run every block's sweep: one graph launch (counter reset + persistent
- * kernel), captured on first use. */
+/* Choose the way explicitly: mode 0 with threads (64/128/256) and
+ * cols_per_item (1..64), or mode 1 with branches (1..16). */
+int weno_sb_batch_configure(int batch, int mode, int threads, int cols_per_item, int branches);
+/* The current choice (any pointer may be NULL). */
+int weno_sb_batch_query(int batch, int *mode, int *threads, int *cols_per_item, int *branches);
+/* Run every block's sweep: one graph launch, captured on first use after
+ * the choice last changed. */
 int weno_sb_batch_launch(int batch, void *stream);
 int weno_sb_batch_destroy(int batch);
 

@@ -71,26 +71,51 @@ def _check(entries, checks):
                 assert rel_err(got, ref) <= tol, (g, d, e["order"], fp32)
 
 
+def _relaunch_and_check(b, entries, checks):
+    import torch
+    for e in entries:
+        e["vL"].fill_(float("nan"))
+        e["vR"].fill_(float("nan"))
+    for _ in range(2):
+        b.launch()
+    torch.cuda.synchronize()
+    _check(entries, checks)
+
+
 @pytest.mark.parametrize("coefficients", ["varying", "uniform"])
 def test_batch_matches_oracle_per_block(oracle_mod, coefficients):
-    import torch
+    """Both ways of running a batch -- the persistent kernel (two tile
+    shapes) and the graph of per-block sweeps (1, 3 and 16 branches) --
+    then the autotuner's choice."""
     import wenostandalone_b200 as wsb
     from wenostandalone_b200 import api
     entries, checks = _make_blocks(wsb, oracle_mod, uniform=coefficients == "uniform")
     b = api.Batch(entries)
     try:
-        for _ in range(2):
-            b.launch()
-        torch.cuda.synchronize()
-        _check(entries, checks)
+        _relaunch_and_check(b, entries, checks)          # the default choice
+        for cfg in ((0, 128, 8, 8), (0, 64, 32, 8), (1, 128, 8, 1), (1, 128, 8, 3), (1, 128, 8, 16)):
+            b.configure(*cfg)
+            assert b.query() == cfg if cfg[0] == 0 else b.query()[0::3] == (1, cfg[3])
+            _relaunch_and_check(b, entries, checks)
         t, u, ms = b.autotune()
         assert t in (64, 128, 256) and u in (4, 8, 16, 32) and ms > 0
-        for e in entries:
-            e["vL"].fill_(float("nan"))
-            e["vR"].fill_(float("nan"))
-        b.launch()
-        torch.cuda.synchronize()
-        _check(entries, checks)
+        mode, _, _, nb = b.query()
+        assert mode in (0, 1) and 1 <= nb <= 16
+        _relaunch_and_check(b, entries, checks)
+    finally:
+        b.close()
+
+
+def test_batch_configure_rejects_bad_choices(oracle_mod):
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import _lib as L, api
+    entries, _ = _make_blocks(wsb, oracle_mod, n_blocks=2)
+    b = api.Batch(entries)
+    try:
+        for cfg in ((2, 128, 8, 8), (0, 96, 8, 8), (0, 128, 0, 8), (1, 128, 8, 0), (1, 128, 8, 17)):
+            with pytest.raises(L.WenoError) as e:
+                b.configure(*cfg)
+            assert e.value.code == L.ERR_ARG
     finally:
         b.close()
 

@@ -2,19 +2,23 @@
 smooth sinusoid field (modes 1-8, amplitude 0.5 on a mean of 1), WENO5 and
 WENO7 with JS weights, x/y/z sweeps, with and without the MP limiter.
 
-The error of the FP32-bulk face states against the FP64 oracle on the FP64
+The error of the FP32-bulk face states against the FP64 result on the FP64
 field splits into
-  (a) storage: the FP64 oracle run on the FP32-rounded field against the FP64
-      oracle on the FP64 field -- what any computation from FP32 inputs
-      inherits, measured here on the CPU;
-  (b) arithmetic: the GPU FP32-bulk result against the FP64 oracle on the
-      same FP32-rounded field.
-Without MP both are small and the total meets the 1e-6 max-norm bar.  With
-MP the limiter's bounds take the input with coefficient sums near 20 (the
-curvature minmod |4 d_j - d_(j+1)| over second differences, times 4/3 and
-1/2), so (a) alone reaches ~1.0-1.1e-6 on this field: the bar for the total
-is then (a) plus the arithmetic bar.  Max and RMS (relative to the array's
-max and RMS) are printed per output array.
+  (a) storage: the FP64 result on the FP32-rounded field against the FP64
+      result on the FP64 field -- what any computation from FP32 inputs
+      inherits;
+  (b) arithmetic: the FP32-bulk result against the FP64 result on the same
+      FP32-rounded field.
+The FP64 results are the library's FP64 sweeps, which the parity tests hold
+to 1e-12 of the oracle; here the oracle pins them again on the first
+variable of every direction (1e-12), so the decomposition rests on the
+oracle without running it on all 10 variables.
+Without MP both parts are small and the total meets the 1e-6 max-norm bar.
+With MP the limiter's bounds take the input with coefficient sums near 20
+(the curvature minmod |4 d_j - d_(j+1)| over second differences, times 4/3
+and 1/2), so (a) alone reaches ~1.0-1.1e-6 on this field, and the bar for
+the total is (a) plus the arithmetic bar.  Max (relative to the array's max)
+and RMS (relative to its RMS) are printed per output array.
 """
 import numpy as np
 import pytest
@@ -22,67 +26,77 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 M, NV = 255, 10
-ARITH_MAX = 3e-7     # (b), max-norm relative, every array
+ARITH_MAX = 1e-7     # (b), max-norm relative, every array (measured ~4.3e-8)
 TOTAL_NO_MP = 1e-6   # (a) + (b) without the limiter: the FP32-bulk bar
 RMS_BAR = 1e-7
 
 
 def _err(got, ref):
-    den = float(np.abs(ref).max())
-    return (float(np.abs(got - ref).max()) / den,
-            float(np.sqrt(np.mean((got - ref) ** 2)) / np.sqrt(np.mean(ref ** 2))))
+    den = float(ref.abs().max())
+    d = got - ref
+    return float(d.abs().max()) / den, float(d.pow(2).mean().sqrt() / ref.pow(2).mean().sqrt())
 
 
-@pytest.mark.parametrize("mp", [True, False])
 @pytest.mark.parametrize("order", [5, 7])
-def test_fp32_bulk_error_at_256cubed(oracle_mod, order, mp):
+def test_fp32_bulk_error_at_256cubed(oracle_mod, order):
     import torch
     import wenostandalone_b200 as wsb
     from wenostandalone_b200 import api, fields
     g = wsb.Grid(M, M, M, NV, 6)
-    vdev = fields.sinusoid_shock_field_dev(M, M, M, NV, 6, seed=11, shock=False)
+    v64 = fields.sinusoid_shock_field_dev(M, M, M, NV, 6, seed=11, shock=False)
+    v32r = v64.float().double()                      # the FP32-rounded field, in FP64
     shp = fields.vf_shape(M, M, M, NV, 6)
-    # the device field is flat in the (x, y, z, nv) Fortran order of v_vf
-    vf = np.asfortranarray(vdev.cpu().numpy().reshape(shp, order="F"))
-    vf32 = np.asfortranarray(vf.astype(np.float32).astype(np.float64))
-    flags = wsb.F_MP if mp else 0
-    worst = {"storage": 0.0, "arith": 0.0, "total": 0.0}
-    for d in range(3):
-        ns = g.extents(d)[0]
-        core = slice(3, ns - 3)
-        coefs = fields.uniform_weno_coefficients(order, g.nc(d))
-        refs = []
-        for field in (vf, vf32):
-            rs = oracle_mod.reshape(field, M, M, M, 6, d)
-            L, R = oracle_mod.reconstruct(rs, coefs, order)
+    nvf = int(np.prod(shp[:3]))
+    # the first variable of the FP64 field on the host, for the oracle pin
+    vf0 = np.asfortranarray(v64[:nvf].cpu().numpy().reshape(shp[:3] + (1,), order="F"))
+    worst = {}
+    for mp in (False, True):
+        flags = wsb.F_MP if mp else 0
+        tag = f"WENO{order}{' + MP' if mp else ''}"
+        for d in range(3):
+            ns = g.extents(d)[0]
+            nface = int(np.prod(g.face_shape(d)))
+            coefs = fields.uniform_weno_coefficients(order, g.nc(d))
+            refs = []
+            for field in (v64, v32r):
+                L = torch.zeros(nface, dtype=torch.float64, device="cuda")
+                R = torch.zeros_like(L)
+                api.weno_uniform(g, d, order, field, coefs, L, R, flags=flags | wsb.F_FOLDED)
+                refs.append((L.view(-1, ns)[:, 3:ns - 3], R.view(-1, ns)[:, 3:ns - 3]))
+            # pin the FP64 reference to the oracle on variable 0
+            rs = oracle_mod.reshape(vf0, M, M, M, 6, d)
+            Lo, Ro = oracle_mod.reconstruct(rs, coefs, order)
             if mp:
-                oracle_mod.preserve_monotonicity(rs, L, R)
-            refs.append((L[core].copy(), R[core].copy()))
-            del rs, L, R
-        rs32 = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float32, device="cuda")
-        api.reshape(g, d, vdev, rs32)
-        L32 = torch.zeros(int(np.prod(g.face_shape(d))), dtype=torch.float32, device="cuda")
-        R32 = torch.zeros_like(L32)
-        api.weno_uniform(g, d, order, rs32, coefs, L32, R32, flags=flags)
-        torch.cuda.synchronize()
-        del rs32
-        for k, (nm, t) in enumerate((("vL", L32), ("vR", R32))):
-            got = t.double().cpu().numpy().reshape(g.face_shape(d), order="F")[core]
-            ref64, ref32 = refs[0][k], refs[1][k]
-            st, st_rms = _err(ref32, ref64)
-            ar, ar_rms = _err(got, ref32)
-            to, to_rms = _err(got, ref64)
-            print(f"WENO{order}{' + MP' if mp else ''} {nm}_{'xyz'[d]}: total max {to:.3e} rms {to_rms:.3e}; "
-                  f"storage max {st:.3e} rms {st_rms:.3e}; arithmetic max {ar:.3e} rms {ar_rms:.3e}")
-            worst["storage"] = max(worst["storage"], st)
-            worst["arith"] = max(worst["arith"], ar)
-            worst["total"] = max(worst["total"], to)
-            assert ar <= ARITH_MAX, (nm, d, ar)
-            assert to_rms <= RMS_BAR and ar_rms <= RMS_BAR, (nm, d, to_rms, ar_rms)
-            if mp:
-                assert to <= st + ARITH_MAX, (nm, d, to, st)
-            else:
-                assert to <= TOTAL_NO_MP, (nm, d, to)
-        del L32, R32, refs
-        torch.cuda.empty_cache()
-    print(f"WENO{order}{' + MP' if mp else ''} worst: {worst}")
+                oracle_mod.preserve_monotonicity(rs, Lo, Ro)
+            n0 = nface // NV
+            for ref, o in ((refs[0][0], Lo), (refs[0][1], Ro)):
+                got0 = ref.reshape(-1)[: n0 // ns * (ns - 6)].cpu().numpy()
+                exp0 = o.reshape(ns, -1, order="F")[3:ns - 3].T.reshape(-1)
+                assert np.max(np.abs(got0 - exp0)) <= 1e-12 * np.max(np.abs(exp0))
+            rs32 = torch.empty(int(np.prod(g.rs_shape(d))), dtype=torch.float32, device="cuda")
+            api.reshape(g, d, v64, rs32)
+            L32 = torch.zeros(nface, dtype=torch.float32, device="cuda")
+            R32 = torch.zeros_like(L32)
+            api.weno_uniform(g, d, order, rs32, coefs, L32, R32, flags=flags)
+            del rs32
+            for k, (nm, t) in enumerate((("vL", L32), ("vR", R32))):
+                got = t.view(-1, ns)[:, 3:ns - 3].double()
+                ref64, ref32 = refs[0][k], refs[1][k]
+                st, st_rms = _err(ref32, ref64)
+                ar, ar_rms = _err(got, ref32)
+                to, to_rms = _err(got, ref64)
+                print(f"{tag} {nm}_{'xyz'[d]}: total max {to:.3e} rms {to_rms:.3e}; storage max {st:.3e} "
+                      f"rms {st_rms:.3e}; arithmetic max {ar:.3e} rms {ar_rms:.3e}")
+                w = worst.setdefault(tag, {"storage": 0.0, "arith": 0.0, "total": 0.0})
+                w["storage"] = max(w["storage"], st)
+                w["arith"] = max(w["arith"], ar)
+                w["total"] = max(w["total"], to)
+                assert ar <= ARITH_MAX, (tag, nm, d, ar)
+                assert to_rms <= RMS_BAR and ar_rms <= RMS_BAR, (tag, nm, d, to_rms, ar_rms)
+                if mp:
+                    assert to <= st + ARITH_MAX, (tag, nm, d, to, st)
+                else:
+                    assert to <= TOTAL_NO_MP, (tag, nm, d, to)
+            del L32, R32, refs
+            torch.cuda.empty_cache()
+    print(f"worst per form: {worst}")

@@ -148,12 +148,13 @@ def test_noalloc_allocates_no_device_memory():
             vals.append(int(v))
         return free, vals, torch.cuda.memory_allocated(), torch.cuda.memory_reserved()
 
-    before = state()
     lib = L.lib()
     k = len(arrays)
     ptrs = (ctypes.c_void_p * k)(*[t.data_ptr() for t in arrays])
     ns = (ctypes.c_int64 * k)(*[t.numel() for t in arrays])
     res = torch.empty(k, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    before = state()
     for _ in range(20):
         L.check(lib.weno_sb_checksum_noalloc(L.FP64, ptrs, ns, k, res.data_ptr(), None))
     torch.cuda.synchronize()

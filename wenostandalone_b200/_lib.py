@@ -56,6 +56,7 @@ EXPORTED = [
     "weno_sb_checksum_scratch_bytes", "weno_sb_checksum_dev", "weno_sb_check_device",
     "weno_sb_selftest_rcp", "weno_sb_selftest_timeout", "weno_sb_checksum_noalloc",
     "weno_sb_coefficients", "weno_sb_batch_create", "weno_sb_batch_autotune", "weno_sb_batch_launch", "weno_sb_batch_destroy",
+    "weno_sb_batch_configure", "weno_sb_batch_query",
 ]
 
 
@@ -146,6 +147,9 @@ def lib() -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_double)], i32),
         "weno_sb_batch_launch": ([i32, vp], i32),
         "weno_sb_batch_destroy": ([i32], i32),
+        "weno_sb_batch_configure": ([i32, i32, i32, i32, i32], i32),
+        "weno_sb_batch_query": ([i32, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

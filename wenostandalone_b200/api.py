@@ -334,7 +334,9 @@ def checksum(arr, stream=None) -> float:
 
 
 class Batch:
-    """Many uneven blocks' sweeps in one persistent, graph-captured launch.
+    """Many uneven blocks' sweeps in one graph launch (a persistent kernel over
+    all blocks, or per-block specialised sweeps on parallel graph branches;
+    autotune() picks the faster).
 
     `entries`: sequence of dicts with keys grid (Grid), dir, order, flags,
     v_in, coefs (5 device tensors), vL, vR (CUDA tensors; float32 tensors
@@ -366,6 +368,17 @@ class Batch:
         check(lib().weno_sb_batch_autotune(self.handle, _stream(stream), ctypes.byref(t), ctypes.byref(u),
                                            ctypes.byref(ms)))
         return t.value, u.value, ms.value
+
+    def configure(self, mode: int, threads: int = 128, cols_per_item: int = 8, branches: int = 8):
+        """mode 0: one persistent kernel (threads x cols_per_item work items);
+        mode 1: a graph of per-block specialised sweeps on `branches` branches."""
+        check(lib().weno_sb_batch_configure(self.handle, mode, threads, cols_per_item, branches))
+
+    def query(self):
+        """(mode, threads, cols_per_item, branches) of the current choice."""
+        v = [ctypes.c_int() for _ in range(4)]
+        check(lib().weno_sb_batch_query(self.handle, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def launch(self, stream=None):
         check(lib().weno_sb_batch_launch(self.handle, _stream(stream)))

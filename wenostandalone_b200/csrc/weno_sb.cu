@@ -470,6 +470,18 @@ int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsign
 // ----------------------------------------------------------------------
 // Batches of uneven blocks (batched.cuh)
 // ----------------------------------------------------------------------
+// Two ways to run a batch, chosen by the autotuner (or weno_sb_batch_configure):
+//  mode 0: one persistent kernel (batch_kernel) takes work items of every
+//          entry from a global counter;
+//  mode 1: every entry's sweep is the single-block sweep kernel specialised
+//          for its order, weights, precision and layout (TMA marching sweeps
+//          where one covers it), and the launches are spread over `branches`
+//          parallel branches of the graph, balanced by longest-processing-
+//          time-first on the entries' estimated cost, so small blocks run
+//          beside each other and beside the tails of large ones.
+// Either way a launch is one cudaGraphLaunch of the captured work.
+constexpr int kBatchMaxBranches = 16;
+
 struct Batch {
     std::vector<weno_sb_block> blocks;
     std::vector<BatchEntry> entries;
@@ -481,6 +493,14 @@ struct Batch {
     int threads = 128;  // face-tile width = CTA size
     int U = 8;          // columns per work item
     int grid = 0;
+    int mode = 1;       // 0: persistent kernel, 1: graph of specialised sweeps
+    int branches = 8;   // mode 1: parallel branches of the graph
+    // mode 1: each entry's face-independent coefficients (Coef<order>
+    // layout), when its arrays hold the same values on every face
+    std::vector<std::vector<double>> ucf;
+    cudaStream_t br[kBatchMaxBranches] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kBatchMaxBranches] = {};
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -534,11 +554,62 @@ int batch_enqueue(Batch* B, cudaStream_t st) {
     return cuda_err(cudaGetLastError(), "batch launch");
 }
 
-// Capture the batch (counter reset + persistent kernel) into a CUDA graph.
+// Estimated cost of one entry's sweep, for balancing the graph branches:
+// its face states, weighted by the measured cost of its engine relative to
+// FP64 WENO5-JS with face-independent coefficients.
+double batch_entry_cost(const Batch* B, size_t i) {
+    const BatchEntry& e = B->entries[i];
+    double c = 2.0 * (double)e.nf * (double)e.g.cols;
+    c *= e.order == 7 ? 1.5 : (e.order == 3 ? 0.85 : 1.0);
+    if (e.wp.scheme == WENO_SB_TENO) c *= 1.3;
+    if (B->ucf[i].empty()) c *= 1.25;
+    if (e.fp32) c *= 0.8;
+    return c;
+}
+
+// Mode 1: every entry's sweep on one of B->branches parallel streams forked
+// from (and joined back into) the capturing stream.
+int batch_enqueue_sweeps(Batch* B, cudaStream_t st) {
+    const int nb = std::max(1, std::min(B->branches, kBatchMaxBranches));
+    WSB_CUDA(cudaEventRecord(B->fork, st));
+    for (int k = 0; k < nb; ++k) WSB_CUDA(cudaStreamWaitEvent(B->br[k], B->fork, 0));
+    std::vector<size_t> order(B->entries.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::vector<double> cost(order.size());
+    for (size_t i = 0; i < order.size(); ++i) cost[i] = batch_entry_cost(B, i);
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+    std::vector<double> load(nb, 0.0);
+    int rc = 0;
+    for (size_t i : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += cost[i];
+        const weno_sb_block& b = B->blocks[i];
+        Dims d;
+        rc = check_grid(&b.grid, &d);
+        if (rc) break;
+        const double* u = B->ucf[i].empty() ? nullptr : B->ucf[i].data();
+        if (b.dtype == WENO_SB_FP64)
+            rc = run_weno<double>(d, &b.grid, b.dir, b.order, b.flags, (const double*)b.v_in, &b.coefs,
+                                  (double*)b.vL, (double*)b.vR, B->br[k], u);
+        else
+            rc = run_weno<float>(d, &b.grid, b.dir, b.order, b.flags, (const float*)b.v_in, &b.coefs, (float*)b.vL,
+                                 (float*)b.vR, B->br[k], u);
+        if (rc) break;
+    }
+    // join every branch, also after a failed launch, so a capture ends cleanly
+    for (int k = 0; k < nb; ++k) {
+        cudaEventRecord(B->join[k], B->br[k]);
+        cudaStreamWaitEvent(st, B->join[k], 0);
+    }
+    return rc;
+}
+
+// Capture the batch into a CUDA graph: mode 0 the counter reset and the
+// persistent kernel, mode 1 the branches of specialised sweeps.
 int batch_build_graph(Batch* B) {
     batch_release_graph(B);
     WSB_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
-    const int rc = batch_enqueue(B, B->cap);
+    const int rc = B->mode == 1 ? batch_enqueue_sweeps(B, B->cap) : batch_enqueue(B, B->cap);
     cudaGraph_t gph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(B->cap, &gph);
     if (rc) {
@@ -561,7 +632,10 @@ unsigned long long batch_signature(const Batch* B) {
             h *= 1099511628211ull;
         }
     };
-    for (const auto& e : B->entries) {
+    for (size_t i = 0; i < B->entries.size(); ++i) {
+        const BatchEntry& e = B->entries[i];
+        mix(e.wp.scheme);
+        mix(B->ucf[i].empty() ? 0 : 1);
         mix(e.order);
         mix(e.g.nv);
         mix(e.fp32);
@@ -1158,6 +1232,22 @@ bool batch_coefs_uniform(const weno_sb_coefs& cf, long long nc, int order, doubl
     return true;
 }
 
+// Release everything a batch owns (also a half-built one).
+void batch_free(Batch* B) {
+    if (B->cap) cudaStreamSynchronize(B->cap);
+    batch_release_graph(B);
+    if (B->d_entries) cudaFree(B->d_entries);
+    if (B->d_counter) cudaFree(B->d_counter);
+    if (B->d_margs) cudaFree(B->d_margs);
+    for (int k = 0; k < kBatchMaxBranches; ++k) {
+        if (B->br[k]) cudaStreamDestroy(B->br[k]);
+        if (B->join[k]) cudaEventDestroy(B->join[k]);
+    }
+    if (B->fork) cudaEventDestroy(B->fork);
+    if (B->cap) cudaStreamDestroy(B->cap);
+    delete B;
+}
+
 int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
     WSB_FAULT("init");
     if (!blocks || n < 1 || !batch) return set_err(WENO_SB_ERR_ARG, "need at least one block and a batch pointer");
@@ -1197,8 +1287,10 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
         const bool js = b.grid.scheme == WENO_SB_JS;
         const bool teno = b.grid.scheme == WENO_SB_TENO;
         double ucf[56];
-        if (kernel_choice() != 1 && ((b.order == 5 || b.order == 7) && (js || teno) || (b.order == 3 && js)) &&
-            batch_coefs_uniform(b.coefs, e.g.nc, b.order, ucf) && march_weights_ok(ucf, b.order)) {
+        const bool uni = batch_coefs_uniform(b.coefs, e.g.nc, b.order, ucf);
+        B->ucf.push_back(uni ? std::vector<double>(ucf, ucf + 56) : std::vector<double>());
+        if (uni && kernel_choice() != 1 && ((b.order == 5 || b.order == 7) && (js || teno) || (b.order == 3 && js)) &&
+            march_weights_ok(ucf, b.order)) {
             B->margs.push_back(make_march_args(e.g, b.v_in, b.vL, b.vR, e.wp, ucf, b.order));
             e.march = (int)B->margs.size();
         }
@@ -1215,13 +1307,14 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
                           "cudaMemcpy");
     }
     if (!rc) rc = cuda_err(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int k = 0; !rc && k < kBatchMaxBranches; ++k) {
+        rc = cuda_err(cudaStreamCreateWithFlags(&B->br[k], cudaStreamNonBlocking), "cudaStreamCreate");
+        if (!rc) rc = cuda_err(cudaEventCreateWithFlags(&B->join[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    if (!rc) rc = cuda_err(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming), "cudaEventCreate");
     if (!rc) rc = batch_layout(B, 128, 8);
     if (rc) {
-        if (B->d_entries) cudaFree(B->d_entries);
-        if (B->d_counter) cudaFree(B->d_counter);
-        if (B->d_margs) cudaFree(B->d_margs);
-        if (B->cap) cudaStreamDestroy(B->cap);
-        delete B;
+        batch_free(B);
         return rc;
     }
     std::lock_guard<std::mutex> lk(g_batch_mu);
@@ -1230,71 +1323,90 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
     return WENO_SB_OK;
 }
 
+// Time both ways of running the batch -- the persistent kernel over its
+// tile shapes (CTA width x columns per item) and the graph of specialised
+// sweeps over its branch counts -- and keep the fastest.  Each candidate is
+// captured into its graph, launched once to warm up and three times timed.
+// With WENO_SB_TUNE_CACHE naming a file, a batch of the same composition
+// reuses the recorded choice (one line: signature, threads, columns per
+// item, milliseconds, mode, branches).
 int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_item, double* best_ms) {
     Batch* B = get_batch(batch);
     if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned long long sig = batch_signature(B);
     const char* cache = getenv("WENO_SB_TUNE_CACHE");
+    auto report = [&](double ms) {
+        if (threads) *threads = B->threads;
+        if (cols_per_item) *cols_per_item = B->U;
+        if (best_ms) *best_ms = ms;
+    };
     if (cache && *cache) {
         std::ifstream f(cache);
         std::string line;
         while (std::getline(f, line)) {
             std::istringstream ls(line);
             unsigned long long h;
-            int t, u;
+            int t, u, mode = 0, nb = 8;
             double ms;
             if ((ls >> std::hex >> h >> std::dec >> t >> u >> ms) && h == sig) {
+                if (!(ls >> mode >> nb)) { mode = 0; nb = 8; }
                 int rc = batch_layout(B, t, u);
                 if (rc) return rc;
-                if (threads) *threads = t;
-                if (cols_per_item) *cols_per_item = u;
-                if (best_ms) *best_ms = ms;
+                B->mode = mode == 1 ? 1 : 0;
+                B->branches = std::max(1, std::min(nb, kBatchMaxBranches));
+                batch_release_graph(B);
+                report(ms);
                 return WENO_SB_OK;
             }
         }
     }
-    static const int cand_t[] = {64, 128, 256};
-    static const int cand_u[] = {4, 8, 16, 32};
+    struct Cand { int mode, t, u, nb; };
+    std::vector<Cand> cands;
+    for (int t : {64, 128, 256})
+        for (int u : {4, 8, 16, 32}) cands.push_back({0, t, u, 0});
+    for (int nb : {1, 2, 4, 8, 16}) cands.push_back({1, 128, 8, nb});
     cudaEvent_t e0, e1;
     WSB_CUDA(cudaEventCreate(&e0));
     WSB_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int bt = 128, bu = 8;
-    for (int t : cand_t) {
-        for (int u : cand_u) {
-            int rc = batch_layout(B, t, u);
-            if (!rc) rc = batch_enqueue(B, st);  // warm-up
-            if (rc) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return rc;
-            }
-            cudaEventRecord(e0, st);
-            for (int r = 0; r < 3; ++r) batch_enqueue(B, st);
-            cudaEventRecord(e1, st);
-            WSB_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= 3.f;
-            if (ms < best) {
-                best = ms;
-                bt = t;
-                bu = u;
-            }
+    Cand bc = cands[0];
+    int rc = 0;
+    for (const Cand& c : cands) {
+        rc = batch_layout(B, c.t, c.u);
+        if (rc) break;
+        B->mode = c.mode;
+        B->branches = c.mode == 1 ? c.nb : B->branches;
+        rc = batch_build_graph(B);
+        if (!rc) rc = cuda_err(cudaGraphLaunch(B->exec, st), "cudaGraphLaunch");  // warm-up
+        if (rc) break;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3; ++r) cudaGraphLaunch(B->exec, st);
+        cudaEventRecord(e1, st);
+        rc = cuda_err(cudaEventSynchronize(e1), "autotune");
+        if (rc) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 3.f;
+        if (ms < best) {
+            best = ms;
+            bc = c;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    int rc = batch_layout(B, bt, bu);
     if (rc) return rc;
+    rc = batch_layout(B, bc.t, bc.u);
+    if (rc) return rc;
+    B->mode = bc.mode;
+    if (bc.mode == 1) B->branches = bc.nb;
+    batch_release_graph(B);
     if (cache && *cache) {
         std::ofstream f(cache, std::ios::app);
-        f << std::hex << sig << std::dec << " " << bt << " " << bu << " " << best << "\n";
+        f << std::hex << sig << std::dec << " " << bc.t << " " << bc.u << " " << best << " " << bc.mode << " "
+          << B->branches << "\n";
     }
-    if (threads) *threads = bt;
-    if (cols_per_item) *cols_per_item = bu;
-    if (best_ms) *best_ms = best;
+    report(best);
     return WENO_SB_OK;
 }
 
@@ -1312,17 +1424,41 @@ int weno_sb_batch_launch(int batch, void* stream) {
 int weno_sb_batch_destroy(int batch) {
     Batch* B = get_batch(batch);
     if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
-    cudaStreamSynchronize(B->cap);
-    batch_release_graph(B);
-    cudaFree(B->d_entries);
-    cudaFree(B->d_counter);
-    if (B->d_margs) cudaFree(B->d_margs);
-    cudaStreamDestroy(B->cap);
     {
         std::lock_guard<std::mutex> lk(g_batch_mu);
         g_batches[batch - 1] = nullptr;
     }
-    delete B;
+    batch_free(B);
+    return WENO_SB_OK;
+}
+
+int weno_sb_batch_configure(int batch, int mode, int threads, int cols_per_item, int branches) {
+    Batch* B = get_batch(batch);
+    if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
+    if (mode != 0 && mode != 1) return set_err(WENO_SB_ERR_ARG, "mode must be 0 (persistent) or 1 (graph of sweeps)");
+    if (mode == 0) {
+        if (threads != 64 && threads != 128 && threads != 256)
+            return set_err(WENO_SB_ERR_ARG, "threads must be 64, 128 or 256 (got %d)", threads);
+        if (cols_per_item < 1 || cols_per_item > 64)
+            return set_err(WENO_SB_ERR_ARG, "cols_per_item must be 1..64 (got %d)", cols_per_item);
+        B->mode = 0;
+        return batch_layout(B, threads, cols_per_item);
+    }
+    if (branches < 1 || branches > kBatchMaxBranches)
+        return set_err(WENO_SB_ERR_ARG, "branches must be 1..%d (got %d)", kBatchMaxBranches, branches);
+    B->mode = 1;
+    B->branches = branches;
+    batch_release_graph(B);
+    return WENO_SB_OK;
+}
+
+int weno_sb_batch_query(int batch, int* mode, int* threads, int* cols_per_item, int* branches) {
+    Batch* B = get_batch(batch);
+    if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
+    if (mode) *mode = B->mode;
+    if (threads) *threads = B->threads;
+    if (cols_per_item) *cols_per_item = B->U;
+    if (branches) *branches = B->branches;
     return WENO_SB_OK;
 }
 

@@ -271,6 +271,19 @@ module m_weno_sb
             type(c_ptr), value :: stream
         end function weno_sb_batch_launch
 
+        integer(c_int) function weno_sb_batch_configure(batch, mode, threads, cols_per_item, branches) &
+            bind(C, name='weno_sb_batch_configure')
+            import :: c_int
+            integer(c_int), value :: batch, mode, threads, cols_per_item, branches
+        end function weno_sb_batch_configure
+
+        integer(c_int) function weno_sb_batch_query(batch, mode, threads, cols_per_item, branches) &
+            bind(C, name='weno_sb_batch_query')
+            import :: c_int
+            integer(c_int), value :: batch
+            integer(c_int), intent(out) :: mode, threads, cols_per_item, branches
+        end function weno_sb_batch_query
+
         integer(c_int) function weno_sb_batch_destroy(batch) bind(C, name='weno_sb_batch_destroy')
             import :: c_int
             integer(c_int), value :: batch
