@@ -460,6 +460,151 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Multi-GPU decompositions other than one block per rank (--decomp)
+# ---------------------------------------------------------------------------
+def zslab_local_field(slab, v_global):
+    """The slab's planes of the block's v_vf (a flat tensor in the Fortran
+    order (E1, E2, E3, V)): (E1, E2, nz + 2G, V), flat."""
+    E3 = v_global.numel() // (slab.E1 * slab.E2 * slab.nv)
+    z0, z1 = slab.global_planes()
+    return v_global.view(slab.nv, E3, slab.E1 * slab.E2)[:, z0:z1, :].contiguous().view(-1)
+
+
+def zslab_step(slab, v_local, sweep, group=None):
+    """One step of the z-slab decomposition: the ghost-plane exchange with
+    the neighbouring slabs, then the slab's x, y and z sweeps (sweep(d))."""
+    slab.exchange(v_local, group)
+    for d in range(3):
+        sweep(d)
+
+
+def batch_assignment(blocks, world):
+    """The batched workload's blocks per rank, longest-processing-time first
+    on their face states (every block's x, y and z sweeps stay on one rank)."""
+    from wenostandalone_b200 import sharding
+    costs = []
+    for cells, nv, order, _scheme in blocks:
+        N = [c + 2 * BUFF for c in cells]
+        fs = 0
+        for d in range(3):
+            ns = N[d]
+            nf = ns if order == 3 else ns - 6
+            fs += 2 * nf * (N[0] * N[1] * N[2] // ns) * nv
+        costs.append(fs * (1.5 if order == 7 else 1.0))
+    return sharding.lpt_assign(costs, world)
+
+
+def run_decomp(args):
+    """--decomp zslab: one 200^3 x 8 block split along z over the ranks
+    (strong scaling): per step every rank exchanges G = buff_size + 3 ghost
+    planes with its neighbours (NCCL point-to-point over NVLink; torch's
+    P2P calls on the sweeps' stream) and sweeps its slab in x, y and z
+    (FP64 WENO5-JS + MP, folded).  --decomp batch: the 96-block batched
+    workload placed on the ranks by LPT, one graph launch per rank per step
+    (strong scaling).  value = the face states of the whole job / the
+    slowest rank's device time per step."""
+    import datetime
+
+    import torch
+
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api, fields, sharding
+    rank, ws, local, dist = dist_init()
+    if dist is not None:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local if dist is not None else 0)
+    torch.cuda.set_device(dev)
+    wsb.lib()
+    stream = torch.cuda.Stream(device=dev)
+    sp = int(stream.cuda_stream)
+    K = args.steps
+    if args.decomp == "zslab":
+        slab = sharding.ZSlab(M, M, M, NV, BUFF, ws, rank)
+        v_global = fields.smooth_jump_field_dev(M, M, M, NV, BUFF, seed=0, device=dev)
+        v = zslab_local_field(slab, v_global)
+        del v_global
+        g = wsb.Grid(M, M, slab.p_local, NV, BUFF)
+        faces = [api.face_coefs(fields.uniform_weno_coefficients(5, g.nc(d))) for d in range(3)]
+        outs = [tuple(torch.empty(int(np.prod(g.face_shape(d))), dtype=torch.float64, device=dev)
+                      for _ in range(2)) for d in range(3)]
+
+        def sweep(d):
+            api.weno_uniform(g, d, 5, v, faces[d], outs[d][0], outs[d][1], flags=wsb.F_MP | wsb.F_FOLDED,
+                             stream=sp)
+
+        def step():
+            with torch.cuda.stream(stream):
+                zslab_step(slab, v, sweep)
+        fs_total = 3 * face_states_per_dir()
+        launches = 3
+        workload = (f"FP64 WENO5-JS + MP, one {M + 1}^3 x {NV} block split along z over {ws} ranks "
+                    f"({slab.nz}-cell slabs + {slab.G} ghost planes a side, exchanged each step by NCCL P2P)")
+    else:
+        blocks = _batch_blocks()
+        mine = batch_assignment(blocks, ws)[rank]
+        entries, fs_total = [], 0
+        for i, (cells, nv, order, scheme) in enumerate(blocks):
+            m, n, p = (c - 1 for c in cells)
+            gb = wsb.Grid(m, n, p, nv, BUFF, scheme=scheme)
+            for d in range(3):
+                ns, c1, c2 = gb.extents(d)
+                fs_total += 2 * (ns if order == 3 else ns - 6) * c1 * c2 * nv
+            if i not in mine:
+                continue
+            vb = fields.smooth_jump_field_dev(m, n, p, nv, BUFF, seed=100 + i, device=dev)
+            for d in range(3):
+                cf = tuple(torch.from_numpy(np.ascontiguousarray(c.ravel(order="F"))).to(dev)
+                           for c in fields.uniform_weno_coefficients(order, gb.nc(d)))
+                nface = int(np.prod(gb.face_shape(d)))
+                entries.append(dict(grid=gb, dir=d, order=order, flags=wsb.F_MP | wsb.F_FOLDED, v_in=vb, coefs=cf,
+                                    vL=torch.empty(nface, dtype=torch.float64, device=dev),
+                                    vR=torch.empty(nface, dtype=torch.float64, device=dev)))
+        b = api.Batch(entries)
+        b.autotune(stream=sp)
+
+        def step():
+            b.launch(stream=sp)
+        launches = 1
+        workload = f"96 uneven blocks (x/y/z + MP each, FP64), LPT-placed over {ws} ranks ({len(mine)} here)"
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+        e0.record(stream)
+        for _ in range(K):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / K
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if args.decomp == "batch":
+        b.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC if args.decomp == "zslab" else "batched face-states/s (96 uneven blocks, FP64)",
+            "value": fs_total / (ms * 1e-3), "unit": "face-states/s", "n_gpus": ws, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload, "decomp": args.decomp, "parallelism": f"{args.decomp} over {ws} ranks"},
+            "gpu_launches": launches * K, "clocks": clk.summary()}), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def read_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (line 'traffic_bytes_per_launch: <int>'), else None."""
@@ -895,6 +1040,10 @@ def main():
                     help="arrays: the main step passes the uniform-grid coefficients as per-face device "
                          "arrays (weno_sb_weno_dev, the drop-in form) instead of one face-independent set; "
                          "stretched: per-face arrays of a tanh-stretched grid (weno_sb_coefficients)")
+    ap.add_argument("--decomp", choices=["blocks", "zslab", "batch"], default="blocks",
+                    help="blocks: one 200^3 x 8 block per rank (weak scaling, the default); zslab: one block "
+                         "split along z with a ghost-plane exchange per step; batch: the 96-block batch placed "
+                         "on the ranks by LPT (both strong scaling)")
     ap.add_argument("--only", choices=["adjoint", "batched"], default=None,
                     help="run only this side measurement on cuda:0 and print its JSON line "
                          "(a short command whose kernels can be profiled alone)")
@@ -911,6 +1060,8 @@ def main():
         args.no_extras = True
     if args.impl == "reference":
         return run_reference(args)
+    if args.decomp != "blocks":
+        return run_decomp(args)
     return run_ours(args)
 
 

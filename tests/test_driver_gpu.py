@@ -90,7 +90,7 @@ def test_modes_other_than_weno5_run_every_family(driver, oracle_mod, tmp_path, m
     out, chk = _run(driver, _small_nml(tmp_path), tmp_path, WENO_KERNEL_MODE=mode, WENO_WARMUP_ITERS=1)
     assert f"Kernel mode              : {mode}" in out
     for k, e in zip("XYZ", exp):
-        assert abs(chk[k] - e) <= 1e-12 * e, (mode, k, chk[k], e)
+        assert abs(chk[k] - e) <= 1e-10 * e, (mode, k, chk[k], e)   # the printed 11 digits
 
 
 @pytest.mark.parametrize("split,specialized", [(0, 0), (1, 0), (0, 1)])
@@ -101,7 +101,7 @@ def test_kernel_scope_repeats_only_the_reconstruction(driver, oracle_mod, tmp_pa
                     WENO5_SPLIT_KERNELS=split, WENO5_SPECIALIZED_COMBINED=specialized)
     assert "WENO5 benchmark scope    : kernel" in out
     for k, e in zip("XYZ", exp):
-        assert abs(chk[k] - e) <= 1e-12 * e, (k, chk[k], e)
+        assert abs(chk[k] - e) <= 1e-10 * e, (k, chk[k], e)   # the printed 11 digits
 
 
 def test_all_mode_with_teno_reports_non_finite_output(driver, tmp_path):

@@ -79,3 +79,49 @@ def lpt_assign(costs, world: int):
         loads[r] += costs[i]
         out[r].append(i)
     return out
+
+
+class ZSlab:
+    """One block of (m+1) x (n+1) x (p+1) cells split along z over `world`
+    ranks: this rank's slab of nz cells, stored as a v_vf array of its own
+    (E1, E2, nz + 2G, V) with G = buff_size + 3 ghost planes per side, so
+    the library sweeps it as a block of p_cells = nz - 1.  The x and y
+    sweeps need nothing from the neighbours; the z sweep needs the G planes
+    next to the slab on each side, which exchange() fetches (MFC's halo
+    exchange).  Neighbouring slabs overlap in buff_size cells on each side of
+    a cut (the slab's own ghost layers), whose results both compute; each
+    cell belongs to one rank (owned_cells)."""
+
+    def __init__(self, m: int, n: int, p: int, nv: int, buff: int, world: int, rank: int):
+        self.m, self.n, self.p, self.nv, self.buff = m, n, p, nv, buff
+        self.world, self.rank = world, rank
+        self.z0, self.nz = slab_bounds(p, world, rank)
+        self.G = ghost_planes(buff)
+        if world > 1 and self.nz < self.G:
+            raise ValueError(f"{p + 1} cells over {world} ranks leaves slabs of {self.nz} cells, thinner than "
+                             f"the {self.G} ghost planes each must supply")
+        self.E1 = m + 2 * buff + 7
+        self.E2 = n + 2 * buff + 7
+        self.E3 = self.nz + 2 * self.G
+        self.p_local = self.nz - 1
+
+    def global_planes(self):
+        """[first, last) planes of the global v_vf array that the slab holds
+        (global plane k holds interior cell k - G)."""
+        return self.z0, self.z0 + self.E3
+
+    def exchange(self, v_local, group=None) -> None:
+        exchange_z_ghosts(v_local, self.E1, self.E2, self.nz, self.nv, self.buff, group)
+
+    def owned_cells(self):
+        """[lo, hi) of the slab's z cells, in local indices 0 .. nz + 2 buff
+        (local index k is global cell z0 + k - buff), whose results this rank
+        owns: its nz interior cells, plus the lower ghost cells on the first
+        rank and the upper ones on the last.  The x and y sweeps' face states
+        of a z plane, and the z sweep's of a face (a face is indexed by its
+        cell), belong to the owner of that cell; a neighbour's copy is
+        identical.  (The z sweep writes core faces only: clip to
+        [3, nz + 2 buff - 3).)"""
+        lo = 0 if self.rank == 0 else self.buff
+        hi = self.nz + 2 * self.buff if self.rank == self.world - 1 else self.buff + self.nz
+        return lo, hi
