@@ -535,6 +535,13 @@ struct March64 {
     double b1n, b2n, b2nn;      // beta_1(J+1), beta_2(J+1), beta_2(J+2)
     double e2;                  // curvature d[J+1] - d[J]
     double mA, mB;              // minmod(e2[J-1], e2[J]), minmod(e2[J], e2[J+1])
+    // MP bounds shared by the two states of an interface (f90:1573-1599):
+    // the left state of face J and the right state of face J-1 sit on the
+    // same interface, whose MD bound is one value, and the LC bound of the
+    // right state of face J is that of the left state of face J-1 plus
+    // 2 (v[J] - v[J-1]); both are carried from face J-1.
+    double mdc;                 // MD of face J's left state
+    double lcc;                 // LC of face J-1's left state
 
     // beta of the three stencils that pair (x, y) = (d[k], d[k+1]) enters:
     // stencil 0 of face k, 1 of face k+1, 2 of face k+2 (coefficients of
@@ -570,6 +577,8 @@ struct March64 {
         e2 = dp1 - d0;
         mA = mm64(em, ez);
         mB = mm64(ez, e2);
+        mdc = fma(-0.5, dm1 + mA, v0);
+        lcc = fma(4.0 / 3.0, mA, fma(-0.5, dm1, vm1));
     }
 
     __device__ __forceinline__ void init(const MarchArgs& a, double c0, double c1, double c2, double c3,
@@ -600,11 +609,11 @@ struct March64 {
     // WENO5-JS (+ MP) state of face J; false when the one-reciprocal form
     // is out of range (the caller redoes the face).
     template <bool MPF>
-    __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) const {
+    __device__ __forceinline__ bool face(const MarchArgs& a, double& L, double& R) {
         return face<MPF, ParamCoefs>(a, ParamCoefs{a}, L, R);
     }
     template <bool MPF, class C>
-    __device__ __forceinline__ bool face(const MarchArgs& a, const C& c, double& L, double& R) const {
+    __device__ __forceinline__ bool face(const MarchArgs& a, const C& c, double& L, double& R) {
         const double q0 = b0 * b0, q1 = b1 * b1, q2 = b2 * b2;
         const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
         const double SL = fma(c.dL(0), P0, fma(c.dL(1), P1, c.dL(2) * P2));
@@ -622,34 +631,40 @@ struct March64 {
         const double r = rcp1(p);
         L = fma(EL * SR, r, v0);
         R = fma(ER * SL, r, v0);
-        if constexpr (MPF) {
-            // median(L, lo, hi) with lo <= v0 <= hi: for L >= v0 (E_L >= 0)
-            // it is min(L, hi) and otherwise max(L, lo), so only one bound
-            // is formed, with min/max chosen by that sign.
-            const double kBetaMP = 4.0 / 3.0;
-            const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
-            {
-                const bool pos = sign_clear(EL);
-                const double UL = fma(-2.0, d0, v0);
-                const double MD = fma(-0.5, dm1 + mA, v0);   // ((v0 + vm1) - mA) / 2
-                const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
-                const double P1 = (pos == up_l) ? v0 : vm1;  // max / min of (v0, vm1)
-                const double P2 = (pos == up_r) ? v0 : UL;   // max / min of (v0, UL)
-                const double A = mm_sel(P1, MD, pos), B = mm_sel(P2, LC, pos);
-                L = mm_sel(mm_sel(L, A, !pos), B, !pos);
-            }
-            {
-                const bool pos = sign_clear(ER);
-                const double UL = fma(2.0, dm1, v0);
-                const double MD = fma(0.5, d0 - mB, v0);     // ((v0 + vp1) - mB) / 2
-                const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
-                const double P1 = (pos == up_r) ? vp1 : v0;  // max / min of (v0, vp1)
-                const double P2 = (pos == up_l) ? UL : v0;   // max / min of (v0, UL)
-                const double A = mm_sel(P1, MD, pos), B = mm_sel(P2, LC, pos);
-                R = mm_sel(mm_sel(R, A, !pos), B, !pos);
-            }
-        }
+        if constexpr (MPF) mp_sided(sign_clear(EL), sign_clear(ER), L, R);
         return ok;
+    }
+
+    // MP limiter (f90:1564-1608) of face J's states, one-sided: since
+    // lo <= v0 <= hi, median(L, lo, hi) is min(L, hi) for L >= v0 (pos) and
+    // max(L, lo) otherwise, so only one bound is formed, with min or max
+    // picked by that sign.  The left state's MD and the right state's LC
+    // come from the carried values; the right state's MD and the left
+    // state's LC are carried on to face J+1.
+    __device__ __forceinline__ void mp_sided(bool posL, bool posR, double& L, double& R) {
+        const double kBetaMP = 4.0 / 3.0;
+        const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
+        const double mdR = fma(0.5, d0 - mB, v0);       // ((v0 + vp1) - mB) / 2
+        const double lcL = fma(kBetaMP, mB, fma(-0.5, d0, v0));
+        {
+            const bool pos = posL;
+            const double UL = fma(-2.0, d0, v0);
+            const double P1 = (pos == up_l) ? v0 : vm1;  // max / min of (v0, vm1)
+            const double P2 = (pos == up_r) ? v0 : UL;   // max / min of (v0, UL)
+            const double A = mm_sel(P1, mdc, pos), B = mm_sel(P2, lcL, pos);
+            L = mm_sel(mm_sel(L, A, !pos), B, !pos);
+        }
+        {
+            const bool pos = posR;
+            const double UL = fma(2.0, dm1, v0);
+            const double lcR = fma(2.0, dm1, lcc);       // v0 + (v0 - vm1) / 2 + beta_mp mA
+            const double P1 = (pos == up_r) ? vp1 : v0;  // max / min of (v0, vp1)
+            const double P2 = (pos == up_l) ? UL : v0;   // max / min of (v0, UL)
+            const double A = mm_sel(P1, mdR, pos), B = mm_sel(P2, lcR, pos);
+            R = mm_sel(mm_sel(R, A, !pos), B, !pos);
+        }
+        mdc = mdR;
+        lcc = lcL;
     }
     // WENO5-TENO (+ MP) state of face J (f90:578-606): tau = |beta_2 - beta_0|,
     // alpha_k = (1 + tau / beta_k)^6, delta_k = [alpha_k / sum alpha >= CT],
@@ -657,11 +672,11 @@ struct March64 {
     // E = sum delta_k (kL_k . differences), S = sum delta_k d_k.  False when a
     // sum leaves the range of the reciprocal form (the caller redoes the face).
     template <bool MPF>
-    __device__ __forceinline__ bool face_teno(const MarchArgs& a, double& L, double& R) const {
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, double& L, double& R) {
         return face_teno<MPF, ParamCoefs>(a, ParamCoefs{a}, L, R);
     }
     template <bool MPF, class C>
-    __device__ __forceinline__ bool face_teno(const MarchArgs& a, const C& c, double& L, double& R) const {
+    __device__ __forceinline__ bool face_teno(const MarchArgs& a, const C& c, double& L, double& R) {
         const double tau = fabs(b2 - b0);
         const double t0 = fma(tau, rcp1(b0), 1.0), t1 = fma(tau, rcp1(b1), 1.0), t2 = fma(tau, rcp1(b2), 1.0);
         const double x0 = t0 * t0, x1 = t1 * t1, x2 = t2 * t2;
@@ -688,31 +703,7 @@ struct March64 {
         const double r = rcp1(p);
         L = fma(EL * SR, r, v0);
         R = fma(ER * SL, r, v0);
-        if constexpr (MPF) {
-            // the one-sided MP median of face()
-            const double kBetaMP = 4.0 / 3.0;
-            const bool up_l = sign_clear(dm1), up_r = sign_clear(d0);
-            {
-                const bool pos = sign_clear(EL);
-                const double UL = fma(-2.0, d0, v0);
-                const double MD = fma(-0.5, dm1 + mA, v0);
-                const double LC = fma(kBetaMP, mB, fma(-0.5, d0, v0));
-                const double Q1 = (pos == up_l) ? v0 : vm1;
-                const double Q2 = (pos == up_r) ? v0 : UL;
-                const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
-                L = mm_sel(mm_sel(L, A, !pos), B, !pos);
-            }
-            {
-                const bool pos = sign_clear(ER);
-                const double UL = fma(2.0, dm1, v0);
-                const double MD = fma(0.5, d0 - mB, v0);
-                const double LC = fma(kBetaMP, mA, fma(0.5, dm1, v0));
-                const double Q1 = (pos == up_r) ? vp1 : v0;
-                const double Q2 = (pos == up_l) ? UL : v0;
-                const double A = mm_sel(Q1, MD, pos), B = mm_sel(Q2, LC, pos);
-                R = mm_sel(mm_sel(R, A, !pos), B, !pos);
-            }
-        }
+        if constexpr (MPF) mp_sided(sign_clear(EL), sign_clear(ER), L, R);
         return ok;
     }
 };

@@ -160,6 +160,11 @@ SweepGeom make_geom(const Dims& d, int dir, bool folded) {
     return g;
 }
 
+// SMs a sweep launch sizes its grid and work items for: the whole GPU, or,
+// while a batch captures its graph branches, the branch's share of it
+// (the branches' kernels run side by side).
+thread_local int t_sm_share = 0;
+
 int num_sms() {
     static int sms = 0;
     if (!sms) {
@@ -168,7 +173,7 @@ int num_sms() {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
     }
-    return sms;
+    return t_sm_share > 0 ? std::min(t_sm_share, sms) : sms;
 }
 
 // ----------------------------------------------------------------------
@@ -580,6 +585,8 @@ int batch_enqueue_sweeps(Batch* B, cudaStream_t st) {
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
     std::vector<double> load(nb, 0.0);
     int rc = 0;
+    const int all_sms = num_sms();
+    t_sm_share = nb > 1 ? (all_sms + nb - 1) / nb : 0;
     for (size_t i : order) {
         const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
         load[k] += cost[i];
@@ -596,6 +603,7 @@ int batch_enqueue_sweeps(Batch* B, cudaStream_t st) {
                                  (float*)b.vR, B->br[k], u);
         if (rc) break;
     }
+    t_sm_share = 0;
     // join every branch, also after a failed launch, so a capture ends cleanly
     for (int k = 0; k < nb; ++k) {
         cudaEventRecord(B->join[k], B->br[k]);
