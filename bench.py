@@ -428,6 +428,8 @@ def run_ours(args):
                          "alg_bytes_per_launch": ab, "launch_ms": dk_ms,
                          "traffic": None if (fp32_main or pf_main or M != 199 or ORDER != 5 or SCHEME != "js") else read_traffic()},
             "per_sweep_ms": [s / K for s in sums],
+            "fp64_issue": (fp64_issue_bound(dk_ms, clk.summary().get("sm_mhz"))
+                           if not (fp32_main or pf_main or M != 199 or ORDER != 5 or SCHEME != "js") else None),
             # the per-face form launches the table build and the sweep
             "gpu_launches": (6 if pf_main else 3) * K,
             "clocks": clk.summary(),
@@ -605,20 +607,46 @@ def run_decomp(args):
     return 0
 
 
-def read_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (line 'traffic_bytes_per_launch: <int>'), else None."""
+def read_profile_value(key, kind=int):
+    """A 'key: <number>' line of the committed ncu summary of the headline
+    sweep (profiles/sweep_march_tma_fp64_200cubed.md), else None."""
     p = os.path.join(ROOT, "profiles", "sweep_march_tma_fp64_200cubed.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
-            if line.strip().startswith("traffic_bytes_per_launch:"):
+            if line.strip().startswith(key + ":"):
                 try:
-                    return int(line.split(":", 1)[1].strip().split()[0])
+                    return kind(line.split(":", 1)[1].strip().split()[0])
                 except ValueError:
                     return None
     return None
+
+
+def read_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (line 'traffic_bytes_per_launch: <int>'), else None."""
+    return read_profile_value("traffic_bytes_per_launch", int)
+
+
+def fp64_issue_bound(launch_ms, sm_mhz, sms=148):
+    """The FP64-pipe bound of the headline sweep beside its HBM bound: the
+    FP64 warp-instructions one launch issues (the measured count per warp
+    and face of the committed ncu summary, times the launch's warp-faces:
+    core faces x 32-column tiles x the other cross axis x variables), at
+    half a warp-instruction per cycle per scheduler (4 per SM) and the SM
+    clock seen during the timed region.  None without the summary."""
+    per = read_profile_value("fp64_warp_inst_per_warp_face", float)
+    if per is None or not sm_mhz:
+        return None
+    N = M + 2 * BUFF + 1
+    NC = N - 6
+    tiles = (N + 31) // 32
+    inst = per * NC * tiles * N * NV
+    floor_ms = inst * 2.0 / (sms * 4 * sm_mhz * 1e6) * 1e3
+    return {"fp64_warp_inst_per_launch": inst, "fp64_warp_inst_per_warp_face": per, "sm_mhz": sm_mhz,
+            "floor_ms": floor_ms, "launch_ms": launch_ms, "frac": floor_ms / launch_ms,
+            "rule": "FP64 warp-instructions x 2 cycles / (148 SMs x 4 schedulers x SM clock)"}
 
 
 def measure_fp32_bulk(g, v, faces, outs64, stream, K, dev):
@@ -701,8 +729,10 @@ def measure_drop_in(g, v, faces, outs, stream, K, dev):
 
 def measure_e2e(g, vf_host, coefs, K, dev, full_download=False):
     """End to end through the C-ABI handle API (what a Fortran caller of the
-    harness does): upload v_vf from pinned host memory, x/y/z folded WENO5 +
-    MP, then read the step's result back to the host -- the harness's result
+    harness does): upload v_vf from pinned host memory (weno_sb_upload_async:
+    the sweeps of each variable start once that variable has arrived), x/y/z
+    folded WENO5 + MP, then read the step's result back to the host -- the
+    harness's result
     is its checksum lines (f_checksum of each face-state array, f90:1617-1620,
     1836-1844), so by default the six checksums, summed on the device; with
     full_download the six face-state arrays themselves (3.66 GB) into pinned
@@ -726,7 +756,9 @@ def measure_e2e(g, vf_host, coefs, K, dev, full_download=False):
         lib = L.lib()
 
         def step():
-            L.check(lib.weno_sb_upload(h.handle, L.A_V_VF, src.data_ptr()))
+            # the copy runs one variable at a time and each folded sweep
+            # waits only for its own variable (weno_sb_upload_async)
+            L.check(lib.weno_sb_upload_async(h.handle, L.A_V_VF, src.data_ptr()))
             for d in range(3):
                 L.check(lib.weno_sb_weno(h.handle, d, 5, wsb.F_MP | wsb.F_FOLDED))
             for d in range(3):
@@ -748,7 +780,8 @@ def measure_e2e(g, vf_host, coefs, K, dev, full_download=False):
     out = {"value": fs / dt, "unit": "face-states/s", "h2d_bytes_per_step": int(vf_host.nbytes),
            "d2h_bytes_per_step": int(6 * nface * 8) if full_download else 6 * 8, "ms_per_step": dt * 1e3,
            "steps": K}
-    out["path"] = ("weno_sb_upload -> weno_sb_weno x3 (folded, MP) -> " +
+    out["path"] = ("weno_sb_upload_async (per-variable copies, each sweep waits for its variable) -> "
+                   "weno_sb_weno x3 (folded, MP) -> " +
                    ("weno_sb_download x6 (all face states), pinned host buffers" if full_download else
                     "weno_sb_checksum x6 (the harness's result: f_checksum of every face-state array)"))
     return out

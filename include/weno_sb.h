@@ -128,7 +128,20 @@ int weno_sb_finalize(int handle);
  * (f90:199-203, 1791, 1831).  Synchronous. */
 int weno_sb_upload(int handle, int which, const double *host);
 int weno_sb_download(int handle, int which, double *host);
-/* Device address, element count and storage dtype (WENO_SB_FP64/FP32). */
+/* weno_sb_upload of v_vf without waiting for it -- no counterpart in the
+ * reference, whose `target update to` is synchronous.  The copy runs on a
+ * copy stream of the handle one variable at a time, and the folded sweeps
+ * (weno_sb_weno with WENO_SB_F_FOLDED, orders 3/5/7) launch one variable at
+ * a time, each waiting only for its own variable, so the sweeps of the first
+ * variables run while the later ones are still crossing PCIe.  Every other
+ * call on the handle waits for the whole copy first.  The host buffer must
+ * not change until weno_sb_sync, weno_sb_download or weno_sb_checksum
+ * returns (they wait for the copy); it overlaps nothing unless page-locked
+ * (cudaHostAlloc / cudaHostRegister).  Other arrays, and FP32 handles, take
+ * the synchronous weno_sb_upload. */
+int weno_sb_upload_async(int handle, int which, const double *host);
+/* Device address, element count and storage dtype (WENO_SB_FP64/FP32).
+ * After weno_sb_upload_async, call weno_sb_sync before reading v_vf there. */
 int weno_sb_array_info(int handle, int which, void **dev_ptr, int64_t *n_elem, int *dtype);
 /* s_initialize_weno_{x,y,z} (f90:281-330): reshape v_vf into v_rs_ws_dir. */
 int weno_sb_initialize_weno(int handle, int dir);

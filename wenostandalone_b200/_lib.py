@@ -48,7 +48,7 @@ A_COUNT = 25
 # Every symbol include/weno_sb.h declares.
 EXPORTED = [
     "weno_sb_version", "weno_sb_last_error_string", "weno_sb_extents",
-    "weno_sb_init", "weno_sb_finalize", "weno_sb_upload", "weno_sb_download",
+    "weno_sb_init", "weno_sb_finalize", "weno_sb_upload", "weno_sb_upload_async", "weno_sb_download",
     "weno_sb_array_info", "weno_sb_initialize_weno", "weno_sb_weno",
     "weno_sb_preserve_monotonicity", "weno_sb_vjp", "weno_sb_checksum", "weno_sb_sync",
     "weno_sb_stream", "weno_sb_reshape_dev", "weno_sb_order1_dev",
@@ -119,6 +119,7 @@ def lib() -> ctypes.CDLL:
         "weno_sb_init": ([gp, i32, ctypes.POINTER(ctypes.c_int)], i32),
         "weno_sb_finalize": ([i32], i32),
         "weno_sb_upload": ([i32, i32, vp], i32),
+        "weno_sb_upload_async": ([i32, i32, vp], i32),
         "weno_sb_download": ([i32, i32, vp], i32),
         "weno_sb_array_info": ([i32, i32, ctypes.POINTER(ctypes.c_void_p), i64p, ctypes.POINTER(ctypes.c_int)], i32),
         "weno_sb_initialize_weno": ([i32, i32], i32),

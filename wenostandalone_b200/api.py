@@ -103,6 +103,16 @@ class Harness:
         assert a.shape == tuple(self.shape_of(which)), (a.shape, self.shape_of(which))
         check(lib().weno_sb_upload(self.handle, which, a.ctypes.data))
 
+    def upload_async(self, which: int, host) -> None:
+        """weno_sb_upload_async from `host` (a page-locked CPU torch tensor
+        or a numpy array in the array's Fortran order), kept referenced until
+        the next upload: the folded sweeps overlap the copy."""
+        if not hasattr(host, "data_ptr"):
+            host = np.asfortranarray(host, dtype=np.float64)
+        self._pending = host
+        ptr = host.data_ptr() if hasattr(host, "data_ptr") else host.ctypes.data
+        check(lib().weno_sb_upload_async(self.handle, which, ptr))
+
     def download(self, which: int) -> np.ndarray:
         out = np.empty(self.shape_of(which), order="F")
         check(lib().weno_sb_download(self.handle, which, out.ctypes.data))

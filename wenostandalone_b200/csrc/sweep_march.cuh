@@ -577,7 +577,9 @@ struct March64 {
         e2 = dp1 - d0;
         mA = mm64(em, ez);
         mB = mm64(ez, e2);
-        mdc = fma(-0.5, dm1 + mA, v0);
+        // the bounds face J-1 would have carried, by the same expressions, so
+        // a face's result does not depend on where its segment starts
+        mdc = fma(0.5, dm1 - mA, vm1);
         lcc = fma(4.0 / 3.0, mA, fma(-0.5, dm1, vm1));
     }
 

@@ -674,7 +674,22 @@ struct Handle {
     // take them from kernel parameters), and face 0's values.
     bool coef_uniform[3][5] = {};
     weno_sb_face_coefs face0[3] = {};
+    // weno_sb_upload_async of v_vf: the copy runs on copy_stream one
+    // variable at a time, var_ready[q] recorded after variable q; while
+    // vf_pending, folded sweeps wait per variable and every other use of the
+    // handle waits for all of them (await_vf)
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> var_ready;
+    cudaEvent_t main_done = nullptr;
+    bool vf_pending = false;
 };
+
+// Make the handle's stream wait for an asynchronous upload of v_vf.
+void await_vf(Handle* H) {
+    if (!H->vf_pending) return;
+    for (cudaEvent_t e : H->var_ready) cudaStreamWaitEvent(H->stream, e, 0);
+    H->vf_pending = false;
+}
 
 std::mutex g_mu;
 std::vector<Handle*> g_handles;
@@ -715,9 +730,13 @@ void note_coefficients(Handle* H, int which, const double* host) {
 }
 
 void free_handle_arrays(Handle* H) {
+    if (H->copy_stream) cudaStreamSynchronize(H->copy_stream);
     for (int i = 0; i < WENO_SB_A_COUNT; ++i)
         if (H->arr[i]) cudaFree(H->arr[i]);
     if (H->sum_scratch) cudaFree(H->sum_scratch);
+    for (cudaEvent_t e : H->var_ready) cudaEventDestroy(e);
+    if (H->main_done) cudaEventDestroy(H->main_done);
+    if (H->copy_stream) cudaStreamDestroy(H->copy_stream);
     if (H->stream) cudaStreamDestroy(H->stream);
 }
 
@@ -810,6 +829,7 @@ int weno_sb_finalize(int handle) {
 int weno_sb_array_info(int handle, int which, void** dev_ptr, int64_t* n_elem, int* dtype) {
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    await_vf(H);
     if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
     if (dev_ptr) *dev_ptr = H->arr[which];
     // the caller may now write the array directly: stop trusting the
@@ -827,6 +847,7 @@ int weno_sb_upload(int handle, int which, const double* host) {
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
     if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
     if (!host) return set_err(WENO_SB_ERR_ARG, "host pointer is NULL");
+    await_vf(H);
     const long long n = H->n[which];
     if (which >= WENO_SB_A_POLYL(0)) note_coefficients(H, which, host);
     if (H->dtype[which] == WENO_SB_FP64) {
@@ -846,6 +867,7 @@ int weno_sb_download(int handle, int which, double* host) {
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
     if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
     if (!host) return set_err(WENO_SB_ERR_ARG, "host pointer is NULL");
+    await_vf(H);
     const long long n = H->n[which];
     if (H->dtype[which] == WENO_SB_FP64) {
         WSB_CUDA(cudaMemcpyAsync(host, H->arr[which], sizeof(double) * n, cudaMemcpyDeviceToHost, H->stream));
@@ -861,7 +883,38 @@ int weno_sb_download(int handle, int which, double* host) {
 int weno_sb_stream(int handle, void** stream) {
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    await_vf(H);
     if (stream) *stream = (void*)H->stream;
+    return WENO_SB_OK;
+}
+
+int weno_sb_upload_async(int handle, int which, const double* host) {
+    WSB_FAULT("upload");
+    Handle* H = get_handle(handle);
+    if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
+    if (!host) return set_err(WENO_SB_ERR_ARG, "host pointer is NULL");
+    // only v_vf of an FP64 handle is pipelined; the rest is weno_sb_upload
+    if (which != WENO_SB_A_V_VF || H->dtype[which] != WENO_SB_FP64) return weno_sb_upload(handle, which, host);
+    const int nv = H->dims.nv;
+    if (!H->copy_stream) {
+        WSB_CUDA(cudaStreamCreateWithFlags(&H->copy_stream, cudaStreamNonBlocking));
+        WSB_CUDA(cudaEventCreateWithFlags(&H->main_done, cudaEventDisableTiming));
+        H->var_ready.resize(nv, nullptr);
+        for (int q = 0; q < nv; ++q) WSB_CUDA(cudaEventCreateWithFlags(&H->var_ready[q], cudaEventDisableTiming));
+    }
+    await_vf(H);
+    // the new copy must not overwrite v_vf while earlier work still reads it
+    WSB_CUDA(cudaEventRecord(H->main_done, H->stream));
+    WSB_CUDA(cudaStreamWaitEvent(H->copy_stream, H->main_done, 0));
+    const long long per = H->n[which] / nv;
+    double* dst = (double*)H->arr[which];
+    for (int q = 0; q < nv; ++q) {
+        WSB_CUDA(cudaMemcpyAsync(dst + per * q, host + per * q, sizeof(double) * per, cudaMemcpyHostToDevice,
+                                 H->copy_stream));
+        WSB_CUDA(cudaEventRecord(H->var_ready[q], H->copy_stream));
+    }
+    H->vf_pending = true;
     return WENO_SB_OK;
 }
 
@@ -869,6 +922,7 @@ int weno_sb_sync(int handle) {
     WSB_FAULT("sync");
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    await_vf(H);
     int rc = cuda_err(cudaStreamSynchronize(H->stream), "cudaStreamSynchronize");
     if (rc) return rc;
     return weno_sb_check_device(H->stream);
@@ -1025,6 +1079,7 @@ int weno_sb_checksum_dev(int dtype, const void* arr, int64_t n, void* scratch, d
 int weno_sb_initialize_weno(int handle, int dir) {
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    await_vf(H);
     int rc = check_dir(dir);
     if (rc) return rc;
     return weno_sb_reshape_dev(&H->grid, dir, H->precision, (const double*)H->arr[WENO_SB_A_V_VF],
@@ -1036,15 +1091,38 @@ int weno_sb_weno(int handle, int dir, int order, unsigned flags) {
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
     int rc = check_dir(dir);
     if (rc) return rc;
+    const bool folded = (flags & WENO_SB_F_FOLDED) != 0;
+    if (H->vf_pending && (order == 1 || !folded || (order != 3 && order != 5 && order != 7))) await_vf(H);
     if (order == 1)
         return weno_sb_order1_dev(&H->grid, dir, H->precision, (const double*)H->arr[WENO_SB_A_V_VF],
                                   H->arr[WENO_SB_A_VL(dir)], H->arr[WENO_SB_A_VR(dir)], H->stream);
     weno_sb_coefs cf{(const double*)H->arr[WENO_SB_A_POLYL(dir)], (const double*)H->arr[WENO_SB_A_POLYR(dir)],
                      (const double*)H->arr[WENO_SB_A_DL(dir)], (const double*)H->arr[WENO_SB_A_DR(dir)],
                      (const double*)H->arr[WENO_SB_A_BETA(dir)]};
-    const void* in = (flags & WENO_SB_F_FOLDED) ? H->arr[WENO_SB_A_V_VF] : H->arr[WENO_SB_A_RS(dir)];
+    const void* in = folded ? H->arr[WENO_SB_A_V_VF] : H->arr[WENO_SB_A_RS(dir)];
     bool uni = true;
     for (int k = 0; k < 5; ++k) uni = uni && H->coef_uniform[dir][k];
+    if (H->vf_pending) {
+        // v_vf is still arriving: one sweep per variable, each after its
+        // variable's copy (the variables of v_vf and of the face states are
+        // contiguous blocks, so a variable is a block of v_size 1)
+        weno_sb_grid g1 = H->grid;
+        g1.v_size = 1;
+        const long long per_in = H->n[WENO_SB_A_V_VF] / H->dims.nv;
+        const long long per_out = H->n[WENO_SB_A_VL(dir)] / H->dims.nv;
+        for (int q = 0; q < H->dims.nv; ++q) {
+            WSB_CUDA(cudaStreamWaitEvent(H->stream, H->var_ready[q], 0));
+            const double* inq = (const double*)in + per_in * q;
+            double* Lq = (double*)H->arr[WENO_SB_A_VL(dir)] + per_out * q;
+            double* Rq = (double*)H->arr[WENO_SB_A_VR(dir)] + per_out * q;
+            rc = (uni && getenv("WENO_SB_PER_FACE") == nullptr)
+                     ? weno_sb_weno_uniform_dev(&g1, dir, order, flags, WENO_SB_FP64, inq, &H->face0[dir], Lq, Rq,
+                                                H->stream)
+                     : weno_sb_weno_dev(&g1, dir, order, flags, WENO_SB_FP64, inq, &cf, Lq, Rq, H->stream);
+            if (rc) return rc;
+        }
+        return WENO_SB_OK;
+    }
     if (uni && getenv("WENO_SB_PER_FACE") == nullptr)
         return weno_sb_weno_uniform_dev(&H->grid, dir, order, flags, H->precision, in, &H->face0[dir],
                                         H->arr[WENO_SB_A_VL(dir)], H->arr[WENO_SB_A_VR(dir)], H->stream);
@@ -1055,6 +1133,7 @@ int weno_sb_weno(int handle, int dir, int order, unsigned flags) {
 int weno_sb_vjp(int handle, int dir, int order, unsigned flags, const double* gL, const double* gR, double* gv) {
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    await_vf(H);
     int rc = check_dir(dir);
     if (rc) return rc;
     if (H->precision != WENO_SB_FP64) return set_err(WENO_SB_ERR_UNSUPPORTED, "the adjoint is FP64 (FP32-bulk handle)");
@@ -1082,6 +1161,7 @@ int weno_sb_preserve_monotonicity(int handle, int dir) {
 int weno_sb_checksum(int handle, int which, double* result) {
     Handle* H = get_handle(handle);
     if (!H) return set_err(WENO_SB_ERR_HANDLE, "unknown handle %d", handle);
+    await_vf(H);
     if (which < 0 || which >= WENO_SB_A_COUNT) return set_err(WENO_SB_ERR_ARG, "unknown array id %d", which);
     if (!result) return set_err(WENO_SB_ERR_ARG, "result pointer is NULL");
     int rc = weno_sb_checksum_dev(H->dtype[which], H->arr[which], H->n[which], H->sum_scratch,

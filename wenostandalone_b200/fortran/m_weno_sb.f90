@@ -77,6 +77,14 @@ module m_weno_sb
             type(c_ptr), value :: host
         end function weno_sb_upload
 
+        !> v_vf without waiting: the folded sweeps overlap the copy; keep the
+        !! (page-locked) host buffer unchanged until weno_sb_sync
+        integer(c_int) function weno_sb_upload_async(handle, which, host) bind(C, name='weno_sb_upload_async')
+            import :: c_int, c_ptr
+            integer(c_int), value :: handle, which
+            type(c_ptr), value :: host
+        end function weno_sb_upload_async
+
         integer(c_int) function weno_sb_download(handle, which, host) bind(C, name='weno_sb_download')
             import :: c_int, c_ptr
             integer(c_int), value :: handle, which
