@@ -858,9 +858,10 @@ def _batch_blocks(n_blocks=96, seed=96):
 def measure_batched(dev, K):
     """96 uneven blocks (x/y/z sweeps each, MP fused, folded input) as one
     CUDA graph launch, run the way the autotuner picks (one persistent
-    kernel over all blocks, or per-block specialised sweeps on parallel
-    graph branches), FP64 and FP32-bulk; the other way and, FP64, one
-    launch per sweep for comparison."""
+    kernel over all blocks; per-block specialised sweeps on parallel graph
+    branches; or grouped TMA marching sweeps, one launch per kernel
+    instance over all its blocks), FP64 and FP32-bulk; the other ways and,
+    FP64, one launch per sweep for comparison."""
     import torch
 
     import wenostandalone_b200 as wsb
@@ -891,21 +892,22 @@ def measure_batched(dev, K):
         b = api.Batch(entries)
         try:
             t, u, tune_ms = b.autotune(stream=sp)
-            mode, _, _, nb = b.query()
+            mode, _, per_item, nb = b.query()
             ms = _time_steps(lambda: b.launch(stream=sp), stream, K)
-            # the other way of running the batch, at its default layout
+            # the other ways of running the batch, at their default layouts
             other = {}
-            if mode == 1:
-                b.configure(0, 128, 8, nb)
-                other["persistent_kernel_ms"] = _time_steps(lambda: b.launch(stream=sp), stream, K)
-            else:
-                b.configure(1, t, u, 8)
-                other["graph_of_sweeps_8_branches_ms"] = _time_steps(lambda: b.launch(stream=sp), stream, K)
+            for m_o, cfg, key in ((0, (0, 128, 8, 8), "persistent_kernel_ms"),
+                                  (1, (1, 128, 8, 8), "graph_of_sweeps_8_branches_ms"),
+                                  (2, (2, 128, 64, 2), "grouped_sweeps_64_faces_2_branches_ms")):
+                if m_o != mode:
+                    b.configure(*cfg)
+                    other[key] = _time_steps(lambda: b.launch(stream=sp), stream, K)
         finally:
             b.close()
-        r = {"ms_per_step": ms, "value": fs / (ms * 1e-3), "face_states": fs,
-             "choice": ({"mode": "graph of specialised sweeps", "branches": nb} if mode == 1 else
-                        {"mode": "persistent kernel", "threads": t, "cols": u}),
+        choice = {0: {"mode": "persistent kernel", "threads": t, "cols": u},
+                  1: {"mode": "graph of specialised sweeps", "branches": nb},
+                  2: {"mode": "grouped TMA marching sweeps", "faces_per_item": per_item, "branches": nb}}[mode]
+        r = {"ms_per_step": ms, "value": fs / (ms * 1e-3), "face_states": fs, "choice": choice,
              "graph_launches_per_step": 1, **other}
         if dt == torch.float64:
             structs = [api.coefs_struct(e["coefs"]) for e in entries]
@@ -926,7 +928,7 @@ def measure_families(g, v, stream, K, dev):
     """Every kernel family of the path at 200^3 x 8 (FP64, x/y/z each):
     reshape (s_initialize_weno), order-1 copy, WENO3 / WENO5 / WENO7 with
     JS weights and MP fused, the standalone MP limiter, and WENO5 with TENO
-    weights (teno_CT 1e-5).  True uniform-grid coefficients go through the
+    (teno_CT 1e-5), mapped and Z weights.  True uniform-grid coefficients go through the
     face-independent entry (weno_sb_weno_uniform_dev, which the handle API
     also takes when its coefficient banks are uniform); the harness's
     coefficient arrays (s_fill_coefficients) through the per-face entry
@@ -972,6 +974,10 @@ def measure_families(g, v, stream, K, dev):
     fc5 = [face(5, d) for d in range(3)]
     timed("weno5_teno_mp", lambda: [
         api.weno_uniform(gt, d, 5, v, fc5[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
+    for name, scheme in (("weno5_mapped_mp", wsb.MAPPED), ("weno5_z_mp", wsb.Z)):
+        gs = wsb.Grid(M, M, M, NV, BUFF, scheme=scheme)
+        timed(name, lambda gs=gs: [
+            api.weno_uniform(gs, d, 5, v, fc5[d], L, R, flags=wsb.F_MP | wsb.F_FOLDED, stream=sp) for d in range(3)])
     res["note"] = ("value = face-states/s of the WENO5 face count (3 x 148,135,424) for every family, so "
                    "the rows compare as times; WENO3 writes all ns faces")
     return res

@@ -255,7 +255,7 @@ int weno_sb_coefficients(int order, int64_t ns, const double *x_cb, double *poly
 
 /* ===================================================================== */
 /* Batches of uneven blocks (no counterpart in the reference, which runs   */
-/* one block): one persistent launch, captured in a CUDA graph.            */
+/* one block): one CUDA graph launch of all the blocks' sweeps.            */
 /* ===================================================================== */
 typedef struct weno_sb_block {
     weno_sb_grid grid;     /* this block's extents, v_size and weights      */
@@ -276,14 +276,22 @@ typedef struct weno_sb_block {
 int weno_sb_batch_create(const weno_sb_block *blocks, int n, int *batch);
 /* Time the ways of running the batch on `stream` and keep the fastest:
  * mode 0, one persistent kernel over all blocks (candidate tile shapes:
- * CTA width x columns per work item), and mode 1, every block's sweep by
- * the sweep kernel specialised for it, spread over 1..16 parallel branches
- * of the graph (candidate branch counts).  With WENO_SB_TUNE_CACHE naming a
- * file, a batch of the same composition reuses the recorded choice.
+ * CTA width x columns per work item); mode 1, every block's sweep by the
+ * sweep kernel specialised for it, spread over 1..16 parallel branches of
+ * the graph (candidate branch counts); mode 2, the blocks with
+ * face-independent coefficients that a marching engine covers grouped by
+ * kernel and coefficients, one TMA marching launch per group over all its
+ * blocks' work items (candidate faces per work item and branch counts),
+ * the other blocks as in mode 1.  With WENO_SB_TUNE_CACHE naming a file, a
+ * batch of the same composition reuses the recorded choice.
  * threads / cols_per_item report the persistent layout. */
 int weno_sb_batch_autotune(int batch, void *stream, int *threads, int *cols_per_item, double *best_ms);
 /* Choose the way explicitly: mode 0 with threads (64/128/256) and
- * cols_per_item (1..64), or mode 1 with branches (1..16). */
+ * cols_per_item (1..64); mode 1 with branches (1..16); or mode 2 (grouped
+ * marching sweeps: one launch per group of blocks with the same kernel and
+ * coefficients) with cols_per_item = faces per work item (8..4096) and
+ * branches (1..16).  weno_sb_batch_query reports the faces per work item
+ * in cols_per_item for mode 2. */
 int weno_sb_batch_configure(int batch, int mode, int threads, int cols_per_item, int branches);
 /* The current choice (any pointer may be NULL). */
 int weno_sb_batch_query(int batch, int *mode, int *threads, int *cols_per_item, int *branches);

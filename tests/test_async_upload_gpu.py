@@ -12,7 +12,7 @@ from gpu_util import rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _run(h, L, field, asynchronous, dirs=(0, 1, 2), flags=None):
+def _run(h, L, field, asynchronous, dirs=(0, 1, 2), flags=None, reshape=False):
     import torch
     import wenostandalone_b200 as wsb
     fl = (wsb.F_MP | wsb.F_FOLDED) if flags is None else flags
@@ -22,6 +22,8 @@ def _run(h, L, field, asynchronous, dirs=(0, 1, 2), flags=None):
     else:
         h.upload(L.A_V_VF, field)
     for d in dirs:
+        if reshape:
+            h.s_initialize_weno(d)
         h.weno(d, 5, fl)
     out = [(h.download(L.A_VL(d)), h.download(L.A_VR(d))) for d in dirs]
     sums = [h.checksum(L.A_VL(d)) + h.checksum(L.A_VR(d)) for d in dirs]
@@ -106,8 +108,10 @@ def test_fp32_handle_takes_the_synchronous_upload():
     with wsb.Harness(g, precision=L.FP32) as h:
         for d in range(3):
             h.upload_coefficients(d, fields.uniform_weno_coefficients(5, g.nc(d)))
-        ref, s_ref = _run(h, L, f, False)
-        got, s_got = _run(h, L, f, True)
+        # (FP32 handles sweep the reshaped FP32 copies: the folded form
+        # reads the FP64 v_vf)
+        ref, s_ref = _run(h, L, f, False, flags=wsb.F_MP, reshape=True)
+        got, s_got = _run(h, L, f, True, flags=wsb.F_MP, reshape=True)
         for (a, b), (c, e) in zip(got, ref):
             assert np.array_equal(a, c) and np.array_equal(b, e)
         assert s_got == s_ref

@@ -84,8 +84,9 @@ def _relaunch_and_check(b, entries, checks):
 
 @pytest.mark.parametrize("coefficients", ["varying", "uniform"])
 def test_batch_matches_oracle_per_block(oracle_mod, coefficients):
-    """Both ways of running a batch -- the persistent kernel (two tile
-    shapes) and the graph of per-block sweeps (1, 3 and 16 branches) --
+    """Every way of running a batch -- the persistent kernel (two tile
+    shapes), the graph of per-block sweeps (1, 3 and 16 branches) and the
+    grouped sweeps (8 to 4096 faces per work item, 1 to 3 branches) --
     then the autotuner's choice."""
     import wenostandalone_b200 as wsb
     from wenostandalone_b200 import api
@@ -93,14 +94,21 @@ def test_batch_matches_oracle_per_block(oracle_mod, coefficients):
     b = api.Batch(entries)
     try:
         _relaunch_and_check(b, entries, checks)          # the default choice
-        for cfg in ((0, 128, 8, 8), (0, 64, 32, 8), (1, 128, 8, 1), (1, 128, 8, 3), (1, 128, 8, 16)):
+        for cfg in ((0, 128, 8, 8), (0, 64, 32, 8), (1, 128, 8, 1), (1, 128, 8, 3), (1, 128, 8, 16),
+                    (2, 128, 8, 1), (2, 128, 64, 3), (2, 128, 4096, 2)):
             b.configure(*cfg)
-            assert b.query() == cfg if cfg[0] == 0 else b.query()[0::3] == (1, cfg[3])
+            q = b.query()
+            if cfg[0] == 0:
+                assert q == cfg
+            elif cfg[0] == 1:
+                assert q[0::3] == (1, cfg[3])
+            else:
+                assert (q[0], q[2], q[3]) == (2, cfg[2], cfg[3])
             _relaunch_and_check(b, entries, checks)
         t, u, ms = b.autotune()
         assert t in (64, 128, 256) and u in (4, 8, 16, 32) and ms > 0
         mode, _, _, nb = b.query()
-        assert mode in (0, 1) and 1 <= nb <= 16
+        assert mode in (0, 1, 2) and 1 <= nb <= 16
         _relaunch_and_check(b, entries, checks)
     finally:
         b.close()
@@ -112,7 +120,8 @@ def test_batch_configure_rejects_bad_choices(oracle_mod):
     entries, _ = _make_blocks(wsb, oracle_mod, n_blocks=2)
     b = api.Batch(entries)
     try:
-        for cfg in ((2, 128, 8, 8), (0, 96, 8, 8), (0, 128, 0, 8), (1, 128, 8, 0), (1, 128, 8, 17)):
+        for cfg in ((3, 128, 8, 8), (-1, 128, 8, 8), (0, 96, 8, 8), (0, 128, 0, 8), (1, 128, 8, 0),
+                    (1, 128, 8, 17), (2, 128, 7, 4), (2, 128, 4097, 4), (2, 128, 64, 0)):
             with pytest.raises(L.WenoError) as e:
                 b.configure(*cfg)
             assert e.value.code == L.ERR_ARG
@@ -128,3 +137,49 @@ def test_batch_rejects_bad_blocks(oracle_mod):
     with pytest.raises(L.WenoError) as e:
         api.Batch(entries)
     assert e.value.code == L.ERR_ARG and "block 1" in L.last_error()
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_grouped_sweeps_mixed_layouts(oracle_mod, fp32):
+    """Grouped sweeps whose entries differ in every per-entry property: odd
+    and even extents (field rows loaded by TMA or per lane, face rows
+    stored by TMA or with plain stores), x / y / z sweeps (row and column
+    tiles), folded and drop-in inputs, and 8-face work items, so each warp
+    runs many items of different entries in turn.  Against the oracle:
+    FP64 1e-12, FP32-bulk 1e-5 on the FP32-rounded field."""
+    import torch
+    import wenostandalone_b200 as wsb
+    from wenostandalone_b200 import api, fields
+    rng = np.random.default_rng(77 if fp32 else 76)
+    dt = torch.float32 if fp32 else torch.float64
+    entries, checks = [], []
+    for i in range(18):
+        m, n, p = (int(x) - 1 for x in rng.integers(24, 47, 3))
+        nv = int(rng.choice([3, 5]))
+        order, scheme = [(5, 0), (5, 3), (7, 0), (3, 0)][i % 4]
+        folded = i % 3 != 2
+        d = i % 3
+        g = wsb.Grid(m, n, p, nv, 6, scheme=scheme)
+        vf = fields.smooth_jump_field(m, n, p, nv, 6, seed=300 + i)
+        if fp32:
+            vf = vf.astype(np.float32).astype(np.float64)
+        coefs = fields.uniform_weno_coefficients(order, g.nc(d))
+        rs = oracle_mod.reshape(np.asfortranarray(vf), m, n, p, 6, d)
+        Lr, Rr = oracle_mod.order1_copy(np.asfortranarray(vf), m, n, p, 6, d)
+        Lr[:] = np.nan
+        Rr[:] = np.nan
+        oracle_mod.reconstruct(rs, coefs, order, scheme=scheme, vL=Lr, vR=Rr)
+        oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+        v_in = to_dev(vf if folded else rs, dt)
+        L, R = nan_dev(g.face_shape(d), dt), nan_dev(g.face_shape(d), dt)
+        entries.append(dict(grid=g, dir=d, order=order, flags=wsb.F_MP | (wsb.F_FOLDED if folded else 0),
+                            v_in=v_in, coefs=tuple(to_dev(c) for c in coefs), vL=L, vR=R))
+        mg = oracle_mod.teno_margin(rs, coefs, order) if scheme == 3 else None
+        checks.append((g, d, scheme, fp32, Lr, Rr, mg))
+    b = api.Batch(entries)
+    try:
+        for cfg in ((2, 128, 8, 1), (2, 128, 16, 4), (2, 128, 64, 2)):
+            b.configure(*cfg)
+            _relaunch_and_check(b, entries, checks)
+    finally:
+        b.close()

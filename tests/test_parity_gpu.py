@@ -155,7 +155,7 @@ def _check(Lg, Rg, Lr, Rr, scheme, what, margin=None):
 @pytest.mark.parametrize("kernel", ["auto", "march", "tma", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
-@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3), (7, 3)])
+@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 2), (5, 3), (7, 3)])
 def test_face_varying_coefficients(wsb, oracle_mod, order, scheme, folded, mp, kernel):
     """Every face has its own coefficients: catches a kernel that reads
     another face's (or one shared) coefficient set.  WENO5 / WENO7 with TENO
@@ -183,10 +183,12 @@ def test_stretched_grid_coefficients(wsb, oracle_mod, order, scheme, folded, mp)
 @pytest.mark.parametrize("kernel", ["auto", "march", "march_ldg", "tma", "cpasync", "generic"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
-@pytest.mark.parametrize("scheme", [0, 3])
+@pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("order", [3, 5, 7])
 def test_uniform_entry_parity(wsb, oracle_mod, order, scheme, folded, mp, kernel):
-    """weno_sb_weno_uniform_dev: face-independent coefficients given on the host."""
+    """weno_sb_weno_uniform_dev: face-independent coefficients given on the
+    host (FP64 WENO5 mapped / Z weights: the marching engine's face_mapped /
+    face_z)."""
     for dims in GRIDS:
         for d in range(3):
             Lg, Rg, Lr, Rr, mg = _run_case(wsb, oracle_mod, dims, d, order, scheme, folded, mp, kernel, "uniform",
@@ -195,7 +197,7 @@ def test_uniform_entry_parity(wsb, oracle_mod, order, scheme, folded, mp, kernel
 
 
 @pytest.mark.parametrize("order", [5, 7])
-@pytest.mark.parametrize("scheme", [0, 3])
+@pytest.mark.parametrize("scheme", [0, 2, 3])
 @pytest.mark.parametrize("kind", ["negative", "negative_uniform"])
 @pytest.mark.parametrize("mp", [False, True])
 @pytest.mark.parametrize("folded", [False, True])
@@ -437,10 +439,11 @@ def test_full_size_teno_mp(wsb, oracle_mod, order, entry):
     assert flips == 0
 
 
-@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 3), (7, 3)])
+@pytest.mark.parametrize("order,scheme", [(3, 0), (5, 0), (7, 0), (5, 1), (5, 2), (5, 3), (7, 3)])
 def test_mid_size_uniform_entry(wsb, oracle_mod, order, scheme):
     """96^3 x 4 (several segments per column, every tile shape), WENO3 / WENO5 /
-    WENO7 with JS and WENO5 / WENO7 with TENO weights, + MP, through the face-independent entry, drop-in and
+    WENO7 with JS, WENO5 with mapped and Z and WENO5 / WENO7 with TENO
+    weights, + MP, through the face-independent entry, drop-in and
     folded, against the oracle at 1e-12 per array (TENO: an entry past that
     must sit on a face whose omega is within rounding of the cutoff)."""
     import torch
@@ -466,6 +469,35 @@ def test_mid_size_uniform_entry(wsb, oracle_mod, order, scheme):
             Lg, Rg = from_dev(L, g.face_shape(d)), from_dev(R, g.face_shape(d))
             mg = oracle_mod.teno_margin(rs, coefs, order) if scheme == 3 else None
             _check(Lg, Rg, Lr, Rr, scheme, (d, folded), mg)
+
+
+@pytest.mark.parametrize("folded", [False, True])
+def test_mapped_weights_outside_the_engines_range(wsb, oracle_mod, folded):
+    """Mapped WENO5 with an ideal weight of 0.85 (face-independent entry):
+    outside (0, 0.8) a mapped weight can change sign, which the marching
+    engine's one-sided MP median cannot take, so another kernel runs; the
+    results match the oracle."""
+    from wenostandalone_b200 import api, fields
+    m, n, p, nv = 23, 23, 23, 3
+    g = wsb.Grid(m, n, p, nv, 6, scheme=1)
+    vf = _field(m, n, p, nv)
+    v = to_dev(vf)
+    for d in range(3):
+        coefs = fields.uniform_weno_coefficients(5, g.nc(d))
+        coefs[2][:3, :] = np.array([0.05, 0.85, 0.10])[:, None]
+        coefs[3][:3, :] = np.array([0.10, 0.85, 0.05])[:, None]
+        rs = oracle_mod.reshape(vf, m, n, p, 6, d)
+        Lr, Rr = oracle_mod.order1_copy(vf, m, n, p, 6, d)
+        oracle_mod.reconstruct(rs, coefs, 5, scheme=1, vL=Lr, vR=Rr)
+        oracle_mod.preserve_monotonicity(rs, Lr, Rr)
+        L, R = nan_dev(g.face_shape(d)), nan_dev(g.face_shape(d))
+        api.order1_copy(g, d, v, L, R)
+        src = v
+        if not folded:
+            src = nan_dev(g.rs_shape(d))
+            api.reshape(g, d, v, src)
+        api.weno_uniform(g, d, 5, src, coefs, L, R, flags=wsb.F_MP | (wsb.F_FOLDED if folded else 0))
+        _check(from_dev(L, g.face_shape(d)), from_dev(R, g.face_shape(d)), Lr, Rr, 1, (d, folded))
 
 
 def test_argument_errors(wsb):

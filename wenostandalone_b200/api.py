@@ -381,7 +381,10 @@ class Batch:
 
     def configure(self, mode: int, threads: int = 128, cols_per_item: int = 8, branches: int = 8):
         """mode 0: one persistent kernel (threads x cols_per_item work items);
-        mode 1: a graph of per-block specialised sweeps on `branches` branches."""
+        mode 1: a graph of per-block specialised sweeps on `branches` branches;
+        mode 2: grouped TMA marching sweeps (one launch per kernel instance and
+        coefficient set, cols_per_item = faces per work item, 8..4096) on
+        `branches` branches, the blocks no group takes as in mode 1."""
         check(lib().weno_sb_batch_configure(self.handle, mode, threads, cols_per_item, branches))
 
     def query(self):

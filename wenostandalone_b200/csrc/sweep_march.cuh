@@ -63,6 +63,9 @@ struct MarchArgs {
     double kL7[12], kR7[12];
     // FP32-bulk WENO7 engine: float polyL[0..11], polyR[0..11] (Coef<7> order)
     float pf7[24];
+    // mapped WENO5 engine: per stencil k, (d + d^2, 3 d, 1 - 2 d, d^2) of the
+    // left / right ideal weights at 4k .. 4k + 3
+    double mcL[12], mcR[12];
     // face-dependent coefficients (FP64 kernels): the per-face table built by
     // march_face_table_kernel, and the arrays it was built from (for faces
     // that are redone); ftab is null for face-independent coefficients
@@ -618,6 +621,72 @@ struct March64 {
     __device__ __forceinline__ bool face(const MarchArgs& a, const C& c, double& L, double& R) {
         const double q0 = b0 * b0, q1 = b1 * b1, q2 = b2 * b2;
         const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+        return fold<MPF>(c, P0, P1, P2, L, R);
+    }
+    // WENO5-Z (+ MP) state of face J (f90:586-590): tau = |beta_2 - beta_0|,
+    // alpha_k = d_k (1 + tau / beta_k).  Times beta_0 beta_1 beta_2 the
+    // weights are d_k P_k / sum d P with P_k = (beta_k + tau) prod_{j != k}
+    // beta_j: the folded form of JS with these P_k.
+    template <bool MPF>
+    __device__ __forceinline__ bool face_z(const MarchArgs& a, double& L, double& R) {
+        return face_z<MPF, ParamCoefs>(a, ParamCoefs{a}, L, R);
+    }
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool face_z(const MarchArgs& a, const C& c, double& L, double& R) {
+        const double tau = fabs(b2 - b0);
+        const double P0 = (b0 + tau) * (b1 * b2), P1 = (b1 + tau) * (b0 * b2), P2 = (b2 + tau) * (b0 * b1);
+        return fold<MPF>(c, P0, P1, P2, L, R);
+    }
+    // Mapped WENO5 (+ MP) state of face J (f90:557-568; Henrick, Aslam and
+    // Powers, J. Comput. Phys. 207 (2005)): per side, with its own ideal
+    // weights d_k, omega_k = d_k P_k / sum d P (the JS weights, P_k =
+    // prod_{j != k} beta_j^2), N_k = d_k (1 + d_k - 3 omega_k) + omega_k^2,
+    // D_k = d_k^2 + omega_k (1 - 2 d_k), mapped weights omega_k N_k / D_k
+    // normalised.  Folded over the denominators, G_k = omega_k N_k prod_{j !=
+    // k} D_j and the state is v0 + sum G_k e_k / sum G_k, e_k the candidate
+    // offsets with the raw coefficients.  Face-independent coefficients
+    // (the per-side constants d + d^2, 3 d, 1 - 2 d, d^2 in MarchArgs::mcL /
+    // mcR); the ideal weights must lie in (0, 0.8), where every G_k >= 0, so
+    // the offset's sign is that of E (the one-sided MP median needs it).
+    // False when a sum leaves the reciprocal forms' range.
+    template <bool MPF>
+    __device__ __forceinline__ bool face_mapped(const MarchArgs& a, double& L, double& R) {
+        const double q0 = b0 * b0, q1 = b1 * b1, q2 = b2 * b2;
+        const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
+        bool ok = true;
+        double EL, GL, ER, GR;
+        mapped_side(a.ucf + 12, a.mcL, a.ucf, P0, P1, P2, EL, GL, ok);
+        mapped_side(a.ucf + 15, a.mcR, a.ucf + 6, P0, P1, P2, ER, GR, ok);
+        const double p = GL * GR;
+        ok = ok && mid_range_prod(p);
+        const double r = rcp1(p);
+        L = fma(EL * GR, r, v0);
+        R = fma(ER * GL, r, v0);
+        if constexpr (MPF) mp_sided(sign_clear(EL), sign_clear(ER), L, R);
+        return ok;
+    }
+    // One side of face_mapped: ideal weights d[0..2], their constants
+    // mc[4k + 0..3] = (d + d^2, 3 d, 1 - 2 d, d^2), raw candidate
+    // coefficients pc[2r + s] (Coef<5> order).
+    __device__ __forceinline__ void mapped_side(const double* d, const double* mc, const double* pc, double P0,
+                                                double P1, double P2, double& E, double& G, bool& ok) const {
+        const double S = fma(d[0], P0, fma(d[1], P1, d[2] * P2));
+        ok = ok && mid_range(S);
+        const double rS = nr_rcp(S);
+        const double w0 = (d[0] * P0) * rS, w1 = (d[1] * P1) * rS, w2 = (d[2] * P2) * rS;
+        const double N0 = fma(w0, w0 - mc[1], mc[0]), N1 = fma(w1, w1 - mc[5], mc[4]),
+                     N2 = fma(w2, w2 - mc[9], mc[8]);
+        const double D0 = fma(w0, mc[2], mc[3]), D1 = fma(w1, mc[6], mc[7]), D2 = fma(w2, mc[10], mc[11]);
+        const double G0 = (w0 * N0) * (D1 * D2), G1 = (w1 * N1) * (D0 * D2), G2 = (w2 * N2) * (D0 * D1);
+        G = (G0 + G1) + G2;
+        const double e0 = fma(pc[1], d0, pc[0] * dp1), e1 = fma(pc[3], dm1, pc[2] * d0),
+                     e2 = fma(pc[5], dm2, pc[4] * dm1);
+        E = fma(G0, e0, fma(G1, e1, G2 * e2));
+    }
+    // The folded state of face J from the stencils' factors P_k (weights
+    // d_k P_k / sum d P; JS and Z weights).
+    template <bool MPF, class C>
+    __device__ __forceinline__ bool fold(const C& c, double P0, double P1, double P2, double& L, double& R) {
         const double SL = fma(c.dL(0), P0, fma(c.dL(1), P1, c.dL(2) * P2));
         const double SR = fma(c.dR(0), P0, fma(c.dR(1), P1, c.dR(2) * P2));
         const double eL0 = fma(c.kL(1), d0, c.kL(0) * dp1), eL1 = fma(c.kL(3), dm1, c.kL(2) * d0),
@@ -1708,6 +1777,13 @@ inline MarchArgs make_march_args(const SweepGeom& g, const void* in, void* vL, v
             a.kR[2 * r + s] = ucf[15 + r] * ucf[6 + 2 * r + s];
         }
     for (int q = 0; q < 6; ++q) a.pf2[q] = make_float2((float)ucf[q], (float)ucf[6 + q]);
+    for (int k = 0; k < 3; ++k) {
+        const double dl = ucf[12 + k], dr = ucf[15 + k];
+        a.mcL[4 * k] = dl + dl * dl; a.mcL[4 * k + 1] = 3.0 * dl; a.mcL[4 * k + 2] = 1.0 - 2.0 * dl;
+        a.mcL[4 * k + 3] = dl * dl;
+        a.mcR[4 * k] = dr + dr * dr; a.mcR[4 * k + 1] = 3.0 * dr; a.mcR[4 * k + 2] = 1.0 - 2.0 * dr;
+        a.mcR[4 * k + 3] = dr * dr;
+    }
     return a;
 }
 

@@ -94,6 +94,8 @@ struct MarchTmaArgs {
     int ring_off;      // byte offset of the input ring within a warp's area
     int rows_off;      // face-dependent coefficients: byte offset of the table-row ring
     int ldr8;          // per-lane loader, row tiles of floats: cells copied in 8-byte pairs
+    int ldr;           // 1: per-lane loader (the field's rows or base do not suit TMA)
+    int pst;           // 1: plain stores of the face states (face rows not 16-byte multiples)
     unsigned box_bytes;
 };
 
@@ -154,22 +156,37 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col,
     march32_redo<MPF>(a, col, o, L, R);
 }
 
-#ifndef WSB_MTMA_MIN_BLOCKS_F32
-#define WSB_MTMA_MIN_BLOCKS_F32 3
-#endif
-#ifndef WSB_MTMA_MIN_BLOCKS_W7
-#define WSB_MTMA_MIN_BLOCKS_W7 2  // WENO7 carries ~27 doubles of state: 3 CTAs per SM would spill
-#endif
+// One sweep of a grouped launch (sweep_march_tma_multi_kernel): its maps,
+// its arguments, and its first work item within the launch.  The sweeps of
+// a group share the kernel instance (order, weights, storage, tile kind,
+// MP), the coefficients (the kernel's MarchArgs) and the shared-memory
+// layout (the kernel's MarchTmaArgs); extents, strides, pointers, map axes,
+// loader and store kind are the entry's.
+struct MtmaEntry {
+    CUtensorMap tin, toutL, toutR;
+    MarchArgs a;
+    MarchTmaArgs t;
+    long long item0;
+};
+
 // PF: face-dependent coefficients from the per-face table a.ftab (FP64).
 // ORDER 7: the WENO7 engine (face-independent coefficients); face f reads
-// cells f .. f+6 and pushes cell f+7.  TENOW: TENO weights (the engines'
-// face_teno; face-independent coefficients).
-template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5, bool TENOW = false>
-__global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
-                                                  : (sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32))
-    sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
-                           const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
-                           const MarchTmaArgs t) {
+// cells f .. f+6 and pushes cell f+7.  WS: the nonlinear weights, numbered
+// as the reference's schemes: 0 JS (the engines' face), 1 mapped
+// (face_mapped; FP64 WENO5, face-independent coefficients), 2 Z (face_z;
+// FP64 WENO5), 3 TENO (face_teno).  MULTI: the work items of
+// several sweeps (entries ents[0 .. n_ents), items numbered entry after
+// entry); each item finds its entry, whose geometry, maps, loader (TMA or
+// per lane) and store kind (TMA or plain) it uses, with the coefficients of
+// the kernel's MarchArgs.
+template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER, int WS, bool MULTI>
+__device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CUtensorMap* toutL0,
+                                               const CUtensorMap* toutR0, const MarchArgs& a, const MarchTmaArgs& t,
+                                               const MtmaEntry* __restrict__ ents, int n_ents, long long n_items) {
+    constexpr bool TENOW = WS == 3;                       // TENO weights
+    static_assert(WS == 0 || WS == 3 || (ORDER == 5 && sizeof(T) == 8),
+                  "mapped / Z weights: the FP64 WENO5 engine");
+    static_assert(WS != 1 || !PF, "mapped weights: face-independent coefficients");
     constexpr int F = kTmaF, S = PF ? kPfStages : kTmaStages;
     constexpr int NOUT = PF ? kPfOut : kTmaOut;             // output tiles per warp
     constexpr unsigned OB = 32u * F * sizeof(T);          // one output array tile
@@ -177,6 +194,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     constexpr int XS = sizeof(T) == 8 ? 1 : 3;            // KIND 1 column of lane 0
     static_assert(ORDER != 3 || !PF || (sizeof(T) == 8 && !TENOW), "WENO3 per-face table: FP64, JS");
     static_assert(ORDER != 7 || !PF || sizeof(T) == 8, "WENO7 per-face table: FP64");
+    static_assert(!MULTI || !PF, "grouped sweeps: face-independent coefficients");
     constexpr int RW = pf_row_doubles(ORDER), RB = pf_chunk_bytes(ORDER);  // per-face table rows
     static_assert(!TENOW || !PF || ORDER != 3, "TENO with a per-face table: WENO5 / WENO7");
     using Engine = std::conditional_t<
@@ -200,17 +218,23 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
     }
     __syncwarp();
 
-    T* __restrict__ outL = (T*)a.vL;
-    T* __restrict__ outR = (T*)a.vR;
     const long long nwarps = (long long)gridDim.x * kTmaWarps;
-    // faces written: the core faces 3 .. ns-4 (chunks from face 4, face 3 by
-    // the prologue), or every face 0 .. ns-1 for WENO3 (chunks from face 0)
-    const int o_last = ORDER == 3 ? (int)a.ns : (int)a.ns - 3;  // one past the last face
     unsigned n_issued = 0, n_waited = 0;      // tiles requested / completed (waited on) by this warp
     unsigned n_chunks = 0;                    // output chunks stored by this warp
+    // grouped sweeps mix tiles loaded by TMA (completed on the stage's
+    // mbarrier) with tiles copied per lane (no mbarrier phase): bit s is the
+    // parity of the next phase of stage s's mbarrier
+    unsigned ph = 0;
     bool failed = false;
 
     auto tile_ptr = [&](unsigned k) { return ring + (size_t)(k % S) * t.stage_bytes; };
+    auto parity = [&](unsigned k) -> unsigned {
+        if constexpr (MULTI) return (ph >> (k % S)) & 1u;
+        else return (k / S) & 1u;
+    };
+    auto phase_done = [&](unsigned k) {
+        if constexpr (MULTI) ph ^= 1u << (k % S);
+    };
     // per-face table rows (PF): in global memory, and the chunk's rows
     // staged with input tile k
     auto row = [&](int f) { return a.ftab + (long long)f * RW; };
@@ -222,90 +246,150 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
         if constexpr (KIND == 0) return swz<T>((unsigned)lane, (unsigned)p);
         else return (unsigned)((p * XW + lane + XS) * sizeof(T));
     };
-    auto column = [&](int u0, int wv, int vv) {
-        const int uc = u0 + lane < a.Nu ? u0 + lane : a.Nu - 1;
-        return (const T*)a.in + a.in_off + uc * a.sU + wv * a.sW + vv * a.sV;
-    };
-    // request tile k (cells J0 .. J0+7) of the column group (u0, w, v)
-    auto issue = [&](unsigned k, int J0, int u0, int w, int v) {
-        if constexpr (LDR == 0) {
-            if (lane == 0) {
-                unsigned long long* bar = &bars[k % S];
-                const int cU = t.uoff + u0, cW = t.woff + w;
-                const int c0 = t.dimJ == 0 ? J0 : (t.dimU == 0 ? cU : cW);
-                const int c1 = t.dimJ == 1 ? J0 : (t.dimU == 1 ? cU : cW);
-                const int c2 = t.dimJ == 2 ? J0 : (t.dimU == 2 ? cU : cW);
-                mbar_arrive_expect_tx(bar, t.box_bytes + (PF ? (unsigned)RB : 0u));
-                tma_load_4d(tile_ptr(k), &tin, bar, c0, c1, c2, v);
-                // rows J0 .. J0 + 8: the faces of the chunk starting at face J0
-                if constexpr (PF) bulk_load_1d((void*)srow(k, 0), row(J0), RB, bar);
-            }
-        } else {
-            // each lane copies its own column's cells; cells past the end of
-            // the column are zero-filled without being read
-            unsigned char* tp = tile_ptr(k);
-            const T* col = column(u0, w, v);
-            const long long ncell = a.ns + 6;
-            if (KIND == 0 && sizeof(T) == 4 && t.ldr8) {
-                // contiguous, 8-byte aligned cell pairs (even J0, even column
-                // offsets, even ncell: a pair is wholly inside or outside the
-                // column); the 32-byte swizzle keeps pairs adjacent
-#pragma unroll
-                for (int p = 0; p < F; p += 2) {
-                    const long long J = (long long)J0 + p;
-                    const bool inb = J < ncell;
-                    const T* src = col + (inb ? J : 0);
-                    const unsigned dst = smem_u32(tp + cell_off(p));
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
-                                 "r"(inb ? 8u : 0u)
-                                 : "memory");
-                }
-            } else {
-#pragma unroll
-                for (int p = 0; p < F; ++p) {
-                    const long long J = (long long)J0 + p;
-                    const bool inb = J < ncell;
-                    const T* src = col + (inb ? J : 0) * a.sJ;
-                    const unsigned dst = smem_u32(tp + cell_off(p));
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src),
-                                 "n"(sizeof(T)), "r"(inb ? (unsigned)sizeof(T) : 0u)
-                                 : "memory");
-                }
-            }
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-        }
-    };
-    auto wait_tile = [&](unsigned k) -> bool {
-        if constexpr (LDR == 0) {
-            if (!mbar_wait(&bars[k % S], (k / S) & 1u)) return false;
-        } else {
-            // copy groups issued after tile k may stay in flight
-            const unsigned after = n_issued - (k + 1);
-            if (after >= 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
-            else if (after == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
-            else if (after == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-            else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        }
-        n_waited = k + 1;
-        return true;
-    };
     // cell at position p (0..7) of tile k for this lane's column
     auto cell = [&](unsigned k, int p) -> T { return *(const T*)(tile_ptr(k) + cell_off(p)); };
 
-    for (long long item = (long long)blockIdx.x * kTmaWarps + warp; item < a.n_items && !failed; item += nwarps) {
-        const int sg = (int)(item % a.n_seg);
-        long long tt = item / a.n_seg;
-        const int ut = (int)(tt % a.n_ut);
-        tt /= a.n_ut;
-        const int wv = (int)(tt % a.Nw);
-        const int vv = (int)(tt / a.Nw);
+    for (long long item = (long long)blockIdx.x * kTmaWarps + warp; item < n_items && !failed; item += nwarps) {
+        long long li = item;
+        const MtmaEntry* E = nullptr;
+        if constexpr (MULTI) {
+            // the entry holding this item (entries in item order)
+            int lo = 0, hi = n_ents - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (ents[mid].item0 <= item) lo = mid;
+                else hi = mid - 1;
+            }
+            E = ents + lo;
+            li = item - E->item0;
+        }
+        // geometry, maps, loader and store kind of this item's sweep
+        const MarchArgs& g = MULTI ? E->a : a;
+        const MarchTmaArgs& te = MULTI ? E->t : t;
+        const CUtensorMap* mapI = MULTI ? &E->tin : tin0;
+        const CUtensorMap* mapL = MULTI ? &E->toutL : toutL0;
+        const CUtensorMap* mapR = MULTI ? &E->toutR : toutR0;
+        const bool ldr = MULTI ? te.ldr != 0 : LDR == 1;
+        // plain stores (face rows not 16-byte multiples): grouped sweeps only
+        // (the single-sweep kernels keep their registers for the face body)
+        const bool pst = MULTI && te.pst != 0;
+        T* __restrict__ outL = (T*)g.vL;
+        T* __restrict__ outR = (T*)g.vR;
+        // faces written: the core faces 3 .. ns-4 (chunks from face 4, face 3 by
+        // the prologue), or every face 0 .. ns-1 for WENO3 (chunks from face 0)
+        const int o_last = ORDER == 3 ? (int)g.ns : (int)g.ns - 3;  // one past the last face
+        auto column = [&](int u0, int wv, int vv) {
+            const int uc = u0 + lane < g.Nu ? u0 + lane : g.Nu - 1;
+            return (const T*)g.in + g.in_off + uc * g.sU + wv * g.sW + vv * g.sV;
+        };
+        // request tile k (cells J0 .. J0+7) of the column group (u0, w, v)
+        auto issue = [&](unsigned k, int J0, int u0, int w, int v) {
+            if (!ldr) {
+                if (lane == 0) {
+                    unsigned long long* bar = &bars[k % S];
+                    const int cU = te.uoff + u0, cW = te.woff + w;
+                    const int c0 = te.dimJ == 0 ? J0 : (te.dimU == 0 ? cU : cW);
+                    const int c1 = te.dimJ == 1 ? J0 : (te.dimU == 1 ? cU : cW);
+                    const int c2 = te.dimJ == 2 ? J0 : (te.dimU == 2 ? cU : cW);
+                    mbar_arrive_expect_tx(bar, te.box_bytes + (PF ? (unsigned)RB : 0u));
+                    tma_load_4d(tile_ptr(k), mapI, bar, c0, c1, c2, v);
+                    // rows J0 .. J0 + 8: the faces of the chunk starting at face J0
+                    if constexpr (PF) bulk_load_1d((void*)srow(k, 0), row(J0), RB, bar);
+                }
+            } else {
+                // each lane copies its own column's cells; cells past the end of
+                // the column are zero-filled without being read
+                unsigned char* tp = tile_ptr(k);
+                const long long ncell = g.ns + 6;
+                const T* col = column(u0, w, v);
+                if (ORDER == 3 && KIND == 0 && sizeof(T) == 4 && te.ldr8) {
+                    // WENO3 (latency-bound, few registers): the warp copies
+                    // the tile together in 8-byte pairs.  In copy k, lane l
+                    // takes pair l % 4 of column l / 4 + 8k, so one
+                    // instruction reads 8 columns' 32 contiguous bytes (8
+                    // sectors) rather than one pair of each of 32 columns;
+                    // wait_tile then syncs the warp.  (WENO5 / WENO7 run
+                    // 2-3% faster with the per-lane pairs below.)
+                    const int pp = 2 * (lane & 3);
+                    const long long J = (long long)J0 + pp;
+                    const bool inb = J < ncell;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const int r = (lane >> 2) + 8 * kk;
+                        const int uc = u0 + r < g.Nu ? u0 + r : g.Nu - 1;
+                        const T* colr = (const T*)g.in + g.in_off + uc * g.sU + w * g.sW + v * g.sV;
+                        const T* src = colr + (inb ? J : 0);
+                        const unsigned dst = smem_u32(tp + swz<T>((unsigned)r, (unsigned)pp));
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
+                                     "r"(inb ? 8u : 0u)
+                                     : "memory");
+                    }
+                } else if (KIND == 0 && sizeof(T) == 4 && te.ldr8) {
+                    // contiguous, 8-byte aligned cell pairs (even J0, even column
+                    // offsets, even ncell: a pair is wholly inside or outside the
+                    // column); the 32-byte swizzle keeps pairs adjacent
+#pragma unroll
+                    for (int p = 0; p < F; p += 2) {
+                        const long long J = (long long)J0 + p;
+                        const bool inb = J < ncell;
+                        const T* src = col + (inb ? J : 0);
+                        const unsigned dst = smem_u32(tp + cell_off(p));
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
+                                     "r"(inb ? 8u : 0u)
+                                     : "memory");
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < F; ++p) {
+                        const long long J = (long long)J0 + p;
+                        const bool inb = J < ncell;
+                        const T* src = col + (inb ? J : 0) * g.sJ;
+                        const unsigned dst = smem_u32(tp + cell_off(p));
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src),
+                                     "n"(sizeof(T)), "r"(inb ? (unsigned)sizeof(T) : 0u)
+                                     : "memory");
+                    }
+                }
+                asm volatile("cp.async.commit_group;\n" ::: "memory");
+            }
+        };
+        auto wait_tile = [&](unsigned k) -> bool {
+            if (!ldr) {
+                if (!mbar_wait(&bars[k % S], parity(k))) return false;
+                phase_done(k);
+            } else {
+                // copy groups issued after tile k may stay in flight (every
+                // tile of earlier items has been waited on)
+                const unsigned after = n_issued - (k + 1);
+                if (after >= 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+                else if (after == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+                else if (after == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                // the cooperative WENO3 loader fills rows that other lanes read
+                if (ORDER == 3 && KIND == 0 && sizeof(T) == 4 && te.ldr8) __syncwarp();
+            }
+            n_waited = k + 1;
+            return true;
+        };
+
+        const int sg = (int)(li % g.n_seg);
+        long long tt = li / g.n_seg;
+        const int ut = (int)(tt % g.n_ut);
+        tt /= g.n_ut;
+        const int wv = (int)(tt % g.Nw);
+        const int vv = (int)(tt / g.Nw);
         const int u0 = ut * 32;
-        const int f_start = (ORDER == 3 ? 0 : 4) + sg * a.seg;    // 4 mod 8 (WENO3: 0 mod 8)
-        int f_end = f_start + a.seg;
+        const int f_start = (ORDER == 3 ? 0 : 4) + sg * g.seg;    // 4 mod 8 (WENO3: 0 mod 8)
+        int f_end = f_start + g.seg;
         if (f_end > o_last) f_end = o_last;
         const int nch = f_end > f_start ? (f_end - f_start + F - 1) / F : 0;
         const int ntiles = nch + 1;                               // tiles 0 .. nch
         const unsigned k0 = n_issued;                             // first tile of this item
+        if (MULTI && !ldr) {
+            // the ring's stages may last have been written by per-lane copies
+            fence_async_shared();
+            __syncwarp();
+        }
         for (int k = 0; k < ntiles && k < S; ++k) issue(k0 + k, f_start + F * k, u0, wv, vv);
         n_issued += (ntiles < S ? ntiles : S);
         if (!wait_tile(k0)) { failed = true; break; }
@@ -317,7 +401,7 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
             bool ok;
             if constexpr (ORDER == 7) {
                 // face 3 reads cells 3 .. 9: cell 3 lies before tile 0 (cells 4 .. 11)
-                const T c3 = __ldg(column(u0, wv, vv) + 3 * a.sJ);
+                const T c3 = __ldg(column(u0, wv, vv) + 3 * g.sJ);
                 if constexpr (PF) {
                     w.init(a, Row7{row(0)}, Row7{row(1)}, Row7{row(2)}, Row7{row(3)}, c3, cell(k0, 0), cell(k0, 1),
                            cell(k0, 2), cell(k0, 3), cell(k0, 4), cell(k0, 5));
@@ -332,22 +416,28 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 w.init(a, BetaRow(row(1)), BetaRow(row(2)), BetaRow(row(3)), cell(k0, 0), cell(k0, 1), cell(k0, 2),
                        cell(k0, 3), cell(k0, 4));
                 if constexpr (TENOW) ok = w.template face_teno<MPF>(a, FaceRow(row(3)), L, R);
+                else if constexpr (WS == 2) ok = w.template face_z<MPF>(a, FaceRow(row(3)), L, R);
                 else ok = w.template face<MPF>(a, FaceRow(row(3)), L, R);
             } else if constexpr (TENOW) {
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
                 ok = w.template face_teno<MPF>(a, L, R);
+            } else if constexpr (WS == 1 || WS == 2) {
+                w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
+                if constexpr (WS == 1) ok = w.template face_mapped<MPF>(a, L, R);
+                else ok = w.template face_z<MPF>(a, L, R);
             } else {
                 w.init(a, cell(k0, 0), cell(k0, 1), cell(k0, 2), cell(k0, 3), cell(k0, 4));
                 ok = w.template face<MPF>(a, L, R);
             }
             if (!ok) {
-                // (the redo sequences take the weights from the arguments)
-                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(a, column(u0, wv, vv), 3, L, R);
-                else if constexpr (ORDER == 7) march7_redo<MPF>(a, column(u0, wv, vv), 3, L, R);
-                else march_redo<MPF, PF>(a, column(u0, wv, vv), 3, L, R);
+                // (the redo sequences take the weights and strides from the
+                // sweep's arguments)
+                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(g, column(u0, wv, vv), 3, L, R);
+                else if constexpr (ORDER == 7) march7_redo<MPF>(g, column(u0, wv, vv), 3, L, R);
+                else march_redo<MPF, PF>(g, column(u0, wv, vv), 3, L, R);
             }
-            if (u0 + lane < a.Nu) {
-                const long long oi = 3 + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
+            if (u0 + lane < g.Nu) {
+                const long long oi = 3 + (long long)(u0 + lane) * g.oU + wv * g.oW + vv * g.oV;
                 outL[oi] = L;
                 outR[oi] = R;
             }
@@ -379,10 +469,15 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
             // the store issued from this buffer NOUT chunks ago must have read
             // it before the chunk's face states are written: waited here, or
             // (one output buffer) just before the first write, so the first
-            // faces' arithmetic overlaps the store
+            // faces' arithmetic overlaps it.  A chunk of plain stores waits
+            // for every store in flight (grouped sweeps: the last bulk store
+            // may be the one from this buffer)
             const bool wait_out = n_chunks >= (unsigned)NOUT;
             if (NOUT > 1 && wait_out) {
-                if (lane == 0) bulk_wait_read1();
+                if (lane == 0) {
+                    if (MULTI && pst) bulk_wait_read0();
+                    else bulk_wait_read1();
+                }
                 __syncwarp();
             }
             unsigned bad = 0;
@@ -417,8 +512,11 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                 else if constexpr (PF && ORDER == 7 && TENOW) ok = w.template face_teno<MPF>(a, Row7{srow(kc, i)}, L, R);
                 else if constexpr (PF && ORDER == 7) ok = w.template face<MPF>(a, Row7{srow(kc, i)}, L, R);
                 else if constexpr (PF && TENOW) ok = w.template face_teno<MPF>(a, FaceRow(srow(kc, i)), L, R);
+                else if constexpr (PF && WS == 2) ok = w.template face_z<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (PF) ok = w.template face<MPF>(a, FaceRow(srow(kc, i)), L, R);
                 else if constexpr (TENOW) ok = w.template face_teno<MPF>(a, L, R);
+                else if constexpr (WS == 2) ok = w.template face_z<MPF>(a, L, R);
+                else if constexpr (WS == 1) ok = w.template face_mapped<MPF>(a, L, R);
                 else ok = w.template face<MPF>(a, L, R);
                 if (!ok) bad |= 1u << i;
                 Lg[i % G] = L;
@@ -453,29 +551,48 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(a, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 7) march7_redo<MPF>(a, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(a, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(a, col, f0 + i, L, R);
-                    else march_redo<MPF, PF>(a, col, f0 + i, L, R);
+                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(g, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 7) march7_redo<MPF>(g, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(g, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(g, col, f0 + i, L, R);
+                    else march_redo<MPF, PF>(g, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
             }
-            const int i_last = ORDER == 3 ? -1 : o_last - 1 - f0;  // the last core face, when in this chunk
-            if (i_last >= 0 && i_last < F && u0 + lane < a.Nu) {
-                // outside the store map's extent (see launch_march_tma)
-                const long long oi = (o_last - 1) + (long long)(u0 + lane) * a.oU + wv * a.oW + vv * a.oV;
-                outL[oi] = *(const T*)(ob + swz<T>((unsigned)lane, (unsigned)i_last));
-                outR[oi] = *(const T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i_last));
-            }
-            fence_async_shared();
-            __syncwarp();
-            if (lane == 0) {
-                const int c1 = t.odimU == 1 ? u0 : wv, c2 = t.odimU == 2 ? u0 : wv;
-                tma_store_4d(&toutL, ob, f0, c1, c2, vv);
-                tma_store_4d(&toutR, ob + OB, f0, c1, c2, vv);
-                bulk_commit();
+            if (pst) {
+                // plain stores: lane l writes face f0 + l % 8 of columns
+                // l / 8, l / 8 + 4, ..., so one instruction writes four
+                // columns' runs of 8 consecutive faces
+                __syncwarp();
+                const int fi = lane & (F - 1);
+                if (fi < nF) {
+#pragma unroll
+                    for (int cc = lane / F; cc < 32; cc += 32 / F) {
+                        if (u0 + cc < g.Nu) {
+                            const long long oi = (long long)(f0 + fi) + (long long)(u0 + cc) * g.oU + wv * g.oW +
+                                                 vv * g.oV;
+                            outL[oi] = *(const T*)(ob + swz<T>((unsigned)cc, (unsigned)fi));
+                            outR[oi] = *(const T*)(ob + OB + swz<T>((unsigned)cc, (unsigned)fi));
+                        }
+                    }
+                }
+            } else {
+                const int i_last = ORDER == 3 ? -1 : o_last - 1 - f0;  // the last core face, when in this chunk
+                if (i_last >= 0 && i_last < F && u0 + lane < g.Nu) {
+                    // outside the store map's extent (see plan_march_tma)
+                    const long long oi = (o_last - 1) + (long long)(u0 + lane) * g.oU + wv * g.oW + vv * g.oV;
+                    outL[oi] = *(const T*)(ob + swz<T>((unsigned)lane, (unsigned)i_last));
+                    outR[oi] = *(const T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i_last));
+                }
+                fence_async_shared();
+                __syncwarp();
+                if (lane == 0) {
+                    const int c1 = te.odimU == 1 ? u0 : wv, c2 = te.odimU == 2 ? u0 : wv;
+                    tma_store_4d(mapL, ob, f0, c1, c2, vv);
+                    tma_store_4d(mapR, ob + OB, f0, c1, c2, vv);
+                    bulk_commit();
+                }
             }
             ++n_chunks;
             // tile c is consumed: refill its stage with tile c + S
@@ -491,30 +608,80 @@ __global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOC
         // let the tiles still in flight land before the CTA's shared memory
         // is released (bounded, as every wait here); tiles are waited in
         // order, so those past the last completed one are the ones in flight
-        for (unsigned k = n_waited; k < n_issued; ++k) mbar_wait(&bars[k % S], (k / S) & 1u);
+        // (only TMA tiles fail, and an item's tiles are all of one kind)
+        for (unsigned k = n_waited; k < n_issued; ++k) {
+            mbar_wait(&bars[k % S], parity(k));
+            phase_done(k);
+        }
     }
-    if constexpr (LDR == 1) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (LDR == 1 || MULTI) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (lane == 0) bulk_wait_all();
     __syncwarp();
 }
 
-// Host side.  Returns 1003 (unsupported) when the layout does not meet the
-// TMA rules (16-byte aligned bases, strides that are multiples of 16 bytes)
-// or the driver entry point is missing; the caller then uses the marching
-// kernel with per-lane loads.
+#ifndef WSB_MTMA_MIN_BLOCKS_F32
+#define WSB_MTMA_MIN_BLOCKS_F32 3
+#endif
+#ifndef WSB_MTMA_MIN_BLOCKS_W7
+#define WSB_MTMA_MIN_BLOCKS_W7 2  // WENO7 carries ~27 doubles of state: 3 CTAs per SM would spill
+#endif
+#define WSB_MTMA_BOUNDS(ORDER, T)                                                      \
+    __launch_bounds__(kTmaWarps * 32, (ORDER) == 7 ? WSB_MTMA_MIN_BLOCKS_W7            \
+                                                   : (sizeof(T) == 8 ? WSB_MTMA_MIN_BLOCKS : WSB_MTMA_MIN_BLOCKS_F32))
+
+// One sweep: maps and arguments in the parameter bank.
+template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER = 5, int WS = 0>
+__global__ void WSB_MTMA_BOUNDS(ORDER, T)
+    sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
+                           const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
+                           const MarchTmaArgs t) {
+    march_tma_body<MPF, KIND, T, LDR, PF, ORDER, WS, false>(&tin, &toutL, &toutR, a, t, nullptr, 0, a.n_items);
+}
+
+// A group of sweeps in one launch: entries (64-byte aligned, in global
+// memory, written before the launch) in item order, n_items in all;
+// coefficients and shared-memory layout of the group in a and t.
+#ifndef WSB_MTMA_MULTI_MIN_BLOCKS
+#define WSB_MTMA_MULTI_MIN_BLOCKS 3
+#endif
+template <bool MPF, int KIND, typename T, int ORDER, int WS>
+__global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7 : WSB_MTMA_MULTI_MIN_BLOCKS)
+    sweep_march_tma_multi_kernel(const MtmaEntry* __restrict__ ents, int n_ents, long long n_items,
+                                 const __grid_constant__ MarchArgs a, const MarchTmaArgs t) {
+    march_tma_body<MPF, KIND, T, 0, false, ORDER, WS, true>(nullptr, nullptr, nullptr, a, t, ents, n_ents,
+                                                              n_items);
+}
+
+// Host side.  A sweep's plan: its maps, arguments and shared-memory layout.
+// Inputs come by TMA when the field's rows are 16-byte multiples from a
+// 16-byte aligned base, else by per-lane copies into the same tiles; face
+// states leave by TMA stores when the face rows (ns elements) are 16-byte
+// multiples from 16-byte aligned bases, else by plain stores from the same
+// staging tiles.  seg_faces > 0 cuts every column into segments of about
+// that many faces; 0 sizes the segments to fill `sms` SMs about eight
+// work items per resident warp.  Returns 1003 (unsupported) for sweeps of
+// fewer than 8 faces, a lane axis the march arguments did not choose, or a
+// missing driver entry point.
+struct MtmaPlan {
+    CUtensorMap mi, mL, mR;
+    MarchArgs a;
+    MarchTmaArgs t;
+    size_t smem;
+};
+
 template <typename T>
-int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const T* in, T* vL,
-                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms, int order = 5, bool teno = false) {
+int plan_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, const T* in, T* vL, T* vR,
+                   const MarchArgs& a0, int sms, int order, long long seg_faces, MtmaPlan& P) {
     constexpr int ES = (int)sizeof(T);
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return 1003;
-    if ((((uintptr_t)vL) | ((uintptr_t)vR)) & 15) return 1003;
     if (((uintptr_t)in) & (ES - 1)) return 1003;
-    // face rows of the outputs must be 16-byte multiples (ns even for FP64,
-    // a multiple of 4 for FP32); then ns - 4 faces is one too
-    if (g.ns < 8 || ((g.ns * ES) & 15)) return 1003;
-    MarchArgs a = a0;
-    MarchTmaArgs t{};
+    if ((((uintptr_t)vL) | ((uintptr_t)vR)) & (ES - 1)) return 1003;
+    if (g.ns < 8) return 1003;
+    std::memset(&P, 0, sizeof(P));
+    MarchArgs& a = P.a;
+    MarchTmaArgs& t = P.t;
+    a = a0;
     const bool kind1 = folded && dir != 0;
     t.kind = kind1 ? 1 : 0;
     cuuint64_t dims[4], strides[3];
@@ -548,16 +715,14 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     strides[1] = dims[0] * dims[1] * ES;
     strides[2] = dims[0] * dims[1] * dims[2] * ES;
     const CUtensorMapDataType dt = ES == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    CUtensorMap mi, mL, mR;
     // input tiles by TMA when the field's rows are 16-byte multiples and its
     // base is 16-byte aligned; otherwise (e.g. FP32 rows of 218 cells) each
     // lane stages its own cells with cp.async into the same tile layout
-    int ldr = 1;
-    std::memset(&mi, 0, sizeof(mi));
+    t.ldr = 1;
     if (strides[0] % 16 == 0 && (((uintptr_t)in) & 15) == 0 &&
-        enc(&mi, dt, 4, (void*)in, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+        enc(&P.mi, dt, 4, (void*)in, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
-        ldr = 0;
+        t.ldr = 0;
     // per-lane loader in 8-byte pairs: float row tiles whose column starts
     // are all even cells from an 8-byte aligned base (chunks start at even
     // cells, and an even column length keeps every pair inside or outside)
@@ -579,11 +744,13 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     else { t.odimU = 2; t.odimW = 1; }
     ob[t.odimU] = 32;
     const CUtensorMapSwizzle oswz = ES == 8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
-    if (enc(&mL, dt, 4, (void*)vL, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, oswz,
-            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
-        enc(&mR, dt, 4, (void*)vR, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, oswz,
-            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return 1003;
+    t.pst = 1;
+    if (((g.ns * ES) & 15) == 0 && ((((uintptr_t)vL) | ((uintptr_t)vR)) & 15) == 0 &&
+        enc(&P.mL, dt, 4, (void*)vL, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, oswz,
+            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+        enc(&P.mR, dt, 4, (void*)vR, od, os, ob, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, oswz,
+            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+        t.pst = 0;
     // the lane axis must be the one the march arguments chose
     if ((t.kind == 1) != (a.sU == 1)) return 1003;
     // segments over faces [4, ns-3), a multiple of 8 faces each
@@ -592,8 +759,13 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
 #ifndef WSB_MTMA_ITEMS_PER_WARP
 #define WSB_MTMA_ITEMS_PER_WARP 8  // target work items per resident warp (200^3: two segments per column)
 #endif
-    const long long want = (long long)sms * kTmaWarps * 3 * WSB_MTMA_ITEMS_PER_WARP;
-    long long nseg = (want + cols - 1) / cols;
+    long long nseg;
+    if (seg_faces > 0) {
+        nseg = (nf4 + seg_faces - 1) / seg_faces;
+    } else {
+        const long long want = (long long)sms * kTmaWarps * 3 * WSB_MTMA_ITEMS_PER_WARP;
+        nseg = (want + cols - 1) / cols;
+    }
     const long long max_seg = (nf4 + kTmaF - 1) / kTmaF;
     if (nseg > max_seg) nseg = max_seg;
     if (nseg < 1) nseg = 1;
@@ -608,7 +780,27 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     t.ring_off = out_bytes;
     t.rows_off = out_bytes + nst * t.stage_bytes;
     t.warp_bytes = ((t.rows_off + (pf ? nst * pf_chunk_bytes(order) : 0) + 1023) / 1024) * 1024;
-    const size_t smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * nst * 8;
+    P.smem = 1024 + (size_t)kTmaWarps * t.warp_bytes + (size_t)kTmaWarps * nst * 8;
+    return 0;
+}
+
+// One sweep.  Returns 1003 (unsupported) as plan_march_tma, for face rows
+// that are not 16-byte multiples, or for a per-face table whose field does
+// not suit TMA; the caller then uses another kernel.
+template <typename T>
+int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const T* in, T* vL,
+                     T* vR, const MarchArgs& a0, cudaStream_t st, int sms, int order = 5, int ws = 0) {
+    MtmaPlan P;
+    const int prc = plan_march_tma<T>(E, g, dir, folded, in, vL, vR, a0, sms, order, 0, P);
+    if (prc) return prc;
+    // face rows that are not 16-byte multiples: the grouped kernel's plain
+    // stores (batches), other kernels here
+    if (P.t.pst) return 1003;
+    const MarchArgs& a = P.a;
+    const MarchTmaArgs& t = P.t;
+    const bool kind1 = t.kind == 1;
+    const int ldr = t.ldr;
+    const size_t smem = P.smem;
     using KFn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, MarchArgs, MarchTmaArgs);
     static const KFn table[2][2][2] = {
         {{sweep_march_tma_kernel<false, 0, T, 0, false>, sweep_march_tma_kernel<false, 0, T, 1, false>},
@@ -616,15 +808,40 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
         {{sweep_march_tma_kernel<true, 0, T, 0, false>, sweep_march_tma_kernel<true, 0, T, 1, false>},
          {sweep_march_tma_kernel<true, 1, T, 0, false>, sweep_march_tma_kernel<true, 1, T, 1, false>}}};
     KFn kfn = table[mp ? 1 : 0][kind1 ? 1 : 0][ldr];
-    if (teno && a.ftab) {
+    const bool teno = ws == 3;
+    if ((ws == 1 || ws == 2) && (order != 5 || sizeof(T) != 8 || (ws == 1 && a.ftab))) return 1003;
+    if (ws == 2 && a.ftab) {
+        // WENO5-Z with the per-face table: FP64 with TMA input tiles
+        if constexpr (sizeof(T) == 8) {
+            if (ldr) return 1003;
+            static const KFn ptablez[2][2] = {
+                {sweep_march_tma_kernel<false, 0, T, 0, true, 5, 2>, sweep_march_tma_kernel<false, 1, T, 0, true, 5, 2>},
+                {sweep_march_tma_kernel<true, 0, T, 0, true, 5, 2>, sweep_march_tma_kernel<true, 1, T, 0, true, 5, 2>}};
+            kfn = ptablez[mp ? 1 : 0][kind1 ? 1 : 0];
+        }
+    } else if (ws == 1 || ws == 2) {
+        // mapped / Z weights of WENO5, FP64, face-independent coefficients
+        if constexpr (sizeof(T) == 8) {
+            static const KFn tablemz[2][2][2][2] = {
+                {{{sweep_march_tma_kernel<false, 0, T, 0, false, 5, 1>, sweep_march_tma_kernel<false, 0, T, 1, false, 5, 1>},
+                  {sweep_march_tma_kernel<false, 1, T, 0, false, 5, 1>, sweep_march_tma_kernel<false, 1, T, 1, false, 5, 1>}},
+                 {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, 1>, sweep_march_tma_kernel<true, 0, T, 1, false, 5, 1>},
+                  {sweep_march_tma_kernel<true, 1, T, 0, false, 5, 1>, sweep_march_tma_kernel<true, 1, T, 1, false, 5, 1>}}},
+                {{{sweep_march_tma_kernel<false, 0, T, 0, false, 5, 2>, sweep_march_tma_kernel<false, 0, T, 1, false, 5, 2>},
+                  {sweep_march_tma_kernel<false, 1, T, 0, false, 5, 2>, sweep_march_tma_kernel<false, 1, T, 1, false, 5, 2>}},
+                 {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, 2>, sweep_march_tma_kernel<true, 0, T, 1, false, 5, 2>},
+                  {sweep_march_tma_kernel<true, 1, T, 0, false, 5, 2>, sweep_march_tma_kernel<true, 1, T, 1, false, 5, 2>}}}};
+            kfn = tablemz[ws == 2 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0][ldr];
+        }
+    } else if (teno && a.ftab) {
         // TENO with the per-face table (WENO5, WENO7): FP64 with TMA input tiles
         if constexpr (sizeof(T) == 8) {
             if (ldr) return 1003;
             static const KFn ptablet[2][2][2] = {
-                {{sweep_march_tma_kernel<false, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<false, 1, T, 0, true, 5, true>},
-                 {sweep_march_tma_kernel<true, 0, T, 0, true, 5, true>, sweep_march_tma_kernel<true, 1, T, 0, true, 5, true>}},
-                {{sweep_march_tma_kernel<false, 0, T, 0, true, 7, true>, sweep_march_tma_kernel<false, 1, T, 0, true, 7, true>},
-                 {sweep_march_tma_kernel<true, 0, T, 0, true, 7, true>, sweep_march_tma_kernel<true, 1, T, 0, true, 7, true>}}};
+                {{sweep_march_tma_kernel<false, 0, T, 0, true, 5, 3>, sweep_march_tma_kernel<false, 1, T, 0, true, 5, 3>},
+                 {sweep_march_tma_kernel<true, 0, T, 0, true, 5, 3>, sweep_march_tma_kernel<true, 1, T, 0, true, 5, 3>}},
+                {{sweep_march_tma_kernel<false, 0, T, 0, true, 7, 3>, sweep_march_tma_kernel<false, 1, T, 0, true, 7, 3>},
+                 {sweep_march_tma_kernel<true, 0, T, 0, true, 7, 3>, sweep_march_tma_kernel<true, 1, T, 0, true, 7, 3>}}};
             kfn = ptablet[order == 7 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0];
         } else {
             return 1003;
@@ -632,22 +849,22 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     } else if (teno) {
         // TENO weights, WENO5 or WENO7: face-independent coefficients
         static const KFn tablet[2][2][2][2] = {
-            {{{sweep_march_tma_kernel<false, 0, T, 0, false, 5, true>,
-               sweep_march_tma_kernel<false, 0, T, 1, false, 5, true>},
-              {sweep_march_tma_kernel<false, 1, T, 0, false, 5, true>,
-               sweep_march_tma_kernel<false, 1, T, 1, false, 5, true>}},
-             {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, true>,
-               sweep_march_tma_kernel<true, 0, T, 1, false, 5, true>},
-              {sweep_march_tma_kernel<true, 1, T, 0, false, 5, true>,
-               sweep_march_tma_kernel<true, 1, T, 1, false, 5, true>}}},
-            {{{sweep_march_tma_kernel<false, 0, T, 0, false, 7, true>,
-               sweep_march_tma_kernel<false, 0, T, 1, false, 7, true>},
-              {sweep_march_tma_kernel<false, 1, T, 0, false, 7, true>,
-               sweep_march_tma_kernel<false, 1, T, 1, false, 7, true>}},
-             {{sweep_march_tma_kernel<true, 0, T, 0, false, 7, true>,
-               sweep_march_tma_kernel<true, 0, T, 1, false, 7, true>},
-              {sweep_march_tma_kernel<true, 1, T, 0, false, 7, true>,
-               sweep_march_tma_kernel<true, 1, T, 1, false, 7, true>}}}};
+            {{{sweep_march_tma_kernel<false, 0, T, 0, false, 5, 3>,
+               sweep_march_tma_kernel<false, 0, T, 1, false, 5, 3>},
+              {sweep_march_tma_kernel<false, 1, T, 0, false, 5, 3>,
+               sweep_march_tma_kernel<false, 1, T, 1, false, 5, 3>}},
+             {{sweep_march_tma_kernel<true, 0, T, 0, false, 5, 3>,
+               sweep_march_tma_kernel<true, 0, T, 1, false, 5, 3>},
+              {sweep_march_tma_kernel<true, 1, T, 0, false, 5, 3>,
+               sweep_march_tma_kernel<true, 1, T, 1, false, 5, 3>}}},
+            {{{sweep_march_tma_kernel<false, 0, T, 0, false, 7, 3>,
+               sweep_march_tma_kernel<false, 0, T, 1, false, 7, 3>},
+              {sweep_march_tma_kernel<false, 1, T, 0, false, 7, 3>,
+               sweep_march_tma_kernel<false, 1, T, 1, false, 7, 3>}},
+             {{sweep_march_tma_kernel<true, 0, T, 0, false, 7, 3>,
+               sweep_march_tma_kernel<true, 0, T, 1, false, 7, 3>},
+              {sweep_march_tma_kernel<true, 1, T, 0, false, 7, 3>,
+               sweep_march_tma_kernel<true, 1, T, 1, false, 7, 3>}}}};
         kfn = tablet[order == 7 ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0][ldr];
     } else if (order == 3 && a.ftab) {
         // WENO3-JS with the per-face table: FP64 with TMA input tiles
@@ -706,8 +923,25 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
     long long blocks = (a.n_items + kTmaWarps - 1) / kTmaWarps;
     const long long cap = (long long)sms * occ;
     if (blocks > cap) blocks = cap;
-    kfn<<<(unsigned)blocks, kTmaWarps * 32, smem, st>>>(mi, mL, mR, a, t);
+    kfn<<<(unsigned)blocks, kTmaWarps * 32, smem, st>>>(P.mi, P.mL, P.mR, a, t);
     return 0;
+}
+
+// Kernel of a group of sweeps, by storage T, order, weights, MP and tile
+// kind (null for WENO3 with TENO weights, which no engine covers).
+using MtmaMultiFn = void (*)(const MtmaEntry*, int, long long, MarchArgs, MarchTmaArgs);
+template <typename T, int ORDER, int WS>
+MtmaMultiFn mtma_multi_pick(bool mp, bool kind1) {
+    static const MtmaMultiFn tab[2][2] = {
+        {sweep_march_tma_multi_kernel<false, 0, T, ORDER, WS>, sweep_march_tma_multi_kernel<false, 1, T, ORDER, WS>},
+        {sweep_march_tma_multi_kernel<true, 0, T, ORDER, WS>, sweep_march_tma_multi_kernel<true, 1, T, ORDER, WS>}};
+    return tab[mp ? 1 : 0][kind1 ? 1 : 0];
+}
+template <typename T>
+MtmaMultiFn mtma_multi_kernel(int order, bool teno, bool mp, bool kind1) {
+    if (order == 3) return teno ? nullptr : mtma_multi_pick<T, 3, 0>(mp, kind1);
+    if (order == 7) return teno ? mtma_multi_pick<T, 7, 3>(mp, kind1) : mtma_multi_pick<T, 7, 0>(mp, kind1);
+    return teno ? mtma_multi_pick<T, 5, 3>(mp, kind1) : mtma_multi_pick<T, 5, 0>(mp, kind1);
 }
 
 }  // namespace wsb

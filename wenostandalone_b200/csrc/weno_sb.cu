@@ -300,6 +300,15 @@ bool march_weights_ok(const double* ucf, int order = 5) {
     return true;
 }
 
+// The mapped-WENO5 engine needs every ideal weight in (0, 0.8): there each
+// mapped weight is positive (numerator and denominator of the map), so a
+// state's offset from v0 has the sign of its folded sum.
+bool march_mapped_ok(const double* ucf) {
+    for (int q = 12; q < 18; ++q)
+        if (!(ucf[q] > 0.0 && ucf[q] < 0.8)) return false;
+    return true;
+}
+
 // FP64 marching sweep with face-dependent coefficient arrays (WENO5 and
 // WENO7 with JS or TENO weights, WENO3-JS): the per-face table (one row per
 // face, 224 bytes for WENO5, 448 for WENO7, 96 for WENO3; ns + 16 rows: the kernel stages rows f0 .. f0 + 8
@@ -309,9 +318,9 @@ bool march_weights_ok(const double* ucf, int order = 5) {
 // or the table cannot be allocated.
 int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool folded, bool mp, const double* in,
                        double* vL, double* vR, const CoefPtrs& cp, const WenoParams& wp, cudaStream_t st,
-                       bool teno = false, int order = 5) {
+                       int ws = 0, int order = 5) {
     if (!cp.polyL || !cp.polyR || !cp.dL || !cp.dR || !cp.beta) return WENO_SB_ERR_UNSUPPORTED;
-    if (g.ns < 8 || ((g.ns * 8) & 15) || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
+    if (g.ns < 8 || ((uintptr_t)in & 15)) return WENO_SB_ERR_UNSUPPORTED;
     const int rows = (int)g.ns + 16;
     double* tab = nullptr;
     // an error left by an earlier call is reported, not cleared by the
@@ -336,7 +345,7 @@ int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool f
     MarchArgs a0 = make_march_args(g, in, vL, vR, wp, nullptr);
     a0.ftab = tab;
     a0.cp = cp;
-    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, teno);
+    const int rc = launch_march_tma<double>(E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, ws);
     const cudaError_t le = cudaGetLastError();
     WSB_CUDA(cudaFreeAsync(tab, st));
     if (rc) return rc;
@@ -360,9 +369,16 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if ((choice == 0 || choice == 3) && ucf && (order == 5 || order == 7) && gr->scheme == WENO_SB_TENO &&
         march_weights_ok(ucf, order)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, order);
-        int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, true);
+        int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, WENO_SB_TENO);
         if (rc != WENO_SB_ERR_UNSUPPORTED)
             return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (TENO)") : rc;
+    }
+    if ((choice == 0 || choice == 3) && ucf && order == 5 && sizeof(T) == 8 &&
+        ((gr->scheme == WENO_SB_Z && march_weights_ok(ucf)) || (gr->scheme == WENO_SB_MAPPED && march_mapped_ok(ucf)))) {
+        const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 5);
+        int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 5, gr->scheme);
+        if (rc != WENO_SB_ERR_UNSUPPORTED)
+            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (mapped / Z)") : rc;
     }
     if ((choice == 0 || choice == 3) && ucf && order == 3 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 3)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 3);
@@ -390,8 +406,8 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
     if constexpr (sizeof(T) == 8) {
         if ((choice == 0 || choice == 3) && !ucf &&
             (((order == 5 || order == 7) && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO)) ||
-             (order == 3 && gr->scheme == WENO_SB_JS))) {
-            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme == WENO_SB_TENO,
+             (order == 5 && gr->scheme == WENO_SB_Z) || (order == 3 && gr->scheme == WENO_SB_JS))) {
+            int rc = launch_march_faces(d.E, g, dir, folded, mp, in, vL, vR, cp, wp, st, gr->scheme,
                                         order);
             if (rc != WENO_SB_ERR_UNSUPPORTED) return rc;
         }
@@ -484,8 +500,27 @@ int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsign
 //          parallel branches of the graph, balanced by longest-processing-
 //          time-first on the entries' estimated cost, so small blocks run
 //          beside each other and beside the tails of large ones.
-// Either way a launch is one cudaGraphLaunch of the captured work.
+//  mode 2: the entries that a marching engine covers are grouped by kernel
+//          instance (storage, order, weights, MP, tile kind) and
+//          coefficients; each group is one launch of the grouped TMA
+//          marching kernel over the work items of all its sweeps (columns
+//          cut into segments of about `seg_faces` faces), the groups spread
+//          over `branches` graph branches by longest-processing-time-first;
+//          the other entries run as in mode 1.
+// Every way a launch is one cudaGraphLaunch of the captured work.
 constexpr int kBatchMaxBranches = 16;
+
+// Mode 2: the sweeps of one grouped launch.
+struct MtmaGroup {
+    int fp32 = 0, order = 5, teno = 0, mp = 0, kind = 0;
+    MarchArgs a{};            // coefficients of the group (its first entry's arguments)
+    MarchTmaArgs t{};         // shared-memory layout (the same for every entry)
+    size_t smem = 0;
+    std::vector<MtmaEntry> ents;
+    MtmaEntry* d_ents = nullptr;
+    long long n_items = 0;
+    double cost = 0;
+};
 
 struct Batch {
     std::vector<weno_sb_block> blocks;
@@ -498,8 +533,11 @@ struct Batch {
     int threads = 128;  // face-tile width = CTA size
     int U = 8;          // columns per work item
     int grid = 0;
-    int mode = 1;       // 0: persistent kernel, 1: graph of specialised sweeps
-    int branches = 8;   // mode 1: parallel branches of the graph
+    int mode = 2;       // 0: persistent kernel, 1: graph of specialised sweeps, 2: grouped sweeps
+    int branches = 8;   // modes 1, 2: parallel branches of the graph
+    int seg_faces = 64; // mode 2: faces per work item (segment of a column)
+    std::vector<MtmaGroup> groups;   // mode 2: grouped launches
+    std::vector<size_t> rest;        // mode 2: entries outside the groups
     // mode 1: each entry's face-independent coefficients (Coef<order>
     // layout), when its arrays hold the same values on every face
     std::vector<std::vector<double>> ucf;
@@ -612,12 +650,160 @@ int batch_enqueue_sweeps(Batch* B, cudaStream_t st) {
     return rc;
 }
 
+void batch_free_groups(Batch* B) {
+    for (auto& G : B->groups)
+        if (G.d_ents) cudaFree(G.d_ents);
+    B->groups.clear();
+    B->rest.clear();
+}
+
+// The coefficient part of two entries' march arguments is the same (the
+// values a grouped launch takes from its kernel parameters).
+bool march_coefs_equal(const MarchArgs& x, const MarchArgs& y) {
+    return x.wp.scheme == y.wp.scheme && std::memcmp(&x.wp.eps, &y.wp.eps, sizeof(double)) == 0 &&
+           std::memcmp(&x.wp.teno_ct, &y.wp.teno_ct, sizeof(double)) == 0 &&
+           std::memcmp(x.ucf, y.ucf, sizeof(x.ucf)) == 0 && std::memcmp(x.ucf32, y.ucf32, sizeof(x.ucf32)) == 0 &&
+           std::memcmp(x.kL, y.kL, sizeof(x.kL)) == 0 && std::memcmp(x.kR, y.kR, sizeof(x.kR)) == 0 &&
+           std::memcmp(x.pf2, y.pf2, sizeof(x.pf2)) == 0 && std::memcmp(x.kL7, y.kL7, sizeof(x.kL7)) == 0 &&
+           std::memcmp(x.kR7, y.kR7, sizeof(x.kR7)) == 0 && std::memcmp(x.pf7, y.pf7, sizeof(x.pf7)) == 0;
+}
+
+// Mode 2: plan every marching entry's sweep (segments of about seg_faces
+// faces), group the sweeps by kernel instance and coefficients, and upload
+// each group's entry table.  Entries that no group takes go to B->rest.
+int batch_plan_groups(Batch* B, int seg_faces) {
+    batch_free_groups(B);
+    B->seg_faces = seg_faces;
+    for (size_t i = 0; i < B->entries.size(); ++i) {
+        const BatchEntry& e = B->entries[i];
+        const weno_sb_block& b = B->blocks[i];
+        bool placed = false;
+        if (e.march && kernel_choice() != 1) {
+            Dims d;
+            if (check_grid(&b.grid, &d) == 0) {
+                const bool folded = (b.flags & WENO_SB_F_FOLDED) != 0;
+                const MarchArgs& a0 = B->margs[e.march - 1];
+                MtmaPlan P;
+                const int prc =
+                    e.fp32 ? plan_march_tma<float>(d.E, e.g, b.dir, folded, (const float*)e.in, (float*)e.vL,
+                                                   (float*)e.vR, a0, num_sms(), e.order, seg_faces, P)
+                           : plan_march_tma<double>(d.E, e.g, b.dir, folded, (const double*)e.in, (double*)e.vL,
+                                                    (double*)e.vR, a0, num_sms(), e.order, seg_faces, P);
+                const bool teno = e.wp.scheme == WENO_SB_TENO;
+                if (prc == 0 && !(e.order == 3 && teno)) {
+                    MtmaGroup* G = nullptr;
+                    for (auto& q : B->groups)
+                        if (q.fp32 == e.fp32 && q.order == e.order && q.teno == (int)teno && q.mp == e.mp &&
+                            q.kind == P.t.kind && march_coefs_equal(q.a, P.a)) {
+                            G = &q;
+                            break;
+                        }
+                    if (!G) {
+                        B->groups.emplace_back();
+                        G = &B->groups.back();
+                        G->fp32 = e.fp32;
+                        G->order = e.order;
+                        G->teno = teno ? 1 : 0;
+                        G->mp = e.mp;
+                        G->kind = P.t.kind;
+                        G->a = P.a;
+                        G->t = P.t;
+                        G->smem = P.smem;
+                    }
+                    MtmaEntry me;
+                    std::memset(&me, 0, sizeof(me));
+                    me.tin = P.mi;
+                    me.toutL = P.mL;
+                    me.toutR = P.mR;
+                    me.a = P.a;
+                    me.t = P.t;
+                    me.item0 = G->n_items;
+                    G->ents.push_back(me);
+                    G->n_items += P.a.n_items;
+                    G->cost += batch_entry_cost(B, i);
+                    placed = true;
+                }
+            }
+        }
+        if (!placed) B->rest.push_back(i);
+    }
+    for (auto& G : B->groups) {
+        WSB_CUDA(cudaMalloc((void**)&G.d_ents, sizeof(MtmaEntry) * G.ents.size()));
+        WSB_CUDA(cudaMemcpy(G.d_ents, G.ents.data(), sizeof(MtmaEntry) * G.ents.size(), cudaMemcpyHostToDevice));
+    }
+    batch_release_graph(B);
+    return WENO_SB_OK;
+}
+
+// Mode 2: the grouped launches and the remaining entries' sweeps on
+// B->branches parallel streams forked from (and joined back into) the
+// capturing stream, longest first onto the least loaded branch.
+int batch_enqueue_groups(Batch* B, cudaStream_t st) {
+    const int nb = std::max(1, std::min(B->branches, kBatchMaxBranches));
+    WSB_CUDA(cudaEventRecord(B->fork, st));
+    for (int k = 0; k < nb; ++k) WSB_CUDA(cudaStreamWaitEvent(B->br[k], B->fork, 0));
+    // work units: groups (index >= 0) and remaining entries (~index)
+    std::vector<std::pair<double, long long>> units;
+    for (size_t q = 0; q < B->groups.size(); ++q) units.push_back({B->groups[q].cost, (long long)q});
+    for (size_t i : B->rest) units.push_back({batch_entry_cost(B, i), ~(long long)i});
+    std::stable_sort(units.begin(), units.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<double> load(nb, 0.0);
+    int rc = 0;
+    const int sms = num_sms();
+    for (const auto& u : units) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += u.first;
+        if (u.second >= 0) {
+            const MtmaGroup& G = B->groups[(size_t)u.second];
+            const MtmaMultiFn kfn = G.fp32 ? mtma_multi_kernel<float>(G.order, G.teno != 0, G.mp != 0, G.kind == 1)
+                                           : mtma_multi_kernel<double>(G.order, G.teno != 0, G.mp != 0, G.kind == 1);
+            if (!kfn) { rc = set_err(WENO_SB_ERR_UNSUPPORTED, "no grouped kernel for a batch group"); break; }
+            rc = cuda_err(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
+                          "cudaFuncSetAttribute");
+            if (rc) break;
+            int occ = 0;
+            rc = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kTmaWarps * 32, G.smem),
+                          "occupancy");
+            if (rc) break;
+            if (occ < 1) occ = 1;
+            long long blocks = (G.n_items + kTmaWarps - 1) / kTmaWarps;
+            blocks = std::min(blocks, (long long)sms * occ);
+            if (blocks < 1) continue;
+            kfn<<<(unsigned)blocks, kTmaWarps * 32, G.smem, B->br[k]>>>(G.d_ents, (int)G.ents.size(), G.n_items, G.a,
+                                                                          G.t);
+            rc = cuda_err(cudaGetLastError(), "grouped sweep launch");
+        } else {
+            const size_t i = (size_t)(~u.second);
+            const weno_sb_block& b = B->blocks[i];
+            Dims d;
+            rc = check_grid(&b.grid, &d);
+            if (rc) break;
+            const double* uc = B->ucf[i].empty() ? nullptr : B->ucf[i].data();
+            if (b.dtype == WENO_SB_FP64)
+                rc = run_weno<double>(d, &b.grid, b.dir, b.order, b.flags, (const double*)b.v_in, &b.coefs,
+                                      (double*)b.vL, (double*)b.vR, B->br[k], uc);
+            else
+                rc = run_weno<float>(d, &b.grid, b.dir, b.order, b.flags, (const float*)b.v_in, &b.coefs,
+                                     (float*)b.vL, (float*)b.vR, B->br[k], uc);
+        }
+        if (rc) break;
+    }
+    // join every branch, also after a failed launch, so a capture ends cleanly
+    for (int k = 0; k < nb; ++k) {
+        cudaEventRecord(B->join[k], B->br[k]);
+        cudaStreamWaitEvent(st, B->join[k], 0);
+    }
+    return rc;
+}
+
 // Capture the batch into a CUDA graph: mode 0 the counter reset and the
-// persistent kernel, mode 1 the branches of specialised sweeps.
+// persistent kernel, mode 1 the branches of specialised sweeps, mode 2 the
+// branches of grouped sweeps.
 int batch_build_graph(Batch* B) {
     batch_release_graph(B);
     WSB_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
-    const int rc = B->mode == 1 ? batch_enqueue_sweeps(B, B->cap) : batch_enqueue(B, B->cap);
+    const int rc = B->mode == 2 ? batch_enqueue_groups(B, B->cap)
+                                : (B->mode == 1 ? batch_enqueue_sweeps(B, B->cap) : batch_enqueue(B, B->cap));
     cudaGraph_t gph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(B->cap, &gph);
     if (rc) {
@@ -1324,6 +1510,7 @@ bool batch_coefs_uniform(const weno_sb_coefs& cf, long long nc, int order, doubl
 void batch_free(Batch* B) {
     if (B->cap) cudaStreamSynchronize(B->cap);
     batch_release_graph(B);
+    batch_free_groups(B);
     if (B->d_entries) cudaFree(B->d_entries);
     if (B->d_counter) cudaFree(B->d_counter);
     if (B->d_margs) cudaFree(B->d_margs);
@@ -1401,6 +1588,7 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
     }
     if (!rc) rc = cuda_err(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming), "cudaEventCreate");
     if (!rc) rc = batch_layout(B, 128, 8);
+    if (!rc) rc = batch_plan_groups(B, B->seg_faces);
     if (rc) {
         batch_free(B);
         return rc;
@@ -1411,13 +1599,14 @@ int weno_sb_batch_create(const weno_sb_block* blocks, int n, int* batch) {
     return WENO_SB_OK;
 }
 
-// Time both ways of running the batch -- the persistent kernel over its
-// tile shapes (CTA width x columns per item) and the graph of specialised
-// sweeps over its branch counts -- and keep the fastest.  Each candidate is
-// captured into its graph, launched once to warm up and three times timed.
-// With WENO_SB_TUNE_CACHE naming a file, a batch of the same composition
-// reuses the recorded choice (one line: signature, threads, columns per
-// item, milliseconds, mode, branches).
+// Time the ways of running the batch -- the persistent kernel over its
+// tile shapes (CTA width x columns per item), the graph of specialised
+// sweeps over its branch counts, the grouped sweeps over segment lengths
+// and branch counts -- and keep the fastest.  Each candidate is captured
+// into its graph, launched once to warm up and three times timed.  With
+// WENO_SB_TUNE_CACHE naming a file, a batch of the same composition reuses
+// the recorded choice (one line: signature, threads, columns per item,
+// milliseconds, mode, branches, faces per grouped work item).
 int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_item, double* best_ms) {
     Batch* B = get_batch(batch);
     if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
@@ -1435,13 +1624,15 @@ int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_
         while (std::getline(f, line)) {
             std::istringstream ls(line);
             unsigned long long h;
-            int t, u, mode = 0, nb = 8;
+            int t, u, mode = 0, nb = 8, sf = 64;
             double ms;
             if ((ls >> std::hex >> h >> std::dec >> t >> u >> ms) && h == sig) {
                 if (!(ls >> mode >> nb)) { mode = 0; nb = 8; }
+                if (!(ls >> sf) || sf < 8 || sf > 4096) sf = 64;
                 int rc = batch_layout(B, t, u);
+                if (!rc && mode == 2 && sf != B->seg_faces) rc = batch_plan_groups(B, sf);
                 if (rc) return rc;
-                B->mode = mode == 1 ? 1 : 0;
+                B->mode = (mode == 1 || mode == 2) ? mode : 0;
                 B->branches = std::max(1, std::min(nb, kBatchMaxBranches));
                 batch_release_graph(B);
                 report(ms);
@@ -1449,11 +1640,14 @@ int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_
             }
         }
     }
-    struct Cand { int mode, t, u, nb; };
+    struct Cand { int mode, t, u, nb, sf; };
     std::vector<Cand> cands;
     for (int t : {64, 128, 256})
-        for (int u : {4, 8, 16, 32}) cands.push_back({0, t, u, 0});
-    for (int nb : {1, 2, 4, 8, 16}) cands.push_back({1, 128, 8, nb});
+        for (int u : {4, 8, 16, 32}) cands.push_back({0, t, u, 0, 0});
+    for (int nb : {1, 2, 4, 8, 16}) cands.push_back({1, 128, 8, nb, 0});
+    if (!B->groups.empty())
+        for (int sf : {32, 64, 128})
+            for (int nb : {1, 2, 4}) cands.push_back({2, 128, 8, nb, sf});
     cudaEvent_t e0, e1;
     WSB_CUDA(cudaEventCreate(&e0));
     WSB_CUDA(cudaEventCreate(&e1));
@@ -1462,9 +1656,10 @@ int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_
     int rc = 0;
     for (const Cand& c : cands) {
         rc = batch_layout(B, c.t, c.u);
+        if (!rc && c.mode == 2 && c.sf != B->seg_faces) rc = batch_plan_groups(B, c.sf);
         if (rc) break;
         B->mode = c.mode;
-        B->branches = c.mode == 1 ? c.nb : B->branches;
+        B->branches = c.mode != 0 ? c.nb : B->branches;
         rc = batch_build_graph(B);
         if (!rc) rc = cuda_err(cudaGraphLaunch(B->exec, st), "cudaGraphLaunch");  // warm-up
         if (rc) break;
@@ -1485,14 +1680,15 @@ int weno_sb_batch_autotune(int batch, void* stream, int* threads, int* cols_per_
     cudaEventDestroy(e1);
     if (rc) return rc;
     rc = batch_layout(B, bc.t, bc.u);
+    if (!rc && bc.mode == 2 && bc.sf != B->seg_faces) rc = batch_plan_groups(B, bc.sf);
     if (rc) return rc;
     B->mode = bc.mode;
-    if (bc.mode == 1) B->branches = bc.nb;
+    if (bc.mode != 0) B->branches = bc.nb;
     batch_release_graph(B);
     if (cache && *cache) {
         std::ofstream f(cache, std::ios::app);
         f << std::hex << sig << std::dec << " " << bc.t << " " << bc.u << " " << best << " " << bc.mode << " "
-          << B->branches << "\n";
+          << B->branches << " " << B->seg_faces << "\n";
     }
     report(best);
     return WENO_SB_OK;
@@ -1523,7 +1719,8 @@ int weno_sb_batch_destroy(int batch) {
 int weno_sb_batch_configure(int batch, int mode, int threads, int cols_per_item, int branches) {
     Batch* B = get_batch(batch);
     if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
-    if (mode != 0 && mode != 1) return set_err(WENO_SB_ERR_ARG, "mode must be 0 (persistent) or 1 (graph of sweeps)");
+    if (mode < 0 || mode > 2)
+        return set_err(WENO_SB_ERR_ARG, "mode must be 0 (persistent), 1 (graph of sweeps) or 2 (grouped sweeps)");
     if (mode == 0) {
         if (threads != 64 && threads != 128 && threads != 256)
             return set_err(WENO_SB_ERR_ARG, "threads must be 64, 128 or 256 (got %d)", threads);
@@ -1534,7 +1731,16 @@ int weno_sb_batch_configure(int batch, int mode, int threads, int cols_per_item,
     }
     if (branches < 1 || branches > kBatchMaxBranches)
         return set_err(WENO_SB_ERR_ARG, "branches must be 1..%d (got %d)", kBatchMaxBranches, branches);
-    B->mode = 1;
+    if (mode == 2) {
+        if (cols_per_item < 8 || cols_per_item > 4096)
+            return set_err(WENO_SB_ERR_ARG, "mode 2: cols_per_item (faces per work item) must be 8..4096 (got %d)",
+                           cols_per_item);
+        if (cols_per_item != B->seg_faces) {
+            const int rc = batch_plan_groups(B, cols_per_item);
+            if (rc) return rc;
+        }
+    }
+    B->mode = mode;
     B->branches = branches;
     batch_release_graph(B);
     return WENO_SB_OK;
@@ -1545,7 +1751,7 @@ int weno_sb_batch_query(int batch, int* mode, int* threads, int* cols_per_item, 
     if (!B) return set_err(WENO_SB_ERR_HANDLE, "unknown batch %d", batch);
     if (mode) *mode = B->mode;
     if (threads) *threads = B->threads;
-    if (cols_per_item) *cols_per_item = B->U;
+    if (cols_per_item) *cols_per_item = B->mode == 2 ? B->seg_faces : B->U;
     if (branches) *branches = B->branches;
     return WENO_SB_OK;
 }

@@ -255,7 +255,9 @@ module m_weno_sb
             real(c_double), intent(out) :: polyL(*), polyR(*), dL(*), dR(*), beta_coef(*)
         end function weno_sb_coefficients
 
-        ! ---- batches of uneven blocks (one persistent launch in a CUDA graph)
+        ! ---- batches of uneven blocks (one CUDA graph launch of all the blocks' sweeps;
+        !      configure mode 0 persistent kernel, 1 graph of per-block sweeps,
+        !      2 grouped marching sweeps with cols_per_item = faces per work item)
 
         integer(c_int) function weno_sb_batch_create(blocks, n, batch) bind(C, name='weno_sb_batch_create')
             import :: c_int, weno_sb_block
