@@ -162,12 +162,45 @@ __device__ __forceinline__ void march_redo(const MarchArgs& a, const float* col,
 // MP), the coefficients (the kernel's MarchArgs) and the shared-memory
 // layout (the kernel's MarchTmaArgs); extents, strides, pointers, map axes,
 // loader and store kind are the entry's.
+// The part of a sweep's arguments a grouped work item reads outside the
+// face body; each item copies it (with the sweep's MarchTmaArgs) into its
+// warp's slot of shared memory, so the chunk loop reads it from there
+// rather than from the entry table (the table stays in global memory, and
+// every asynchronous copy or wait in the loop would reload it).
+struct MtmaGeo {
+    const void* in;
+    void* vL;
+    void* vR;
+    long long ns, sJ, sU, sW, sV, in_off, oU, oW, oV;
+    int Nu, Nw, n_ut, seg, n_seg, pad_;
+};
+struct MtmaItemArgs {
+    MtmaGeo geo;
+    MarchTmaArgs t;
+};
+static_assert(sizeof(MtmaItemArgs) % 8 == 0 && sizeof(MtmaItemArgs) <= 256, "per-warp argument slot");
+constexpr int kMtmaSlot = 256;  // bytes of shared memory per warp for the item's arguments
+inline MtmaGeo mtma_geo(const MarchArgs& a) {
+    MtmaGeo g{};
+    g.in = a.in; g.vL = a.vL; g.vR = a.vR;
+    g.ns = a.ns; g.sJ = a.sJ; g.sU = a.sU; g.sW = a.sW; g.sV = a.sV; g.in_off = a.in_off;
+    g.oU = a.oU; g.oW = a.oW; g.oV = a.oV;
+    g.Nu = a.Nu; g.Nw = a.Nw; g.n_ut = a.n_ut; g.seg = a.seg; g.n_seg = a.n_seg;
+    return g;
+}
 struct MtmaEntry {
     CUtensorMap tin, toutL, toutR;
-    MarchArgs a;
-    MarchTmaArgs t;
-    long long item0;
+    MtmaItemArgs ia;
+    MarchArgs a;  // for the faces redone by the reference sequence
 };
+
+// The geometry of an item: the kernel's parameters (one sweep) or the
+// warp's shared-memory copy (grouped sweeps).
+template <bool MULTI>
+__device__ __forceinline__ const auto& mtma_geo_of(const MarchArgs& a, const MtmaItemArgs* slot) {
+    if constexpr (MULTI) return slot->geo;
+    else return a;
+}
 
 // PF: face-dependent coefficients from the per-face table a.ftab (FP64).
 // ORDER 7: the WENO7 engine (face-independent coefficients); face f reads
@@ -182,7 +215,8 @@ struct MtmaEntry {
 template <bool MPF, int KIND, typename T, int LDR, bool PF, int ORDER, int WS, bool MULTI>
 __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CUtensorMap* toutL0,
                                                const CUtensorMap* toutR0, const MarchArgs& a, const MarchTmaArgs& t,
-                                               const MtmaEntry* __restrict__ ents, int n_ents, long long n_items) {
+                                               const MtmaEntry* __restrict__ ents,
+                                               const long long* __restrict__ item0s, int n_ents, long long n_items) {
     constexpr bool TENOW = WS == 3;                       // TENO weights
     static_assert(WS == 0 || WS == 3 || (ORDER == 5 && sizeof(T) == 8),
                   "mapped / Z weights: the FP64 WENO5 engine");
@@ -212,6 +246,9 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
     unsigned char* obuf = wbase;
     unsigned char* ring = wbase + t.ring_off;
     unsigned long long* bars = (unsigned long long*)(base + (size_t)kTmaWarps * warp_bytes) + warp * S;
+    // grouped sweeps: the warp's argument slot, after the mbarriers
+    MtmaItemArgs* slot = (MtmaItemArgs*)(base + (size_t)kTmaWarps * warp_bytes + (size_t)kTmaWarps * S * 8 +
+                                         (size_t)warp * kMtmaSlot);
     if (lane == 0) {
         for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -253,19 +290,30 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
         long long li = item;
         const MtmaEntry* E = nullptr;
         if constexpr (MULTI) {
-            // the entry holding this item (entries in item order)
+            // the entry holding this item: entries in item order, their first
+            // items in the dense array item0s (a few hundred bytes, L1-resident)
             int lo = 0, hi = n_ents - 1;
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (ents[mid].item0 <= item) lo = mid;
+                if (__ldg(item0s + mid) <= item) lo = mid;
                 else hi = mid - 1;
             }
             E = ents + lo;
-            li = item - E->item0;
+            li = item - __ldg(item0s + lo);
+            // the item's arguments into the warp's slot (the previous item's
+            // reads of it are done at the first sync)
+            constexpr int NW = (int)(sizeof(MtmaItemArgs) / 8);
+            __syncwarp();
+            if (lane < NW)
+                reinterpret_cast<unsigned long long*>(slot)[lane] =
+                    __ldg(reinterpret_cast<const unsigned long long*>(&E->ia) + lane);
+            __syncwarp();
         }
-        // geometry, maps, loader and store kind of this item's sweep
-        const MarchArgs& g = MULTI ? E->a : a;
-        const MarchTmaArgs& te = MULTI ? E->t : t;
+        // geometry, maps, loader and store kind of this item's sweep; the
+        // sweep's full arguments for the faces redone by the reference sequence
+        const auto& g = mtma_geo_of<MULTI>(a, slot);
+        const MarchTmaArgs& te = MULTI ? slot->t : t;
+        const MarchArgs& ga = MULTI ? E->a : a;
         const CUtensorMap* mapI = MULTI ? &E->tin : tin0;
         const CUtensorMap* mapL = MULTI ? &E->toutL : toutL0;
         const CUtensorMap* mapR = MULTI ? &E->toutR : toutR0;
@@ -432,9 +480,9 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
             if (!ok) {
                 // (the redo sequences take the weights and strides from the
                 // sweep's arguments)
-                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(g, column(u0, wv, vv), 3, L, R);
-                else if constexpr (ORDER == 7) march7_redo<MPF>(g, column(u0, wv, vv), 3, L, R);
-                else march_redo<MPF, PF>(g, column(u0, wv, vv), 3, L, R);
+                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(ga, column(u0, wv, vv), 3, L, R);
+                else if constexpr (ORDER == 7) march7_redo<MPF>(ga, column(u0, wv, vv), 3, L, R);
+                else march_redo<MPF, PF>(ga, column(u0, wv, vv), 3, L, R);
             }
             if (u0 + lane < g.Nu) {
                 const long long oi = 3 + (long long)(u0 + lane) * g.oU + wv * g.oW + vv * g.oV;
@@ -551,11 +599,11 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(g, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 7) march7_redo<MPF>(g, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(g, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(g, col, f0 + i, L, R);
-                    else march_redo<MPF, PF>(g, col, f0 + i, L, R);
+                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(ga, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 7) march7_redo<MPF>(ga, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(ga, col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(ga, col, f0 + i, L, R);
+                    else march_redo<MPF, PF>(ga, col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
@@ -635,20 +683,28 @@ __global__ void WSB_MTMA_BOUNDS(ORDER, T)
     sweep_march_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap toutL,
                            const __grid_constant__ CUtensorMap toutR, const __grid_constant__ MarchArgs a,
                            const MarchTmaArgs t) {
-    march_tma_body<MPF, KIND, T, LDR, PF, ORDER, WS, false>(&tin, &toutL, &toutR, a, t, nullptr, 0, a.n_items);
+    march_tma_body<MPF, KIND, T, LDR, PF, ORDER, WS, false>(&tin, &toutL, &toutR, a, t, nullptr, nullptr, 0,
+                                                              a.n_items);
 }
 
 // A group of sweeps in one launch: entries (64-byte aligned, in global
 // memory, written before the launch) in item order, n_items in all;
 // coefficients and shared-memory layout of the group in a and t.
+// FP64 grouped kernels run 2 CTAs per SM: with the entry lookup and both
+// loaders and store kinds, 3 CTAs (168 registers) spill 28-68 bytes in the
+// WENO5 face body, and the 96-block batch runs 3.5% faster at 2; FP32 fits
+// 3 without spills and is 6% faster there.
 #ifndef WSB_MTMA_MULTI_MIN_BLOCKS
-#define WSB_MTMA_MULTI_MIN_BLOCKS 3
+#define WSB_MTMA_MULTI_MIN_BLOCKS 2
 #endif
 template <bool MPF, int KIND, typename T, int ORDER, int WS>
-__global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7 : WSB_MTMA_MULTI_MIN_BLOCKS)
-    sweep_march_tma_multi_kernel(const MtmaEntry* __restrict__ ents, int n_ents, long long n_items,
-                                 const __grid_constant__ MarchArgs a, const MarchTmaArgs t) {
-    march_tma_body<MPF, KIND, T, 0, false, ORDER, WS, true>(nullptr, nullptr, nullptr, a, t, ents, n_ents,
+__global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
+                                                  : (sizeof(T) == 8 ? WSB_MTMA_MULTI_MIN_BLOCKS
+                                                                    : WSB_MTMA_MIN_BLOCKS_F32))
+    sweep_march_tma_multi_kernel(const MtmaEntry* __restrict__ ents, const long long* __restrict__ item0s,
+                                 int n_ents, long long n_items, const __grid_constant__ MarchArgs a,
+                                 const MarchTmaArgs t) {
+    march_tma_body<MPF, KIND, T, 0, false, ORDER, WS, true>(nullptr, nullptr, nullptr, a, t, ents, item0s, n_ents,
                                                               n_items);
 }
 
@@ -929,7 +985,7 @@ int launch_march_tma(const long long E[3], const SweepGeom& g, int dir, bool fol
 
 // Kernel of a group of sweeps, by storage T, order, weights, MP and tile
 // kind (null for WENO3 with TENO weights, which no engine covers).
-using MtmaMultiFn = void (*)(const MtmaEntry*, int, long long, MarchArgs, MarchTmaArgs);
+using MtmaMultiFn = void (*)(const MtmaEntry*, const long long*, int, long long, MarchArgs, MarchTmaArgs);
 template <typename T, int ORDER, int WS>
 MtmaMultiFn mtma_multi_pick(bool mp, bool kind1) {
     static const MtmaMultiFn tab[2][2] = {

@@ -517,7 +517,9 @@ struct MtmaGroup {
     MarchTmaArgs t{};         // shared-memory layout (the same for every entry)
     size_t smem = 0;
     std::vector<MtmaEntry> ents;
+    std::vector<long long> item0s;  // first work item of each entry
     MtmaEntry* d_ents = nullptr;
+    long long* d_item0s = nullptr;
     long long n_items = 0;
     double cost = 0;
 };
@@ -651,8 +653,10 @@ int batch_enqueue_sweeps(Batch* B, cudaStream_t st) {
 }
 
 void batch_free_groups(Batch* B) {
-    for (auto& G : B->groups)
+    for (auto& G : B->groups) {
         if (G.d_ents) cudaFree(G.d_ents);
+        if (G.d_item0s) cudaFree(G.d_item0s);
+    }
     B->groups.clear();
     B->rest.clear();
 }
@@ -708,17 +712,19 @@ int batch_plan_groups(Batch* B, int seg_faces) {
                         G->kind = P.t.kind;
                         G->a = P.a;
                         G->t = P.t;
-                        G->smem = P.smem;
+                        // plus the warps' argument slots
+                        G->smem = P.smem + (size_t)kTmaWarps * kMtmaSlot;
                     }
                     MtmaEntry me;
                     std::memset(&me, 0, sizeof(me));
                     me.tin = P.mi;
                     me.toutL = P.mL;
                     me.toutR = P.mR;
+                    me.ia.geo = mtma_geo(P.a);
+                    me.ia.t = P.t;
                     me.a = P.a;
-                    me.t = P.t;
-                    me.item0 = G->n_items;
                     G->ents.push_back(me);
+                    G->item0s.push_back(G->n_items);
                     G->n_items += P.a.n_items;
                     G->cost += batch_entry_cost(B, i);
                     placed = true;
@@ -730,6 +736,9 @@ int batch_plan_groups(Batch* B, int seg_faces) {
     for (auto& G : B->groups) {
         WSB_CUDA(cudaMalloc((void**)&G.d_ents, sizeof(MtmaEntry) * G.ents.size()));
         WSB_CUDA(cudaMemcpy(G.d_ents, G.ents.data(), sizeof(MtmaEntry) * G.ents.size(), cudaMemcpyHostToDevice));
+        WSB_CUDA(cudaMalloc((void**)&G.d_item0s, sizeof(long long) * G.item0s.size()));
+        WSB_CUDA(cudaMemcpy(G.d_item0s, G.item0s.data(), sizeof(long long) * G.item0s.size(),
+                            cudaMemcpyHostToDevice));
     }
     batch_release_graph(B);
     return WENO_SB_OK;
@@ -769,8 +778,8 @@ int batch_enqueue_groups(Batch* B, cudaStream_t st) {
             long long blocks = (G.n_items + kTmaWarps - 1) / kTmaWarps;
             blocks = std::min(blocks, (long long)sms * occ);
             if (blocks < 1) continue;
-            kfn<<<(unsigned)blocks, kTmaWarps * 32, G.smem, B->br[k]>>>(G.d_ents, (int)G.ents.size(), G.n_items, G.a,
-                                                                          G.t);
+            kfn<<<(unsigned)blocks, kTmaWarps * 32, G.smem, B->br[k]>>>(G.d_ents, G.d_item0s, (int)G.ents.size(),
+                                                                          G.n_items, G.a, G.t);
             rc = cuda_err(cudaGetLastError(), "grouped sweep launch");
         } else {
             const size_t i = (size_t)(~u.second);
