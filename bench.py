@@ -836,9 +836,40 @@ def measure_adjoint(dev, K):
 
     f_ms = _time_steps(fwd, stream, K)
     b_ms = _time_steps(bwd, stream, K)
+    # the other families: forward and VJP of the same step
+    fam = {}
+    for name, order, scheme, arrays in (("weno3_js", 3, wsb.JS, False), ("weno7_js", 7, wsb.JS, False),
+                                        ("weno5_teno", 5, wsb.TENO, False), ("weno7_teno", 7, wsb.TENO, False),
+                                        ("weno5_z", 5, wsb.Z, False), ("weno5_mapped", 5, wsb.MAPPED, False),
+                                        ("weno5_js_per_face_arrays", 5, wsb.JS, True)):
+        gf = wsb.Grid(m, m, m, nv, BUFF, scheme=scheme)
+        if arrays:
+            # (the device tensors stay referenced while their pointers are used)
+            held = [tuple(torch.from_numpy(np.ascontiguousarray(c.ravel(order="F"))).to(dev)
+                          for c in fields.uniform_weno_coefficients(order, g.nc(d))) for d in range(3)]
+            cf = held
+        else:
+            cf = [api.face_coefs(fields.uniform_weno_coefficients(order, g.nc(d))) for d in range(3)]
+
+        def fwd_f(gf=gf, cf=cf, order=order, arrays=arrays):
+            for d in range(3):
+                if arrays:
+                    api.weno(gf, d, order, v, cf[d], outs[0], outs[1], flags=fl, stream=sp)
+                else:
+                    api.weno_uniform(gf, d, order, v, cf[d], outs[0], outs[1], flags=fl, stream=sp)
+
+        def bwd_f(gf=gf, cf=cf, order=order, arrays=arrays):
+            for d in range(3):
+                api.vjp(gf, d, order, v, cf[d], gs[d][0], gs[d][1], gv, stream=sp, uniform=not arrays,
+                        flags=fl | (wsb.F_ACCUMULATE if d > 0 else 0))
+
+        ff = _time_steps(fwd_f, stream, K)
+        bb = _time_steps(bwd_f, stream, K)
+        fam[name] = {"forward_ms": ff, "vjp_ms": bb, "vjp_over_forward": bb / ff}
     return {"workload": "VJP of FP64 WENO5-JS + MP, x/y/z, 128^3 cells x 5 vars, folded input, "
                         "uniform coefficients, cotangents N(0,1)",
-            "forward_ms": f_ms, "vjp_ms": b_ms, "vjp_over_forward": b_ms / f_ms, "target_ratio": 2.5}
+            "forward_ms": f_ms, "vjp_ms": b_ms, "vjp_over_forward": b_ms / f_ms, "target_ratio": 2.5,
+            "families": fam}
 
 
 def _batch_blocks(n_blocks=96, seed=96):
@@ -855,24 +886,29 @@ def _batch_blocks(n_blocks=96, seed=96):
     return out
 
 
-def measure_batched(dev, K):
+def measure_batched(dev, K, n_blocks=96, layout=None, dtypes=("fp64", "fp32")):
     """96 uneven blocks (x/y/z sweeps each, MP fused, folded input) as one
     CUDA graph launch, run the way the autotuner picks (one persistent
     kernel over all blocks; per-block specialised sweeps on parallel graph
     branches; or grouped TMA marching sweeps, one launch per kernel
     instance over all its blocks), FP64 and FP32-bulk; the other ways and,
-    FP64, one launch per sweep for comparison."""
+    FP64, one launch per sweep for comparison.  n_blocks < 96 takes the
+    first blocks of the list; layout = (mode, threads, cols_per_item,
+    branches) fixes the way instead of autotuning and skips the comparisons
+    (a short command for profiling one way's kernels)."""
     import torch
 
     import wenostandalone_b200 as wsb
     from wenostandalone_b200 import api, fields
     stream = torch.cuda.Stream(device=dev)
     sp = int(stream.cuda_stream)
-    blocks = _batch_blocks()
+    blocks = _batch_blocks()[:n_blocks]
     res = {"workload": "96 blocks, cells per axis U{16..112}, v_size {5,8,10}, order {3,5,7}, JS/TENO "
                        "(teno_CT 1e-5), smooth-plus-jump fields, x/y/z sweeps + MP each = 288 sweeps",
            "blocks": len(blocks)}
     for dt_name, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        if dt_name not in dtypes:
+            continue
         entries, fs = [], 0
         for i, (cells, nv, order, scheme) in enumerate(blocks):
             m, n, p = (c - 1 for c in cells)
@@ -891,7 +927,11 @@ def measure_batched(dev, K):
                 fs += 2 * nf * c1 * c2 * nv
         b = api.Batch(entries)
         try:
-            t, u, tune_ms = b.autotune(stream=sp)
+            if layout is None:
+                t, u, tune_ms = b.autotune(stream=sp)
+            else:
+                b.configure(*layout)
+                t, u = layout[1], layout[2]
             mode, _, per_item, nb = b.query()
             ms = _time_steps(lambda: b.launch(stream=sp), stream, K)
             # the other ways of running the batch, at their default layouts
@@ -899,7 +939,7 @@ def measure_batched(dev, K):
             for m_o, cfg, key in ((0, (0, 128, 8, 8), "persistent_kernel_ms"),
                                   (1, (1, 128, 8, 8), "graph_of_sweeps_8_branches_ms"),
                                   (2, (2, 128, 64, 2), "grouped_sweeps_64_faces_2_branches_ms")):
-                if m_o != mode:
+                if m_o != mode and layout is None:
                     b.configure(*cfg)
                     other[key] = _time_steps(lambda: b.launch(stream=sp), stream, K)
         finally:
@@ -909,7 +949,7 @@ def measure_batched(dev, K):
                   2: {"mode": "grouped TMA marching sweeps", "faces_per_item": per_item, "branches": nb}}[mode]
         r = {"ms_per_step": ms, "value": fs / (ms * 1e-3), "face_states": fs, "choice": choice,
              "graph_launches_per_step": 1, **other}
-        if dt == torch.float64:
+        if dt == torch.float64 and layout is None:
             structs = [api.coefs_struct(e["coefs"]) for e in entries]
 
             def seq():
@@ -1054,8 +1094,12 @@ def run_only(args):
     import torch
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    fn = {"adjoint": measure_adjoint, "batched": measure_batched}[args.only]
-    res = fn(dev, max(1, args.steps))
+    if args.only == "batched":
+        layout = tuple(int(x) for x in args.batch_layout.split(",")) if args.batch_layout else None
+        dtypes = ("fp64", "fp32") if args.batch_dtype == "both" else (args.batch_dtype,)
+        res = measure_batched(dev, max(1, args.steps), n_blocks=args.batch_blocks, layout=layout, dtypes=dtypes)
+    else:
+        res = measure_adjoint(dev, max(1, args.steps))
     print(json.dumps({"measurement": args.only, **res}))
     return 0
 
@@ -1086,6 +1130,13 @@ def main():
     ap.add_argument("--only", choices=["adjoint", "batched"], default=None,
                     help="run only this side measurement on cuda:0 and print its JSON line "
                          "(a short command whose kernels can be profiled alone)")
+    ap.add_argument("--batch-blocks", type=int, default=96,
+                    help="--only batched: the first N blocks of the 96-block list")
+    ap.add_argument("--batch-layout", default=None,
+                    help="--only batched: MODE,THREADS,COLS_PER_ITEM,BRANCHES instead of autotuning "
+                         "(no comparisons with the other ways)")
+    ap.add_argument("--batch-dtype", choices=["fp64", "fp32", "both"], default="both",
+                    help="--only batched: storage precisions to run")
     args = ap.parse_args()
     if args.only:
         return run_only(args)

@@ -178,7 +178,15 @@ struct MtmaItemArgs {
     MtmaGeo geo;
     MarchTmaArgs t;
 };
-static_assert(sizeof(MtmaItemArgs) % 8 == 0 && sizeof(MtmaItemArgs) <= 256, "per-warp argument slot");
+struct MtmaEntry;
+// A warp's slot: the item's arguments and its entry (read where the maps or
+// the full arguments are needed, so no register holds it across the face
+// body).
+struct MtmaSlot {
+    MtmaItemArgs ia;
+    const MtmaEntry* e;
+};
+static_assert(sizeof(MtmaItemArgs) % 8 == 0 && sizeof(MtmaSlot) <= 256, "per-warp argument slot");
 constexpr int kMtmaSlot = 256;  // bytes of shared memory per warp for the item's arguments
 inline MtmaGeo mtma_geo(const MarchArgs& a) {
     MtmaGeo g{};
@@ -197,8 +205,8 @@ struct MtmaEntry {
 // The geometry of an item: the kernel's parameters (one sweep) or the
 // warp's shared-memory copy (grouped sweeps).
 template <bool MULTI>
-__device__ __forceinline__ const auto& mtma_geo_of(const MarchArgs& a, const MtmaItemArgs* slot) {
-    if constexpr (MULTI) return slot->geo;
+__device__ __forceinline__ const auto& mtma_geo_of(const MarchArgs& a, const MtmaSlot* slot) {
+    if constexpr (MULTI) return slot->ia.geo;
     else return a;
 }
 
@@ -247,8 +255,8 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
     unsigned char* ring = wbase + t.ring_off;
     unsigned long long* bars = (unsigned long long*)(base + (size_t)kTmaWarps * warp_bytes) + warp * S;
     // grouped sweeps: the warp's argument slot, after the mbarriers
-    MtmaItemArgs* slot = (MtmaItemArgs*)(base + (size_t)kTmaWarps * warp_bytes + (size_t)kTmaWarps * S * 8 +
-                                         (size_t)warp * kMtmaSlot);
+    MtmaSlot* slot = (MtmaSlot*)(base + (size_t)kTmaWarps * warp_bytes + (size_t)kTmaWarps * S * 8 +
+                                 (size_t)warp * kMtmaSlot);
     if (lane == 0) {
         for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -305,18 +313,23 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
             constexpr int NW = (int)(sizeof(MtmaItemArgs) / 8);
             __syncwarp();
             if (lane < NW)
-                reinterpret_cast<unsigned long long*>(slot)[lane] =
+                reinterpret_cast<unsigned long long*>(&slot->ia)[lane] =
                     __ldg(reinterpret_cast<const unsigned long long*>(&E->ia) + lane);
+            if (lane == 0) slot->e = E;
             __syncwarp();
         }
         // geometry, maps, loader and store kind of this item's sweep; the
         // sweep's full arguments for the faces redone by the reference sequence
         const auto& g = mtma_geo_of<MULTI>(a, slot);
-        const MarchTmaArgs& te = MULTI ? slot->t : t;
-        const MarchArgs& ga = MULTI ? E->a : a;
-        const CUtensorMap* mapI = MULTI ? &E->tin : tin0;
-        const CUtensorMap* mapL = MULTI ? &E->toutL : toutL0;
-        const CUtensorMap* mapR = MULTI ? &E->toutR : toutR0;
+        const MarchTmaArgs& te = MULTI ? slot->ia.t : t;
+        // (grouped: read from the slot where used)
+        auto ga = [&]() -> const MarchArgs& {
+            if constexpr (MULTI) return slot->e->a;
+            else return a;
+        };
+        auto mapI = [&]() { return MULTI ? &slot->e->tin : tin0; };
+        auto mapL = [&]() { return MULTI ? &slot->e->toutL : toutL0; };
+        auto mapR = [&]() { return MULTI ? &slot->e->toutR : toutR0; };
         const bool ldr = MULTI ? te.ldr != 0 : LDR == 1;
         // plain stores (face rows not 16-byte multiples): grouped sweeps only
         // (the single-sweep kernels keep their registers for the face body)
@@ -340,7 +353,7 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
                     const int c1 = te.dimJ == 1 ? J0 : (te.dimU == 1 ? cU : cW);
                     const int c2 = te.dimJ == 2 ? J0 : (te.dimU == 2 ? cU : cW);
                     mbar_arrive_expect_tx(bar, te.box_bytes + (PF ? (unsigned)RB : 0u));
-                    tma_load_4d(tile_ptr(k), mapI, bar, c0, c1, c2, v);
+                    tma_load_4d(tile_ptr(k), mapI(), bar, c0, c1, c2, v);
                     // rows J0 .. J0 + 8: the faces of the chunk starting at face J0
                     if constexpr (PF) bulk_load_1d((void*)srow(k, 0), row(J0), RB, bar);
                 }
@@ -480,9 +493,9 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
             if (!ok) {
                 // (the redo sequences take the weights and strides from the
                 // sweep's arguments)
-                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(ga, column(u0, wv, vv), 3, L, R);
-                else if constexpr (ORDER == 7) march7_redo<MPF>(ga, column(u0, wv, vv), 3, L, R);
-                else march_redo<MPF, PF>(ga, column(u0, wv, vv), 3, L, R);
+                if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(ga(), column(u0, wv, vv), 3, L, R);
+                else if constexpr (ORDER == 7) march7_redo<MPF>(ga(), column(u0, wv, vv), 3, L, R);
+                else march_redo<MPF, PF>(ga(), column(u0, wv, vv), 3, L, R);
             }
             if (u0 + lane < g.Nu) {
                 const long long oi = 3 + (long long)(u0 + lane) * g.oU + wv * g.oW + vv * g.oV;
@@ -599,11 +612,11 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
                     const int i = __ffs(bad) - 1;
                     bad &= bad - 1;
                     T L, R;
-                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(ga, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 7) march7_redo<MPF>(ga, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(ga, col, f0 + i, L, R);
-                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(ga, col, f0 + i, L, R);
-                    else march_redo<MPF, PF>(ga, col, f0 + i, L, R);
+                    if constexpr (ORDER == 7 && PF) march64_7_redo_faces<MPF>(ga(), col, f0 + i, L, R);
+                    else if constexpr (ORDER == 7) march7_redo<MPF>(ga(), col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3 && PF) march3_redo_faces<MPF>(ga(), col, f0 + i, L, R);
+                    else if constexpr (ORDER == 3) march3_redo<MPF, T>(ga(), col, f0 + i, L, R);
+                    else march_redo<MPF, PF>(ga(), col, f0 + i, L, R);
                     *(T*)(ob + swz<T>((unsigned)lane, (unsigned)i)) = L;
                     *(T*)(ob + OB + swz<T>((unsigned)lane, (unsigned)i)) = R;
                 }
@@ -615,14 +628,15 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
                 __syncwarp();
                 const int fi = lane & (F - 1);
                 if (fi < nF) {
-#pragma unroll
-                    for (int cc = lane / F; cc < 32; cc += 32 / F) {
-                        if (u0 + cc < g.Nu) {
-                            const long long oi = (long long)(f0 + fi) + (long long)(u0 + cc) * g.oU + wv * g.oW +
-                                                 vv * g.oV;
-                            outL[oi] = *(const T*)(ob + swz<T>((unsigned)cc, (unsigned)fi));
-                            outR[oi] = *(const T*)(ob + OB + swz<T>((unsigned)cc, (unsigned)fi));
-                        }
+                    // (a rolled loop with one running index: unrolled, its
+                    // addresses took 24 registers of the face body)
+                    const int c_end = g.Nu - u0 < 32 ? g.Nu - u0 : 32;
+                    const long long step = (long long)(32 / F) * g.oU;
+                    long long oi = (long long)(f0 + fi) + (long long)(u0 + lane / F) * g.oU + wv * g.oW + vv * g.oV;
+#pragma unroll 1
+                    for (int cc = lane / F; cc < c_end; cc += 32 / F, oi += step) {
+                        outL[oi] = *(const T*)(ob + swz<T>((unsigned)cc, (unsigned)fi));
+                        outR[oi] = *(const T*)(ob + OB + swz<T>((unsigned)cc, (unsigned)fi));
                     }
                 }
             } else {
@@ -637,8 +651,8 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
                 __syncwarp();
                 if (lane == 0) {
                     const int c1 = te.odimU == 1 ? u0 : wv, c2 = te.odimU == 2 ? u0 : wv;
-                    tma_store_4d(mapL, ob, f0, c1, c2, vv);
-                    tma_store_4d(mapR, ob + OB, f0, c1, c2, vv);
+                    tma_store_4d(mapL(), ob, f0, c1, c2, vv);
+                    tma_store_4d(mapR(), ob + OB, f0, c1, c2, vv);
                     bulk_commit();
                 }
             }
@@ -690,17 +704,21 @@ __global__ void WSB_MTMA_BOUNDS(ORDER, T)
 // A group of sweeps in one launch: entries (64-byte aligned, in global
 // memory, written before the launch) in item order, n_items in all;
 // coefficients and shared-memory layout of the group in a and t.
-// FP64 grouped kernels run 2 CTAs per SM: with the entry lookup and both
-// loaders and store kinds, 3 CTAs (168 registers) spill 28-68 bytes in the
-// WENO5 face body, and the 96-block batch runs 3.5% faster at 2; FP32 fits
-// 3 without spills and is 6% faster there.
+// CTAs per SM the FP64 grouped kernels are bounded for: column tiles 3
+// (WENO5's body fits 168 registers there), row tiles 2 (at 3 their WENO5
+// body spills 36-44 bytes and runs 2-3% slower); FP32 3.
 #ifndef WSB_MTMA_MULTI_MIN_BLOCKS
-#define WSB_MTMA_MULTI_MIN_BLOCKS 2
+#define WSB_MTMA_MULTI_MIN_BLOCKS 2     // FP64 row tiles
+#endif
+#ifndef WSB_MTMA_MULTI_MIN_BLOCKS_K1
+#define WSB_MTMA_MULTI_MIN_BLOCKS_K1 3  // FP64 column tiles
 #endif
 template <bool MPF, int KIND, typename T, int ORDER, int WS>
-__global__ void __launch_bounds__(kTmaWarps * 32, ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
-                                                  : (sizeof(T) == 8 ? WSB_MTMA_MULTI_MIN_BLOCKS
-                                                                    : WSB_MTMA_MIN_BLOCKS_F32))
+__global__ void __launch_bounds__(kTmaWarps * 32,
+                                  ORDER == 7 ? WSB_MTMA_MIN_BLOCKS_W7
+                                             : (sizeof(T) == 8 ? (KIND == 1 ? WSB_MTMA_MULTI_MIN_BLOCKS_K1
+                                                                            : WSB_MTMA_MULTI_MIN_BLOCKS)
+                                                               : WSB_MTMA_MIN_BLOCKS_F32))
     sweep_march_tma_multi_kernel(const MtmaEntry* __restrict__ ents, const long long* __restrict__ item0s,
                                  int n_ents, long long n_items, const __grid_constant__ MarchArgs a,
                                  const MarchTmaArgs t) {
