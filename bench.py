@@ -836,11 +836,11 @@ def measure_adjoint(dev, K):
 
     f_ms = _time_steps(fwd, stream, K)
     b_ms = _time_steps(bwd, stream, K)
-    # the other families: forward and VJP of the same step
+    # the other families the adjoint covers (JS and TENO weights): forward
+    # and VJP of the same step
     fam = {}
     for name, order, scheme, arrays in (("weno3_js", 3, wsb.JS, False), ("weno7_js", 7, wsb.JS, False),
                                         ("weno5_teno", 5, wsb.TENO, False), ("weno7_teno", 7, wsb.TENO, False),
-                                        ("weno5_z", 5, wsb.Z, False), ("weno5_mapped", 5, wsb.MAPPED, False),
                                         ("weno5_js_per_face_arrays", 5, wsb.JS, True)):
         gf = wsb.Grid(m, m, m, nv, BUFF, scheme=scheme)
         if arrays:

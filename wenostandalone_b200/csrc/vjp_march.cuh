@@ -1,6 +1,6 @@
-// vjp_march.cuh -- adjoint (VJP) of the FP64 WENO5-JS (+MP) sweep with
-// face-independent coefficients, marching along the sweep like the forward
-// kernel of sweep_march_tma.cuh.
+// vjp_march.cuh -- adjoint (VJP) of the FP64 WENO5 (+MP) sweep with JS or
+// TENO weights and face-independent coefficients, marching along the sweep
+// like the forward kernel of sweep_march_tma.cuh.
 //
 // A warp owns 32 adjacent columns of one (w, v) and walks the whole column.
 // At face J it recomputes the forward state from the carried window
@@ -13,8 +13,9 @@
 //     the minmod to the curvature it picked).  Faces whose median passes the
 //     WENO value through -- the common case -- skip this part as a warp.
 //   * weights: d out/d p_k = w_k, d out/d beta_k = -2 w_k (p_k - out)/beta_k
-//     (JS); sum_k w_k = 1, so d out/d v0 through the candidates is the
-//     cotangent itself;
+//     (JS); TENO weights d_k delta_k / sum d delta are constant between
+//     cutoff flips, so they pull nothing back to beta; sum_k w_k = 1, so
+//     d out/d v0 through the candidates is the cotangent itself;
 //   * candidates and beta are linear / quadratic in the differences
 //     d[k] = v[k+1] - v[k]; their gradients are summed per difference and a
 //     difference is turned into its two cells once its last face is done.
@@ -124,14 +125,26 @@ struct MarchVjp {
     // cotangent routed after the chunk (route_side).  `ok` is false when a
     // beta is outside [2^-100, 2^100): the face then contributes nothing
     // here and is redone after the chunk with the generic pull-back.
-    template <bool MPF>
+    // TENOW: TENO weights (f90:578-606), d_k delta_k / sum d delta with the
+    // cutoff flags delta_k of the forward sequence; the flags are constant
+    // between cutoff flips, so the weights pull nothing back to beta.
+    template <bool MPF, bool TENOW = false>
     __device__ __forceinline__ void face(const MarchArgs& a, double gLin, double gRin, int& pick, bool& ok) {
         const March64& w = f;
         ok = beta_ok(w.b0) && beta_ok(w.b1) && beta_ok(w.b2);
         const double B0 = ok ? w.b0 : 1.0, B1 = ok ? w.b1 : 1.0, B2 = ok ? w.b2 : 1.0;
+        double P0, P1, P2;
+        if constexpr (TENOW) {
+            bool k0, k1, k2;
+            ok = teno5_keep(B0, B1, B2, a.wp.teno_ct, k0, k1, k2) && ok;
+            P0 = k0 ? 1.0 : 0.0;
+            P1 = k1 ? 1.0 : 0.0;
+            P2 = k2 ? 1.0 : 0.0;
+        } else {
+            const double q0 = B0 * B0, q1 = B1 * B1, q2 = B2 * B2;
+            P0 = q1 * q2; P1 = q0 * q2; P2 = q0 * q1;
+        }
         const double gL = ok ? gLin : 0.0, gR = ok ? gRin : 0.0;
-        const double q0 = B0 * B0, q1 = B1 * B1, q2 = B2 * B2;
-        const double P0 = q1 * q2, P1 = q0 * q2, P2 = q0 * q1;
         const double aL0 = a.ucf[12] * P0, aL1 = a.ucf[13] * P1, aL2 = a.ucf[14] * P2;
         const double aR0 = a.ucf[15] * P0, aR1 = a.ucf[16] * P1, aR2 = a.ucf[17] * P2;
         const double SL = (aL0 + aL1) + aL2, SR = (aR0 + aR1) + aR2;
@@ -178,6 +191,7 @@ struct MarchVjp {
         gd0 = fma(a.ucf[1], gpL0, fma(a.ucf[7], gpR0, fma(a.ucf[2], gpL1, fma(a.ucf[8], gpR1, gd0))));
         gdm1 = fma(a.ucf[3], gpL1, fma(a.ucf[9], gpR1, fma(a.ucf[4], gpL2, fma(a.ucf[10], gpR2, gdm1))));
         gdm2 = fma(a.ucf[5], gpL2, fma(a.ucf[11], gpR2, gdm2));
+        if constexpr (TENOW) return;
         // d out / d beta_k = -2 w_k (e_k - x) / beta_k
         const double t0 = fma(gpL0, eL0 - xL, gpR0 * (eR0 - xR));
         const double t1 = fma(gpL1, eL1 - xL, gpR1 * (eR1 - xR));
@@ -260,7 +274,7 @@ __device__ __forceinline__ void route_side(bool left, int code, double g, const 
     }
 }
 
-template <bool MPF, int KIND>
+template <bool MPF, int KIND, bool TENOW = false>
 __global__ void __launch_bounds__(kVjpWarps * 32, 1)
     vjp_march_kernel(const __grid_constant__ CUtensorMap tv, const __grid_constant__ CUtensorMap tgL,
                      const __grid_constant__ CUtensorMap tgR, const __grid_constant__ CUtensorMap tgo,
@@ -359,7 +373,7 @@ __global__ void __launch_bounds__(kVjpWarps * 32, 1)
             const double gL = live ? __ldg(t.gLp + oi) : 0.0, gR = live ? __ldg(t.gRp + oi) : 0.0;
             int pk;
             bool ok;
-            m.face<MPF>(a, gL, gR, pk, ok);
+            m.face<MPF, TENOW>(a, gL, gR, pk, ok);
             if (pk || (!ok && live)) {
                 // cells 3..9 of the column = J-3 .. J+3 of face 3 (J = 6)
                 double c7[7], acc7[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -408,7 +422,7 @@ __global__ void __launch_bounds__(kVjpWarps * 32, 1)
                 const double gR = valid ? cot(kc, 1, i) : 0.0;
                 int pk;
                 bool ok;
-                m.face<MPF>(a, gL, gR, pk, ok);
+                m.face<MPF, TENOW>(a, gL, gR, pk, ok);
                 picks |= (unsigned long long)(valid ? pk : 0) << (6 * i);
                 bad |= (ok || !valid) ? 0u : (1u << i);
                 outv[i] = m.advance(a, (i < 2) ? cell(kc, 6 + i) : cell(kc + 1, i - 2)) + oldg(kc, i);
@@ -436,7 +450,7 @@ __global__ void __launch_bounds__(kVjpWarps * 32, 1)
                         for (int q = 0; q < 6; ++q) { cf.pL[q] = a.ucf[q]; cf.pR[q] = a.ucf[6 + q]; }
                         for (int q = 0; q < 3; ++q) { cf.dL[q] = a.ucf[12 + q]; cf.dR[q] = a.ucf[15 + q]; }
                         for (int q = 0; q < 9; ++q) cf.b[q] = a.ucf[18 + q];
-                        face_vjp<5>(c7 + 3, cf, JS, a.wp.eps, 0.0, MPF, gL, gR, acc7);
+                        face_vjp<5>(c7 + 3, cf, TENOW ? TENO : JS, a.wp.eps, a.wp.teno_ct, MPF, gL, gR, acc7);
                     } else {
                         route_side(true, pk & 7, gL, c7 + 1, acc7 + 1);
                         route_side(false, pk >> 3, gR, c7 + 1, acc7 + 1);
@@ -573,8 +587,13 @@ inline int launch_vjp_march(const long long E[3], const SweepGeom& g, int dir, b
     const size_t smem = 1024 + (size_t)kVjpWarps * t.warp_bytes + (size_t)kVjpWarps * kVjpStages * 8;
     using KFn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, CUtensorMap, CUtensorMap, MarchArgs, VjpMarchArgs,
                          double*);
-    const KFn kfn = mp ? (kind1 ? vjp_march_kernel<true, 1> : vjp_march_kernel<true, 0>)
-                       : (kind1 ? vjp_march_kernel<false, 1> : vjp_march_kernel<false, 0>);
+    const bool teno = wp.scheme == TENO;
+    static const KFn table[2][2][2] = {
+        {{vjp_march_kernel<false, 0, false>, vjp_march_kernel<false, 1, false>},
+         {vjp_march_kernel<true, 0, false>, vjp_march_kernel<true, 1, false>}},
+        {{vjp_march_kernel<false, 0, true>, vjp_march_kernel<false, 1, true>},
+         {vjp_march_kernel<true, 0, true>, vjp_march_kernel<true, 1, true>}}};
+    const KFn kfn = table[teno ? 1 : 0][mp ? 1 : 0][kind1 ? 1 : 0];
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kVjpWarps * 32, smem);

@@ -466,7 +466,8 @@ int launch_vjp(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsign
     if (folded && !acc_flag)
         WSB_CUDA(cudaMemsetAsync(gv, 0, sizeof(double) * d.E[0] * d.E[1] * d.E[2] * d.nv, st));
     const bool uni = ucf != nullptr;
-    if (uni && order == 5 && gr->scheme == WENO_SB_JS && kernel_choice() != 1 && march_weights_ok(ucf)) {
+    if (uni && order == 5 && (gr->scheme == WENO_SB_JS || gr->scheme == WENO_SB_TENO) && kernel_choice() != 1 &&
+        march_weights_ok(ucf)) {
         int rc = launch_vjp_march(d.E, a.g, dir, folded, a.mp != 0, a.accumulate != 0, v, ucf, a.wp, gL, gR, gv, st,
                                   num_sms());
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "vjp march launch") : rc;
