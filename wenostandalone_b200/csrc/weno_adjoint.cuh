@@ -238,17 +238,21 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
             } else {
                 tau = fabs(beta[R - 1] - beta[0]);
             }
+            // (quotients here and below by Newton-refined reciprocals: an
+            // FP64 division is a long instruction sequence, and these paths
+            // had up to 5R + 1 of them per face)
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+                const double x = fma(tau, mid_range(beta[r]) ? nr_rcp(beta[r]) : 1.0 / beta[r], 1.0);
                 if (ORDER == 7) {
-                    const double a3 = ipow3(1.0 + tau / beta[r]);
+                    const double a3 = ipow3(x);
                     al[r] = a3 * a3;
                 } else {
-                    al[r] = ipow6(1.0 + tau / beta[r]);
+                    al[r] = ipow6(x);
                 }
             }
             if (ORDER == 7) {
-                const double a3 = ipow3(1.0 + tau / eps);
+                const double a3 = ipow3(fma(tau, nr_rcp(eps), 1.0));
                 a4 = a3 * a3;
             }
             // reference sums in weight order q = 0..
@@ -259,8 +263,9 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
                 s += al[r];
             }
             if (ORDER == 7) s += a4;
+            const double rs = mid_range(s) ? nr_rcp(s) : 1.0 / s;
 #pragma unroll
-            for (int r = 0; r < R; ++r) delta[r] = (al[r] / s < teno_ct) ? 0.0 : 1.0;
+            for (int r = 0; r < R; ++r) delta[r] = (al[r] * rs < teno_ct) ? 0.0 : 1.0;
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -269,8 +274,12 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
                 aL[r] = delta[r] * cf_d<ORDER>(cf, true, q);
                 aR[r] = delta[r] * cf_d<ORDER>(cf, false, q);
             } else {
-                aL[r] = cf_d<ORDER>(cf, true, q) / (beta[r] * beta[r]);
-                aR[r] = cf_d<ORDER>(cf, false, q) / (beta[r] * beta[r]);
+                // d / beta^2 by one reciprocal shared by both sides (division
+                // outside the reciprocal's range)
+                const double q2 = beta[r] * beta[r];
+                const double rq = mid_range(q2) ? nr_rcp(q2) : 1.0 / q2;
+                aL[r] = cf_d<ORDER>(cf, true, q) * rq;
+                aR[r] = cf_d<ORDER>(cf, false, q) * rq;
             }
             SL += aL[r];
             SR += aR[r];
@@ -279,10 +288,13 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
             SL += a4;
             SR += a4;
         }
+        {
+            const double rL = mid_range(SL) ? nr_rcp(SL) : 1.0 / SL, rR = mid_range(SR) ? nr_rcp(SR) : 1.0 / SR;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            wL[r] = aL[r] / SL;
-            wR[r] = aR[r] / SR;
+            for (int r = 0; r < R; ++r) {
+                wL[r] = aL[r] * rL;
+                wR[r] = aR[r] * rR;
+            }
         }
         SL4 = SL;
         SR4 = SR;
@@ -352,10 +364,11 @@ __device__ void face_vjp(const double* v, const Coef<ORDER>& cf, int scheme, dou
     }
     if (ORDER == 7 && scheme == TENO) {
         // alpha(4) = (1 + |eps - beta(3)|/eps)^6 sits in both sums
-        const double ga4 = gLw * (0.0 - Lw) / SL4 + gRw * (0.0 - Rw) / SR4;
-        const double base = 1.0 + tau4 / eps;
+        const double re = nr_rcp(eps);
+        const double ga4 = (gLw * (0.0 - Lw)) * nr_rcp(SL4) + (gRw * (0.0 - Rw)) * nr_rcp(SR4);
+        const double base = fma(tau4, re, 1.0);
         const double b2 = base * base;
-        const double da4 = 6.0 * (b2 * b2 * base) / eps;   // d a4 / d tau
+        const double da4 = 6.0 * (b2 * b2 * base) * re;   // d a4 / d tau
         const double sgn = (beta[0] - eps) >= 0.0 ? 1.0 : -1.0;
         gbeta[0] += ga4 * da4 * sgn;
     }
@@ -427,27 +440,52 @@ __global__ void __launch_bounds__(128) vjp_kernel(const VjpArgs a) {
         for (int q = 0; q < 6; ++q) w[q] = __ldg(vin + q * sJ);
 #pragma unroll
         for (int q = 0; q < 7; ++q) acc[q] = 0.0;
+        // the new cell, the two cotangents and (accumulating) the old
+        // gradient of step o are loaded four steps earlier and passed down a
+        // chain of registers (each step's loads used at once, the gradient's
+        // read-modify-write among them, left the kernel waiting on memory
+        // latency at every step).  Only this thread touches the column's
+        // cells in this launch, so the old gradient read ahead is current.
+        // Loads past the column's end read its last element and are unused.
+        const long long ncell = ns + 6;
+        const bool acc_on = a.accumulate != 0;
+        auto fetch = [&](long long o, double& x, double& l, double& r, double& q) {
+            const long long jc = o + 6 < ncell ? o + 6 : ncell - 1;
+            const long long oc = o < ns ? o : ns - 1;
+            x = __ldg(vin + jc * sJ);
+            l = __ldg(gLc + oc);
+            r = __ldg(gRc + oc);
+            q = acc_on ? gout[oc * sJ] : 0.0;
+        };
+        double x0, x1, x2, x3, l0, l1, l2, l3, r0, r1, r2, r3, q0, q1, q2, q3;
+        fetch(0, x0, l0, r0, q0);
+        fetch(1, x1, l1, r1, q1);
+        fetch(2, x2, l2, r2, q2);
+        fetch(3, x3, l3, r3, q3);
         for (long long o = 0; o < ns; ++o) {
-            w[6] = __ldg(vin + (o + 6) * sJ);
+            w[6] = x0;
+            const double gLo = l0, gRo = r0, gvo = q0;
+            x0 = x1; x1 = x2; x2 = x3;
+            l0 = l1; l1 = l2; l2 = l3;
+            r0 = r1; r1 = r2; r2 = r3;
+            q0 = q1; q1 = q2; q2 = q3;
+            fetch(o + 4, x3, l3, r3, q3);
             const bool face_ok = (ORDER == 3) || (o >= 3 && o <= ns - 4);
             if (face_ok) {
                 const bool core = (o >= 3 && o <= ns - 4);
                 if constexpr (UNI) {
                     face_vjp<ORDER>(w + 3, *reinterpret_cast<const Coef<ORDER>*>(a.uc.v), a.wp.scheme, a.wp.eps,
-                                    a.wp.teno_ct, a.mp && core, __ldg(gLc + o), __ldg(gRc + o), acc);
+                                    a.wp.teno_ct, a.mp && core, gLo, gRo, acc);
                 } else {
                     long long c = o - 3;
                     c = c < 0 ? 0 : (c > a.g.nc - 1 ? a.g.nc - 1 : c);
                     Coef<ORDER> cf;
                     cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.g.nc, c);
-                    face_vjp<ORDER>(w + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, a.mp && core, __ldg(gLc + o),
-                                    __ldg(gRc + o), acc);
+                    face_vjp<ORDER>(w + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, a.mp && core, gLo, gRo, acc);
                 }
             }
             // cell J = o is complete
-            double* dst = gout + o * sJ;
-            if (a.accumulate) *dst += acc[0];
-            else *dst = acc[0];
+            gout[o * sJ] = gvo + acc[0];
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
                 acc[q] = acc[q + 1];
