@@ -441,12 +441,14 @@ __global__ void __launch_bounds__(128) vjp_kernel(const VjpArgs a) {
 #pragma unroll
         for (int q = 0; q < 7; ++q) acc[q] = 0.0;
         // the new cell, the two cotangents and (accumulating) the old
-        // gradient of step o are loaded four steps earlier and passed down a
-        // chain of registers (each step's loads used at once, the gradient's
-        // read-modify-write among them, left the kernel waiting on memory
-        // latency at every step).  Only this thread touches the column's
-        // cells in this launch, so the old gradient read ahead is current.
-        // Loads past the column's end read its last element and are unused.
+        // gradient of step o are loaded four steps earlier into slot o % 4 of
+        // a register ring (the loop is unrolled four times, so no register
+        // moves wait on a load in flight; each step's loads used at once,
+        // the gradient's read-modify-write among them, left the kernel
+        // waiting on memory latency at every step).  Only this thread touches
+        // the column's cells in this launch, so the old gradient read ahead
+        // is current.  Loads past the column's end read its last element and
+        // are not used.
         const long long ncell = ns + 6;
         const bool acc_on = a.accumulate != 0;
         auto fetch = [&](long long o, double& x, double& l, double& r, double& q) {
@@ -457,41 +459,41 @@ __global__ void __launch_bounds__(128) vjp_kernel(const VjpArgs a) {
             r = __ldg(gRc + oc);
             q = acc_on ? gout[oc * sJ] : 0.0;
         };
-        double x0, x1, x2, x3, l0, l1, l2, l3, r0, r1, r2, r3, q0, q1, q2, q3;
-        fetch(0, x0, l0, r0, q0);
-        fetch(1, x1, l1, r1, q1);
-        fetch(2, x2, l2, r2, q2);
-        fetch(3, x3, l3, r3, q3);
-        for (long long o = 0; o < ns; ++o) {
-            w[6] = x0;
-            const double gLo = l0, gRo = r0, gvo = q0;
-            x0 = x1; x1 = x2; x2 = x3;
-            l0 = l1; l1 = l2; l2 = l3;
-            r0 = r1; r1 = r2; r2 = r3;
-            q0 = q1; q1 = q2; q2 = q3;
-            fetch(o + 4, x3, l3, r3, q3);
-            const bool face_ok = (ORDER == 3) || (o >= 3 && o <= ns - 4);
-            if (face_ok) {
-                const bool core = (o >= 3 && o <= ns - 4);
-                if constexpr (UNI) {
-                    face_vjp<ORDER>(w + 3, *reinterpret_cast<const Coef<ORDER>*>(a.uc.v), a.wp.scheme, a.wp.eps,
-                                    a.wp.teno_ct, a.mp && core, gLo, gRo, acc);
-                } else {
-                    long long c = o - 3;
-                    c = c < 0 ? 0 : (c > a.g.nc - 1 ? a.g.nc - 1 : c);
-                    Coef<ORDER> cf;
-                    cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.g.nc, c);
-                    face_vjp<ORDER>(w + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, a.mp && core, gLo, gRo, acc);
-                }
-            }
-            // cell J = o is complete
-            gout[o * sJ] = gvo + acc[0];
+        constexpr int P = 4;
+        double px[P], pl[P], pr[P], pq[P];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                acc[q] = acc[q + 1];
-                w[q] = w[q + 1];
+        for (int k = 0; k < P; ++k) fetch(k, px[k], pl[k], pr[k], pq[k]);
+        for (long long o0 = 0; o0 < ns; o0 += P) {
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const long long o = o0 + k;
+                if (o >= ns) break;
+                w[6] = px[k];
+                const double gLo = pl[k], gRo = pr[k], gvo = pq[k];
+                fetch(o + P, px[k], pl[k], pr[k], pq[k]);
+                const bool face_ok = (ORDER == 3) || (o >= 3 && o <= ns - 4);
+                if (face_ok) {
+                    const bool core = (o >= 3 && o <= ns - 4);
+                    if constexpr (UNI) {
+                        face_vjp<ORDER>(w + 3, *reinterpret_cast<const Coef<ORDER>*>(a.uc.v), a.wp.scheme, a.wp.eps,
+                                        a.wp.teno_ct, a.mp && core, gLo, gRo, acc);
+                    } else {
+                        long long c = o - 3;
+                        c = c < 0 ? 0 : (c > a.g.nc - 1 ? a.g.nc - 1 : c);
+                        Coef<ORDER> cf;
+                        cf.load(a.cp.polyL, a.cp.polyR, a.cp.dL, a.cp.dR, a.cp.beta, a.g.nc, c);
+                        face_vjp<ORDER>(w + 3, cf, a.wp.scheme, a.wp.eps, a.wp.teno_ct, a.mp && core, gLo, gRo, acc);
+                    }
+                }
+                // cell J = o is complete
+                gout[o * sJ] = gvo + acc[0];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    acc[q] = acc[q + 1];
+                    w[q] = w[q + 1];
+                }
+                acc[6] = 0.0;
             }
-            acc[6] = 0.0;
         }
         // cells ns .. ns+5
 #pragma unroll
