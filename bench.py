@@ -385,6 +385,7 @@ def run_ours(args):
     adjoint = batched = mixed = families = None
     if not args.no_extras and rank == 0 and ws == 1 and not fp32_main:
         Kx = max(3, min(K, 10))
+        torch.cuda.empty_cache()
         adjoint = measure_adjoint(dev, Kx)
         torch.cuda.empty_cache()
         batched = measure_batched(dev, Kx)

@@ -185,7 +185,9 @@ int weno_sb_reshape_dev(const weno_sb_grid *g, int dir, int dtype, const double 
 int weno_sb_order1_dev(const weno_sb_grid *g, int dir, int dtype, const double *v_vf,
                        void *vL, void *vR, void *stream);
 /* Reconstruction, order 3/5/7 (f90:392-1542).  v_in is v_rs_ws_dir, or
- * v_vf when flags has WENO_SB_F_FOLDED. */
+ * v_vf when flags has WENO_SB_F_FOLDED.  Per-face coefficient arrays take a
+ * per-face table, allocated and freed stream-ordered on `stream`
+ * (cudaMallocAsync). */
 int weno_sb_weno_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, int dtype,
                      const void *v_in, const weno_sb_coefs *coefs, void *vL, void *vR,
                      void *stream);
@@ -194,7 +196,7 @@ int weno_sb_weno_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, 
  * f90:256-277 fills identically for every face): the kernels take them from
  * the kernel-parameter bank instead of per-thread registers.  The handle
  * API uses this path by itself when the uploaded coefficient arrays are
- * face-independent. */
+ * face-independent.  Allocates nothing. */
 int weno_sb_weno_uniform_dev(const weno_sb_grid *g, int dir, int order, unsigned flags, int dtype,
                              const void *v_in, const weno_sb_face_coefs *face, void *vL, void *vR,
                              void *stream);

@@ -315,7 +315,16 @@ __device__ __forceinline__ void march_tma_body(const CUtensorMap* tin0, const CU
             if (lane < NW)
                 reinterpret_cast<unsigned long long*>(&slot->ia)[lane] =
                     __ldg(reinterpret_cast<const unsigned long long*>(&E->ia) + lane);
-            if (lane == 0) slot->e = E;
+            if (lane == 0) {
+                slot->e = E;
+                // the entry's maps are read by the TMA unit from global
+                // memory, where a table freed and allocated again may hold
+                // other maps at the same address: drop any copy cached for
+                // it (lane 0 issues the item's bulk copies)
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&E->tin) : "memory");
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&E->toutL) : "memory");
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&E->toutR) : "memory");
+            }
             __syncwarp();
         }
         // geometry, maps, loader and store kind of this item's sweep; the

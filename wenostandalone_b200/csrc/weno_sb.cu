@@ -352,6 +352,14 @@ int launch_march_faces(const long long E[3], const SweepGeom& g, int dir, bool f
     return cuda_err(le, "march sweep launch (per-face coefficients)");
 }
 
+// Status of a marching launch helper as the library's: 0 -> the launch's
+// own error, a CUDA error (< 1000) with its message, else as is.
+int march_rc(int rc, const char* what) {
+    if (rc == 0) return cuda_err(cudaGetLastError(), what);
+    if (rc < 1000) return cuda_err((cudaError_t)rc, what);
+    return rc;
+}
+
 // Coefficients come either per face (cf, device arrays) or, when ucf is
 // non-null, as one face-independent set laid out like Coef<order>.
 template <typename T>
@@ -371,26 +379,26 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, order);
         int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), order, WENO_SB_TENO);
         if (rc != WENO_SB_ERR_UNSUPPORTED)
-            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (TENO)") : rc;
+            return march_rc(rc, "march tma sweep launch (TENO)");
     }
     if ((choice == 0 || choice == 3) && ucf && order == 5 && sizeof(T) == 8 &&
         ((gr->scheme == WENO_SB_Z && march_weights_ok(ucf)) || (gr->scheme == WENO_SB_MAPPED && march_mapped_ok(ucf)))) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 5);
         int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 5, gr->scheme);
         if (rc != WENO_SB_ERR_UNSUPPORTED)
-            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (mapped / Z)") : rc;
+            return march_rc(rc, "march tma sweep launch (mapped / Z)");
     }
     if ((choice == 0 || choice == 3) && ucf && order == 3 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 3)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 3);
         int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 3);
         if (rc != WENO_SB_ERR_UNSUPPORTED)
-            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (WENO3)") : rc;
+            return march_rc(rc, "march tma sweep launch (WENO3)");
     }
     if ((choice == 0 || choice == 3) && ucf && order == 7 && gr->scheme == WENO_SB_JS && march_weights_ok(ucf, 7)) {
         const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf, 7);
         int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms(), 7);
         if (rc != WENO_SB_ERR_UNSUPPORTED)
-            return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch (WENO7)") : rc;
+            return march_rc(rc, "march tma sweep launch (WENO7)");
     }
     if ((choice == 0 || choice == 3 || choice == 5) && ucf && order == 5 && gr->scheme == WENO_SB_JS &&
         march_weights_ok(ucf)) {
@@ -398,7 +406,7 @@ int run_weno(const Dims& d, const weno_sb_grid* gr, int dir, int order, unsigned
             const MarchArgs a0 = make_march_args(g, in, vL, vR, wp, ucf);
             int rc = launch_march_tma<T>(d.E, g, dir, folded, mp, in, vL, vR, a0, st, num_sms());
             if (rc != WENO_SB_ERR_UNSUPPORTED)
-                return rc == 0 ? cuda_err(cudaGetLastError(), "march tma sweep launch") : rc;
+                return march_rc(rc, "march tma sweep launch");
         }
         int rc = launch_march_sweep<T>(g, mp, in, vL, vR, wp, ucf, st, num_sms());
         if (rc != WENO_SB_ERR_UNSUPPORTED) return rc == 0 ? cuda_err(cudaGetLastError(), "march sweep launch") : rc;
